@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Throughput benchmark: Kelvin-Helmholtz 4096^2, PLM + HLLC + RK2, FP64.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One "step" is one RK2 time step over the whole 4096^2 grid (the hot path of
+Sim::Advance).  Prints one JSON line (rank 0).
+
+ours (default):
+  * value: zone-updates/s over exactly K device-resident steps, timed with
+    CUDA events on the library's stream between a barrier + synchronize on
+    both sides; max over ranks.  The state (4 x 4100^2 doubles, 538 MB per
+    buffer) is larger than L2, so no flush is needed between steps.
+  * e2e: the same metric through the public C ABI with host buffers: every
+    step uploads the state from pinned host memory (gk_upload_cons), runs one
+    time step (gk_run_steps) and downloads it (gk_download_planes).
+  * roofline: the fused stage kernel's algorithmic HBM bytes per launch
+    (80 B per cell on average: stage 1 reads and writes 4 doubles, stage 2
+    reads 8 and writes 4) over its average launch time, measured with CUDA
+    events around each launch in an un-graphed pass of the same workload.
+  * cpu_baseline: the reference itself (oracle/_ref/ref_fast_kh_baseline,
+    built from the reference sources with its Makefile flags) on this host's
+    cores, on a bounded number of steps of the same problem; rank 0, N=1.
+  With N > 1 each rank runs an independent replica (weak scaling, no
+  collective on the data path); torch.distributed is used only for the
+  barrier and the max over ranks.
+
+reference: the reference's OpenMP CPU path on the host cores, same metric;
+  each step is one time step of KH at the largest size from {4096^2,
+  2048^2, 1024^2} that keeps the whole run within about two minutes.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s"
+UNIT = "zone-updates/s"
+BYTES_PER_ZU_RK2 = 160  # 5 * V * 8 B with V = 4 (2D): algorithmic HBM bytes per zone-update
+STAGE_BYTES_PER_CELL = 80  # per stage launch, averaged over the two RK2 stages
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per stage-kernel launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "stage2d_kh4096_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.device)], stdout=self.out,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"],
+                    "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def config_dict(n, mode, extra=None):
+    d = {"workload": f"Kelvin-Helmholtz {n}x{n}, PLM (van Leer) + HLLC + RK2, CFL 0.4, periodic",
+         "grid": [n, n], "integrator": "rk2", "reconstruction": "plm-vanleer", "riemann": "hllc",
+         "arith_mode": mode, "l2": "state larger than L2 (538 MB per buffer); no flush needed",
+         "parallelism": "replicas"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# --------------------------------------------------------------- reference
+def run_reference_binary(exe, n, steps, threads, timeout=900):
+    """Runs the reference build on KH n^2 for `steps` steps; returns the
+    driver's JSON (per-step timestamps included)."""
+    from gaukuk_b200 import problems
+    p, _ = problems.kh(8)
+    import dataclasses
+    p = dataclasses.replace(p, nx=n, ny=n, stepmax=steps, tmax=2.0, dtoutput=2.0)
+    with tempfile.TemporaryDirectory() as td:
+        inf = os.path.join(td, "kh.in")
+        with open(inf, "w") as f:
+            f.write(p.to_in_text({"seed": 0, "amp": 0.01, "noise": 1e-3}))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        r = subprocess.run([exe, "-i", inf, "--step-times"], cwd=td, capture_output=True,
+                           text=True, timeout=timeout, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference run failed: {r.stderr[-500:]}")
+        return json.loads(r.stderr.strip().splitlines()[-1])
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_rate(exe, n, warm, steps, threads):
+    """zone-updates/s of the reference over steps warm+1 .. warm+steps."""
+    d = run_reference_binary(exe, n, warm + steps, threads)
+    st = d["step_stamps"]
+    # stamps[i] is written at the end of step i+1
+    t = st[warm + steps - 1] - st[warm - 1] if warm >= 1 else st[steps - 1]
+    return n * n * steps / t, t, d
+
+
+def reference_exe():
+    return os.path.join(ROOT, "oracle", "_ref", "ref_fast_kh_baseline")
+
+
+def main_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    exe = reference_exe()
+    base = {"metric": METRIC, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference build oracle/_ref missing (run build())"}))
+        return 0
+    threads = host_threads()
+    # calibrate on 1024^2: seconds per zone-update on this host
+    rate0, _, _ = cpu_rate(exe, 1024, 1, 3, threads)
+    budget_s = 120.0
+    n = 1024
+    for cand in (4096, 2048, 1024):
+        if cand * cand * (args.warmup + args.steps) / rate0 <= budget_s:
+            n = cand
+            break
+    warm = max(1, args.warmup)
+    rate, secs, _ = cpu_rate(exe, n, warm, args.steps, threads)
+    cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+           "sample": f"KH {n}^2 RK2 PLM HLLC, steps {warm + 1}..{warm + args.steps} of one run, "
+                     f"reference Makefile flags (-O3 -ffast-math -funroll-loops, OpenMP) "
+                     f"with -march=x86-64-v3"}
+    out = dict(base)
+    out.update({"value": rate, "ms_per_step": 1000.0 * secs / args.steps,
+                "config": config_dict(args.n, "reference-cpu",
+                                      {"reference_grid": [n, n], "parallelism": "openmp"}),
+                "cpu_baseline": cpu,
+                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}})
+    print(json.dumps(out))
+    return 0
+
+
+# --------------------------------------------------------------- ours
+def main_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    from gaukuk_b200 import problems
+    from gaukuk_b200.sim import Sim
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(local_rank)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = args.n
+    p, c = problems.kh(n, seed=rank)
+    cells = p.nx * p.ny
+    sim = Sim(p, c, mode=args.mode, device=local_rank)
+    stream = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", local_rank))
+    steps_per_graph, launches_per_step = sim.graph_info()
+
+    # warm-up
+    sim.run_steps(args.warmup)
+    step0 = sim.get_step()
+
+    def timed(sim_, k):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        ev0.record(stream)
+        sim_.enqueue_steps(k)
+        ev1.record(stream)
+        ev1.synchronize()
+        barrier()
+        return ev0.elapsed_time(ev1)
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    ms = timed(sim, args.steps)
+    clocks = sampler.stop()
+    took = sim.get_step() - step0
+    if took != args.steps:
+        raise RuntimeError(f"expected {args.steps} steps, device ran {took}")
+    ms_max = max_over_ranks(ms)
+    value = world * cells * args.steps / (ms_max / 1000.0)
+
+    # the other arithmetic mode, same workload (reported, not the headline)
+    other_mode = "parity" if args.mode == "fast" else "fast"
+    sim2 = Sim(p, c, mode=other_mode, device=local_rank)
+    sim2.run_steps(args.warmup)
+    ms2 = max_over_ranks(timed(sim2, max(2, args.steps // 4)))
+    other = {"arith_mode": other_mode,
+             "value": world * cells * max(2, args.steps // 4) / (ms2 / 1000.0),
+             "ms_per_step": ms2 / max(2, args.steps // 4)}
+    sim2.close()
+
+    # per-kernel profile (events around every launch, un-graphed)
+    prof_steps = 4
+    prof = sim.profile(prof_steps)
+    total = sum(v[0] for v in prof.values())
+    shares = {k: {"ms_total": v[0], "launches": v[1], "share": v[0] / total if total else None}
+              for k, v in prof.items()}
+    stage_ms, stage_n = prof.get("stage2d", (0.0, 0))
+    avg_stage_s = (stage_ms / stage_n) / 1000.0 if stage_n else None
+    peak, peak_kind = measured_peaks()
+    roof = None
+    if avg_stage_s:
+        achieved = STAGE_BYTES_PER_CELL * cells / avg_stage_s / 1e9
+        roof = {"bound": "hbm", "kernel": "gk_fast::k_stage2d" if args.mode == "fast"
+                else "gk_parity::k_stage2d",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6.65 TB/s",
+                "algorithmic_bytes_per_launch": STAGE_BYTES_PER_CELL * cells,
+                "avg_launch_ms": avg_stage_s * 1000.0,
+                "traffic": ncu_traffic(),
+                "step_frac_of_hbm_roofline": (BYTES_PER_ZU_RK2 * value / world / 1e9) / peak}
+
+    # end to end through the C ABI with pinned host buffers
+    e2e_steps = max(1, args.e2e_steps)
+    host = torch.empty(p.shape, dtype=torch.float64, pin_memory=True).numpy()
+    host[...] = c
+    g = p.ng
+    h2d = 5 * p.lenx * p.leny * 8
+    d2h = 5 * p.lenx * p.leny * 8
+    sim.upload(host)
+    sim.run_steps(1)
+    sim.download(host, planes_only=True)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim.upload(host)
+        sim.run_steps(1)
+        sim.download(host, planes_only=True)
+    t1 = time.perf_counter()
+    e2e_s = max_over_ranks(t1 - t0)
+    e2e_value = world * cells * e2e_steps / e2e_s
+    assert np.isfinite(host[0, g, g:g + p.ny, g:g + p.nx]).all()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        exe = reference_exe()
+        if os.path.exists(exe):
+            threads = host_threads()
+            rate0, _, _ = cpu_rate(exe, 1024, 1, 3, threads)
+            # bounded sample: about 15 s of CPU work on the full grid
+            nsteps = int(max(3, min(40, 15.0 * rate0 / cells)))
+            rate, secs, _ = cpu_rate(exe, n, 1, nsteps, threads)
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"KH {n}^2, steps 2..{nsteps + 1} of one run ({secs:.1f} s), "
+                             f"reference Makefile flags with -march=x86-64-v3, OpenMP"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
+                   "sample": "reference build absent"}
+
+    if rank == 0:
+        launches = launches_per_step * steps_per_graph * (-(-args.steps // steps_per_graph)) + 1
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic (seeded KH initial condition of the named shape)",
+               "config": config_dict(n, args.mode, {"path": sim.path}),
+               "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                       "timing": "host wall clock around the C-ABI calls, max over ranks"},
+               "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+               "gpu_launches": launches, "kernel_shares": shares, "other_mode": other}
+        print(json.dumps(out))
+    sim.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=None)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="fast", choices=["fast", "parity"])
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if args.gpus is not None and world == 1 and args.gpus > 1:
+        print(json.dumps({"error": "launch N>1 with torch.distributed.run"}))
+        return 2
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return main_reference(args, rank, world)
+    return main_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

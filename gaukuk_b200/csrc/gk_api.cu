@@ -1,0 +1,657 @@
+// gk_api.cu -- the C ABI of include/gaukuk_cuda.h.
+//
+// A handle owns: three state buffers (A holds the state between steps; B and
+// C are the RK stage results), the generic path's primitive and face-flux
+// buffers (allocated only if that path runs), the device clock (DevTime) with
+// its dt log, a stream, and a CUDA graph holding a fixed number of whole time
+// steps.  Sim::Advance's loop runs on the device: every kernel of a step
+// first reads DevTime::active, which the step epilogue (last CTA of the CFL
+// kernel) clears once the output time, stepmax or an error ends the call.
+// The host launches the graph repeatedly and only looks at `active` between
+// batches, so surplus launches cost one no-op kernel each.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gaukuk_cuda.h"
+#include "gk_internal.h"
+
+namespace {
+
+struct KernelSet {
+    decltype(&gk_parity::launch_bc) bc;
+    decltype(&gk_parity::launch_c2p) c2p;
+    decltype(&gk_parity::launch_flux) flux;
+    decltype(&gk_parity::launch_update) update;
+    decltype(&gk_parity::launch_kick) kick;
+    decltype(&gk_parity::launch_cfl) cfl;
+    decltype(&gk_parity::launch_stage2d) stage2d;
+    decltype(&gk_parity::launch_begin) begin;
+    decltype(&gk_parity::launch_mtz_check) mtz_check;
+};
+
+const KernelSet kParity = {gk_parity::launch_bc,     gk_parity::launch_c2p,
+                           gk_parity::launch_flux,   gk_parity::launch_update,
+                           gk_parity::launch_kick,   gk_parity::launch_cfl,
+                           gk_parity::launch_stage2d, gk_parity::launch_begin,
+                           gk_parity::launch_mtz_check};
+const KernelSet kFast = {gk_fast::launch_bc,     gk_fast::launch_c2p,     gk_fast::launch_flux,
+                         gk_fast::launch_update, gk_fast::launch_kick,    gk_fast::launch_cfl,
+                         gk_fast::launch_stage2d, gk_fast::launch_begin,  gk_fast::launch_mtz_check};
+
+constexpr int kLogCap = 1 << 20;
+
+inline double smin(double a, double b) { return (b < a) ? b : a; }
+
+// Reference var index (DEN,MTX,MTY,MTZ,ENG) -> device slot.
+constexpr int kSlotOf[5] = {gk::S_DEN, gk::S_MTX, gk::S_MTY, gk::S_MTZ, gk::S_ENG};
+
+// Optional per-launch event recording (gk_profile_steps).
+struct Profiler {
+    std::vector<int> cls;
+    std::vector<cudaEvent_t> ev;  // pairs
+};
+
+}  // namespace
+
+struct gk_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    gk_grid_desc gd{};
+    gk_phys_desc pd{};
+    gk::Ctx ctx{};
+    const KernelSet* ks = nullptr;
+    double *A = nullptr, *B = nullptr, *C = nullptr;
+    double *W = nullptr, *F1 = nullptr, *F2 = nullptr, *F3 = nullptr;
+    gk::DevTime* tm = nullptr;
+    gk::DevTime* htm = nullptr;  // pinned mirror
+    double* dlog = nullptr;
+    int* dflag = nullptr;
+    int path = 0;  // 0 generic, 1 fused 2D
+    bool uploaded = false;
+    cudaGraphExec_t gexec = nullptr;
+    int graph_steps = 0;
+    int graph_path = -1;
+    std::string err;
+};
+
+namespace {
+
+int fail(gk_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+#define GK_CUDA(h, call)                                                                    \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail((h), GK_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+long long round_up(long long a, long long b) { return (a + b - 1) / b * b; }
+
+int build_ctx(gk_handle* h) {
+    const gk_grid_desc& gd = h->gd;
+    const gk_phys_desc& pd = h->pd;
+    gk::Geom& g = h->ctx.g;
+    gk::Phys& ph = h->ctx.ph;
+    if (gd.nx <= 0 || gd.ny <= 0 || gd.nz <= 0 || gd.nghost < 0)
+        return fail(h, GK_ERR_INVALID, "Invalid grid parameters from config");
+    if (gd.nghost != 2)
+        return fail(h, GK_ERR_UNSUPPORTED, "the device path is built for NGhost = 2");
+    if ((gd.nx > 1 && gd.nx < gd.nghost) || (gd.ny > 1 && gd.ny < gd.nghost) ||
+        (gd.nz > 1 && gd.nz < gd.nghost))
+        return fail(h, GK_ERR_UNSUPPORTED, "a direction with more than one cell needs at least NGhost cells");
+    if (gd.nx == 1 && (gd.ny > 1 || gd.nz > 1))
+        return fail(h, GK_ERR_UNSUPPORTED, "x must be the first active direction");
+    if (!(pd.gamma > 1.0)) return fail(h, GK_ERR_INVALID, "gamma must exceed 1");
+    if (!(pd.cfl > 0.0)) return fail(h, GK_ERR_INVALID, "CFL must be positive");
+    if (pd.mode != GK_MODE_PARITY && pd.mode != GK_MODE_FAST)
+        return fail(h, GK_ERR_INVALID, "unknown arithmetic mode");
+    g.nx = gd.nx; g.ny = gd.ny; g.nz = gd.nz; g.ng = gd.nghost;
+    g.lenx = g.nx + 2 * g.ng; g.leny = g.ny + 2 * g.ng; g.lenz = g.nz + 2 * g.ng;
+    g.ib = g.ng; g.ie = g.ib + g.nx;
+    g.jb = g.ng; g.je = g.jb + g.ny;
+    g.kb = g.ng; g.ke = g.kb + g.nz;
+    g.ndim = g.nz > 1 ? 3 : (g.ny > 1 ? 2 : 1);
+    g.pitch = (int)round_up(g.lenx, 16);
+    g.nzs = g.nz > 1 ? g.lenz : 1;
+    g.kofs = g.nz > 1 ? 0 : g.kb;
+    g.kstride = (long long)g.pitch * g.leny;
+    g.vstride = g.kstride * g.nzs;
+    g.fpitch = (int)round_up(g.lenx + 1, 16);
+    g.fkstride = (long long)g.fpitch * (g.leny + 1);
+    g.fvstride = g.fkstride * (g.nzs + 1);
+    // Domain (sim.cpp:16-36)
+    g.dx = (gd.xmax - gd.xmin) / gd.nx;
+    g.dy = (gd.ymax - gd.ymin) / gd.ny;
+    g.dz = (gd.zmax - gd.zmin) / gd.nz;
+    g.dxRec = 1. / g.dx;
+    g.dyRec = 1. / g.dy;
+    g.dzRec = 1. / g.dz;
+    if (gd.ny <= 1) g.dyRec = 0;
+    if (gd.nz <= 1) g.dzRec = 0;
+    g.drmin = smin(smin(g.dx, g.dy), g.dz);
+    // EquationOfState (adiabatic.cpp:12-16), hllc.cpp:28-29
+    ph.gamma = pd.gamma;
+    ph.gm1 = pd.gamma - 1.0;
+    ph.gm1Rec = 1.0 / (pd.gamma - 1.0);
+    ph.gmRec = 1.0 / pd.gamma;
+    ph.cq = 0.5 * (1 + ph.gmRec);
+    ph.cfl = pd.cfl;
+    ph.dmin = pd.dfloor;
+    ph.pmin = pd.pfloor;
+    for (int d = 0; d < 3; ++d) ph.grav[d] = pd.grav[d];
+    ph.has_grav = (pd.grav[0] != 0 || pd.grav[1] != 0 || pd.grav[2] != 0);
+    ph.integrator = pd.integrator == 1 ? 1 : (pd.integrator == 3 ? 3 : 2);
+    ph.plm = pd.rc_order != 1;
+    ph.stepmax = pd.stepmax;
+    // Boundary::Boundary (boundary.cpp:13-125): unknown ids copy; type 4 needs
+    // snapshot data this path does not carry.
+    for (int s = 0; s < 6; ++s) {
+        int t = pd.bc[s];
+        if (t == GK_BC_FIXED) return fail(h, GK_ERR_UNSUPPORTED, "fixed (type 4) boundaries are not implemented on the device");
+        if (t < 0 || t > 3) t = 0;
+        ph.bc[s] = t;
+    }
+    ph.fill_z = 0;
+    if (g.ndim == 3) {
+        // z sides of type 0 run OutflowCopyYL/YR after the y fill
+        // (boundary.cpp:92,104,109,121, 127-142): the y ghosts end as copies
+        // and those z ghosts are never filled.
+        for (int side = 0; side < 2; ++side) {
+            if (ph.bc[4 + side] == 0) ph.bc[2 + side] = 0;
+            else ph.fill_z |= 1 << side;
+        }
+    }
+    h->ctx.has_vz = 1;
+    return GK_OK;
+}
+
+int alloc_state(gk_handle* h) {
+    const gk::Geom& g = h->ctx.g;
+    size_t bytes = sizeof(double) * 5 * (size_t)g.vstride;
+    GK_CUDA(h, cudaMalloc(&h->A, bytes));
+    GK_CUDA(h, cudaMalloc(&h->B, bytes));
+    GK_CUDA(h, cudaMemsetAsync(h->A, 0, bytes, h->stream));
+    GK_CUDA(h, cudaMemsetAsync(h->B, 0, bytes, h->stream));
+    if (h->ctx.ph.integrator == 3) {
+        GK_CUDA(h, cudaMalloc(&h->C, bytes));
+        GK_CUDA(h, cudaMemsetAsync(h->C, 0, bytes, h->stream));
+    }
+    GK_CUDA(h, cudaMalloc(&h->tm, sizeof(gk::DevTime)));
+    GK_CUDA(h, cudaMalloc(&h->dlog, sizeof(double) * kLogCap));
+    GK_CUDA(h, cudaMalloc(&h->dflag, sizeof(int)));
+    GK_CUDA(h, cudaMallocHost(&h->htm, sizeof(gk::DevTime)));
+    gk::DevTime t{};
+    t.t = 0; t.dt = 1e10; t.tNext = 0; t.dtUntilOutput = 1e10;  // sim.cpp:45-46
+    t.cmax_last = 1e-16;
+    double seed = 1e-16;
+    std::memcpy(&t.cmax_acc, &seed, sizeof(double));
+    t.done_ctas = 0; t.step = 0; t.is_continue = 1; t.active = 0; t.status = 0;
+    t.steps_left = -1; t.nlog = 0; t.log_cap = kLogCap; t.log = h->dlog;
+    *h->htm = t;
+    GK_CUDA(h, cudaMemcpyAsync(h->tm, h->htm, sizeof(gk::DevTime), cudaMemcpyHostToDevice, h->stream));
+    GK_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->ctx.tm = h->tm;
+    return GK_OK;
+}
+
+int alloc_generic(gk_handle* h) {
+    if (h->W) return GK_OK;
+    const gk::Geom& g = h->ctx.g;
+    size_t sb = sizeof(double) * 5 * (size_t)g.vstride;
+    size_t fb = sizeof(double) * 5 * (size_t)g.fvstride;
+    GK_CUDA(h, cudaMalloc(&h->W, sb));
+    GK_CUDA(h, cudaMalloc(&h->F1, fb));
+    GK_CUDA(h, cudaMalloc(&h->F2, fb));
+    GK_CUDA(h, cudaMalloc(&h->F3, fb));
+    GK_CUDA(h, cudaMemsetAsync(h->W, 0, sb, h->stream));
+    GK_CUDA(h, cudaMemsetAsync(h->F1, 0, fb, h->stream));
+    GK_CUDA(h, cudaMemsetAsync(h->F2, 0, fb, h->stream));
+    GK_CUDA(h, cudaMemsetAsync(h->F3, 0, fb, h->stream));
+    return GK_OK;
+}
+
+// Rows per CTA segment of the fused kernel: enough segments for about four
+// CTAs per SM, at least 8 rows each.
+int stage_rows(const gk::Geom& g) {
+    int strips = (g.nx + 123) / 124;
+    int target = 148 * 4;
+    int segs = std::max(1, (target + strips - 1) / strips);
+    int rows = (g.ny + segs - 1) / segs;
+    return std::max(8, rows);
+}
+
+// One time step.  Kernel order per RK stage follows Sim::RK2_/RK3_/
+// ForwardEuler_ (rk2.cpp:11-23, rk3.cpp:11-29, forward_euler.cpp:11-18),
+// wrapped in the Strang half kicks of sim.cpp:85-91; the step ends with the
+// CFL reduction and epilogue.  The state is in A before and after.
+void enqueue_step(gk_handle* h, Profiler* prof) {
+    const KernelSet& k = *h->ks;
+    const gk::Ctx& c = h->ctx;
+    cudaStream_t s = h->stream;
+    auto mark = [&](int cls) {
+        if (!prof) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, s);
+        prof->cls.push_back(cls);
+        prof->ev.push_back(e);
+    };
+#define GK_L(cls, stmt) \
+    do {                \
+        mark(cls);      \
+        stmt;           \
+        mark(-1);       \
+    } while (0)
+    double* A = h->A;
+    double* B = h->B;
+    double* Cb = h->C;
+    const int integ = c.ph.integrator;
+    const double frac13 = 1.0 / 3.0;
+    if (c.ph.has_grav) GK_L(gk::K_KICK, k.kick(c, A, s));
+    if (h->path == 1) {
+        GK_L(gk::K_BC, k.bc(c, A, s));
+        GK_L(gk::K_STAGE, k.stage2d(c, A, nullptr, B, 0, 1.0, 1.0, 0.0, s));
+        GK_L(gk::K_BC, k.bc(c, B, s));
+        if (integ == 3) {
+            GK_L(gk::K_STAGE, k.stage2d(c, B, A, Cb, 1, 0.75, 0.25, 0.25, s));
+            GK_L(gk::K_BC, k.bc(c, Cb, s));
+            GK_L(gk::K_STAGE, k.stage2d(c, Cb, A, A, 1, frac13, 2 * frac13, 2 * frac13, s));
+        } else {
+            GK_L(gk::K_STAGE, k.stage2d(c, B, A, A, 1, 0.5, 0.5, 0.5, s));
+        }
+    } else {
+        auto fluxes = [&](const double* u) {
+            GK_L(gk::K_C2P, k.c2p(c, u, h->W, s));
+            GK_L(gk::K_FLUX, k.flux(c, 0, h->W, h->F1, s));
+            if (c.g.ndim >= 2) GK_L(gk::K_FLUX, k.flux(c, 1, h->W, h->F2, s));
+            if (c.g.ndim == 3) GK_L(gk::K_FLUX, k.flux(c, 2, h->W, h->F3, s));
+        };
+        GK_L(gk::K_BC, k.bc(c, A, s));
+        fluxes(A);
+        if (integ == 1) {
+            GK_L(gk::K_UPDATE, k.update(c, nullptr, A, A, h->F1, h->F2, h->F3, 0, 1.0, 1.0, 0.0, s));
+        } else {
+            GK_L(gk::K_UPDATE, k.update(c, nullptr, A, B, h->F1, h->F2, h->F3, 0, 1.0, 1.0, 0.0, s));
+            GK_L(gk::K_BC, k.bc(c, B, s));
+            fluxes(B);
+            if (integ == 3) {
+                GK_L(gk::K_UPDATE, k.update(c, A, B, B, h->F1, h->F2, h->F3, 1, 0.75, 0.25, 0.25, s));
+                GK_L(gk::K_BC, k.bc(c, B, s));
+                fluxes(B);
+                GK_L(gk::K_UPDATE, k.update(c, A, B, A, h->F1, h->F2, h->F3, 1, frac13, 2 * frac13,
+                                            2 * frac13, s));
+            } else {
+                GK_L(gk::K_UPDATE, k.update(c, A, B, A, h->F1, h->F2, h->F3, 1, 0.5, 0.5, 0.5, s));
+            }
+        }
+    }
+    if (c.ph.has_grav) GK_L(gk::K_KICK, k.kick(c, A, s));
+    GK_L(gk::K_CFL, k.cfl(c, A, 1, s));
+#undef GK_L
+}
+
+int steps_per_graph_of(const gk::Geom& g) {
+    long long cells = (long long)g.nx * g.ny * g.nz;
+    if (cells >= (1LL << 22)) return 2;
+    if (cells >= (1LL << 18)) return 8;
+    return 32;
+}
+
+int ensure_graph(gk_handle* h) {
+    if (h->gexec && h->graph_path == h->path) return GK_OK;
+    if (h->gexec) {
+        cudaGraphExecDestroy(h->gexec);
+        h->gexec = nullptr;
+    }
+    h->graph_steps = steps_per_graph_of(h->ctx.g);
+    cudaGraph_t graph;
+    GK_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < h->graph_steps; ++i) enqueue_step(h, nullptr);
+    GK_CUDA(h, cudaStreamEndCapture(h->stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(&h->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(h, GK_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    h->graph_path = h->path;
+    return GK_OK;
+}
+
+int pull_time(gk_handle* h) {
+    GK_CUDA(h, cudaMemcpyAsync(h->htm, h->tm, sizeof(gk::DevTime), cudaMemcpyDeviceToHost, h->stream));
+    GK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return GK_OK;
+}
+
+int check_ready(gk_handle* h) {
+    if (!h) return GK_ERR_INVALID;
+    if (!h->uploaded) return fail(h, GK_ERR_STATE, "no state uploaded");
+    GK_CUDA(h, cudaSetDevice(h->device));
+    return GK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gk_create(const gk_grid_desc* grid, const gk_phys_desc* phys, gk_handle** out) {
+    if (!grid || !phys || !out) return GK_ERR_INVALID;
+    *out = nullptr;
+    gk_handle* h = new gk_handle();
+    h->gd = *grid;
+    h->pd = *phys;
+    h->device = phys->device;
+    int rc = build_ctx(h);
+    if (rc != GK_OK) {
+        std::fprintf(stderr, "gk_create: %s\n", h->err.c_str());
+        delete h;
+        return rc;
+    }
+    h->ks = phys->mode == GK_MODE_FAST ? &kFast : &kParity;
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "gk_create: %s\n", cudaGetErrorString(e));
+        delete h;
+        return GK_ERR_CUDA;
+    }
+    rc = alloc_state(h);
+    if (rc != GK_OK) {
+        std::fprintf(stderr, "gk_create: %s\n", h->err.c_str());
+        gk_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return GK_OK;
+}
+
+void gk_destroy(gk_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    for (double* p : {h->A, h->B, h->C, h->W, h->F1, h->F2, h->F3, h->dlog}) cudaFree(p);
+    cudaFree(h->tm);
+    cudaFree(h->dflag);
+    if (h->htm) cudaFreeHost(h->htm);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+long long gk_state_size(const gk_handle* h) {
+    if (!h) return 0;
+    const gk::Geom& g = h->ctx.g;
+    return 5LL * g.lenz * g.leny * g.lenx;
+}
+
+int gk_upload_cons(gk_handle* h, const double* cons) {
+    if (!h || !cons) return GK_ERR_INVALID;
+    GK_CUDA(h, cudaSetDevice(h->device));
+    const gk::Geom& g = h->ctx.g;
+    for (int n = 0; n < 5; ++n) {
+        for (int kk = 0; kk < g.nzs; ++kk) {
+            const int k = g.kofs + kk;
+            const double* src = cons + ((size_t)(n * g.lenz + k) * g.leny) * g.lenx;
+            double* dst = h->A + (size_t)kSlotOf[n] * g.vstride + (size_t)kk * g.kstride;
+            GK_CUDA(h, cudaMemcpy2DAsync(dst, sizeof(double) * g.pitch, src, sizeof(double) * g.lenx,
+                                         sizeof(double) * g.lenx, g.leny, cudaMemcpyHostToDevice,
+                                         h->stream));
+        }
+    }
+    // Path: the fused kernel evolves four variables; it applies when the run
+    // is 2D and MTZ is zero on every active cell (it then stays zero).
+    h->ctx.has_vz = 1;
+    if (g.ndim <= 2) {
+        GK_CUDA(h, cudaMemsetAsync(h->dflag, 0, sizeof(int), h->stream));
+        h->ks->mtz_check(h->ctx, h->A, h->dflag, h->stream);
+        int flag = 0;
+        GK_CUDA(h, cudaMemcpyAsync(&flag, h->dflag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        GK_CUDA(h, cudaStreamSynchronize(h->stream));
+        h->ctx.has_vz = flag;
+    }
+    h->path = (g.ndim == 2 && !h->ctx.has_vz && h->ctx.ph.integrator != 1) ? 1 : 0;
+    h->ctx.h2d_rows = stage_rows(g);
+    if (h->path == 0) {
+        int rc = alloc_generic(h);
+        if (rc != GK_OK) return rc;
+    }
+    // reset the step machinery; the clock (t, step, isContinue) is kept
+    int rc = pull_time(h);
+    if (rc != GK_OK) return rc;
+    gk::DevTime t = *h->htm;
+    double seed = 1e-16;
+    std::memcpy(&t.cmax_acc, &seed, sizeof(double));
+    t.done_ctas = 0;
+    t.status = 0;
+    t.nlog = 0;
+    t.active = 0;
+    *h->htm = t;
+    GK_CUDA(h, cudaMemcpyAsync(h->tm, h->htm, sizeof(gk::DevTime), cudaMemcpyHostToDevice, h->stream));
+    h->ks->cfl(h->ctx, h->A, 0, h->stream);
+    GK_CUDA(h, cudaGetLastError());
+    rc = pull_time(h);
+    if (rc != GK_OK) return rc;
+    h->uploaded = true;
+    if (h->htm->status) return fail(h, GK_ERR_NONFINITE, "non-finite state in the uploaded array");
+    return GK_OK;
+}
+
+static int download(gk_handle* h, double* cons, bool zero_other_planes) {
+    int rc = check_ready(h);
+    if (rc != GK_OK) return rc;
+    if (!cons) return GK_ERR_INVALID;
+    const gk::Geom& g = h->ctx.g;
+    for (int n = 0; n < 5; ++n) {
+        for (int kk = 0; kk < g.nzs; ++kk) {
+            const int k = g.kofs + kk;
+            double* dst = cons + ((size_t)(n * g.lenz + k) * g.leny) * g.lenx;
+            const double* src = h->A + (size_t)kSlotOf[n] * g.vstride + (size_t)kk * g.kstride;
+            GK_CUDA(h, cudaMemcpy2DAsync(dst, sizeof(double) * g.lenx, src, sizeof(double) * g.pitch,
+                                         sizeof(double) * g.lenx, g.leny, cudaMemcpyDeviceToHost,
+                                         h->stream));
+        }
+    }
+    if (g.nzs == 1 && zero_other_planes) {
+        const size_t plane = (size_t)g.leny * g.lenx;
+        for (int n = 0; n < 5; ++n)
+            for (int k = 0; k < g.lenz; ++k)
+                if (k != g.kofs) std::memset(cons + (size_t)(n * g.lenz + k) * plane, 0, plane * sizeof(double));
+    }
+    GK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return GK_OK;
+}
+
+int gk_download_cons(gk_handle* h, double* cons) { return download(h, cons, true); }
+int gk_download_planes(gk_handle* h, double* cons) { return download(h, cons, false); }
+
+static int run_loop(gk_handle* h, double dtoutput, int nsteps, bool wait) {
+    int rc = ensure_graph(h);
+    if (rc != GK_OK) return rc;
+    h->ks->begin(h->ctx, dtoutput, nsteps, h->stream);
+    GK_CUDA(h, cudaGetLastError());
+    if (nsteps > 0) {
+        int launches = (nsteps + h->graph_steps - 1) / h->graph_steps;
+        for (int i = 0; i < launches; ++i) GK_CUDA(h, cudaGraphLaunch(h->gexec, h->stream));
+        if (!wait) return GK_OK;
+        return pull_time(h);
+    }
+    int batch = 1;
+    for (;;) {
+        for (int i = 0; i < batch; ++i) GK_CUDA(h, cudaGraphLaunch(h->gexec, h->stream));
+        GK_CUDA(h, cudaMemcpyAsync(&h->htm->active, &h->tm->active, sizeof(int),
+                                   cudaMemcpyDeviceToHost, h->stream));
+        GK_CUDA(h, cudaStreamSynchronize(h->stream));
+        if (!h->htm->active) break;
+        batch = std::min(batch * 2, 64);
+    }
+    return pull_time(h);
+}
+
+int gk_advance(gk_handle* h, double dtoutput, double* t, int* step, int* is_continue) {
+    int rc = check_ready(h);
+    if (rc != GK_OK) return rc;
+    rc = run_loop(h, dtoutput, 0, true);
+    if (rc != GK_OK) return rc;
+    if (t) *t = h->htm->t;
+    if (step) *step = h->htm->step;
+    if (is_continue) *is_continue = h->htm->is_continue;
+    if (h->htm->status) return fail(h, GK_ERR_NONFINITE, "CFL reduction met a non-finite state");
+    return GK_OK;
+}
+
+int gk_run_steps(gk_handle* h, int nsteps, int* done) {
+    int rc = check_ready(h);
+    if (rc != GK_OK) return rc;
+    if (nsteps <= 0) {
+        if (done) *done = 0;
+        return GK_OK;
+    }
+    rc = pull_time(h);
+    if (rc != GK_OK) return rc;
+    const int before = h->htm->step;
+    rc = run_loop(h, 0.0, nsteps, true);
+    if (rc != GK_OK) return rc;
+    if (done) *done = h->htm->step - before;
+    if (h->htm->status) return fail(h, GK_ERR_NONFINITE, "CFL reduction met a non-finite state");
+    return GK_OK;
+}
+
+int gk_enqueue_steps(gk_handle* h, int nsteps) {
+    int rc = check_ready(h);
+    if (rc != GK_OK) return rc;
+    if (nsteps <= 0) return GK_OK;
+    return run_loop(h, 0.0, nsteps, false);
+}
+
+int gk_get_time(gk_handle* h, double* t, double* dt, int* step, int* is_continue) {
+    if (!h) return GK_ERR_INVALID;
+    GK_CUDA(h, cudaSetDevice(h->device));
+    int rc = pull_time(h);
+    if (rc != GK_OK) return rc;
+    if (t) *t = h->htm->t;
+    if (dt) *dt = h->htm->dt;
+    if (step) *step = h->htm->step;
+    if (is_continue) *is_continue = h->htm->is_continue;
+    return GK_OK;
+}
+
+int gk_set_time(gk_handle* h, double t, int step) {
+    if (!h) return GK_ERR_INVALID;
+    GK_CUDA(h, cudaSetDevice(h->device));
+    int rc = pull_time(h);
+    if (rc != GK_OK) return rc;
+    h->htm->t = t;
+    h->htm->step = step;
+    h->htm->is_continue = !(h->ctx.ph.stepmax > 0 && step >= h->ctx.ph.stepmax);
+    GK_CUDA(h, cudaMemcpyAsync(h->tm, h->htm, sizeof(gk::DevTime), cudaMemcpyHostToDevice, h->stream));
+    GK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return GK_OK;
+}
+
+int gk_dt_log(gk_handle* h, double* buf, int cap, int* n) {
+    if (!h) return GK_ERR_INVALID;
+    GK_CUDA(h, cudaSetDevice(h->device));
+    int rc = pull_time(h);
+    if (rc != GK_OK) return rc;
+    int total = h->htm->nlog;
+    int avail = std::min(total, kLogCap);
+    int m = std::min(avail, cap);
+    if (buf && m > 0)
+        GK_CUDA(h, cudaMemcpy(buf, h->dlog, sizeof(double) * m, cudaMemcpyDeviceToHost));
+    if (n) *n = total;
+    return GK_OK;
+}
+
+int gk_cmax(gk_handle* h, double* cmax) {
+    int rc = check_ready(h);
+    if (rc != GK_OK) return rc;
+    h->ks->cfl(h->ctx, h->A, 0, h->stream);
+    GK_CUDA(h, cudaGetLastError());
+    rc = pull_time(h);
+    if (rc != GK_OK) return rc;
+    if (cmax) *cmax = h->htm->cmax_last;
+    return GK_OK;
+}
+
+int gk_stream(gk_handle* h, void** stream) {
+    if (!h || !stream) return GK_ERR_INVALID;
+    *stream = (void*)h->stream;
+    return GK_OK;
+}
+
+int gk_path(gk_handle* h, int* path) {
+    if (!h || !path) return GK_ERR_INVALID;
+    *path = h->path;
+    return GK_OK;
+}
+
+int gk_graph_info(gk_handle* h, int* steps_per_graph, int* launches_per_step) {
+    if (!h) return GK_ERR_INVALID;
+    const gk::Ctx& c = h->ctx;
+    const int stages = c.ph.integrator;  // 1, 2 or 3 stages
+    int per = c.ph.has_grav ? 2 : 0;
+    if (h->path == 1) per += 2 * stages;
+    else per += stages * (3 + c.g.ndim);
+    per += 1;  // CFL + epilogue
+    if (steps_per_graph) *steps_per_graph = steps_per_graph_of(c.g);
+    if (launches_per_step) *launches_per_step = per;
+    return GK_OK;
+}
+
+int gk_profile_steps(gk_handle* h, int nsteps, char* names, int names_cap, double* total_ms,
+                     int* launches, int cap, int* n) {
+    int rc = check_ready(h);
+    if (rc != GK_OK) return rc;
+    h->ks->begin(h->ctx, 0.0, nsteps, h->stream);
+    Profiler prof;
+    for (int i = 0; i < nsteps; ++i) enqueue_step(h, &prof);
+    GK_CUDA(h, cudaStreamSynchronize(h->stream));
+    std::vector<double> ms(gk::K_NCLASS, 0.0);
+    std::vector<int> cnt(gk::K_NCLASS, 0);
+    for (size_t i = 0; i + 1 < prof.ev.size(); i += 2) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, prof.ev[i], prof.ev[i + 1]);
+        ms[prof.cls[i]] += t;
+        cnt[prof.cls[i]] += 1;
+    }
+    for (cudaEvent_t e : prof.ev) cudaEventDestroy(e);
+    std::string nm;
+    int m = 0;
+    for (int c = 0; c < gk::K_NCLASS; ++c) {
+        if (!cnt[c]) continue;
+        if (m < cap) {
+            if (total_ms) total_ms[m] = ms[c];
+            if (launches) launches[m] = cnt[c];
+        }
+        nm += (m ? ";" : "");
+        nm += gk::kClassNames[c];
+        ++m;
+    }
+    if (names && names_cap > 0) {
+        std::strncpy(names, nm.c_str(), names_cap - 1);
+        names[names_cap - 1] = 0;
+    }
+    if (n) *n = m;
+    return pull_time(h);
+}
+
+const char* gk_strerror(int status) {
+    switch (status) {
+        case GK_OK: return "ok";
+        case GK_ERR_INVALID: return "invalid argument or configuration";
+        case GK_ERR_CUDA: return "CUDA runtime error";
+        case GK_ERR_NONFINITE: return "non-finite state in the CFL reduction";
+        case GK_ERR_UNSUPPORTED: return "configuration not supported by the device path";
+        case GK_ERR_STATE: return "call out of order";
+        default: return "unknown status";
+    }
+}
+
+const char* gk_last_error(const gk_handle* h) { return h ? h->err.c_str() : ""; }
+
+}  // extern "C"

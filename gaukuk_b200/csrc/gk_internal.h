@@ -1,0 +1,103 @@
+// gk_internal.h -- types shared by the C-ABI layer and the kernel units.
+//
+// Device state layout (one allocation per state buffer): five variable
+// planes in slot order DEN, MTX, MTY, ENG, MTZ, so that the four variables a
+// 2D run evolves are contiguous and MTZ is last.  Each plane holds `nzs`
+// z-planes (1 in 1D/2D, lenz in 3D) of `leny` rows with a row pitch of
+// `pitch` doubles (lenx rounded up to 16 doubles = 128 bytes).  Column i and
+// row j are the reference's own indices (ghosts at 0..nghost-1), so ghost
+// fills and face indices read exactly like the reference loops.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace gk {
+
+// Device variable slots.
+enum Slot { S_DEN = 0, S_MTX = 1, S_MTY = 2, S_ENG = 3, S_MTZ = 4 };
+// Primitive slots use the same positions: rho, vx, vy, p, vz.
+enum PSlot { P_RHO = 0, P_VX = 1, P_VY = 2, P_PRE = 3, P_VZ = 4 };
+
+struct Geom {
+    int nx, ny, nz, ng;
+    int lenx, leny, lenz;
+    int ib, ie, jb, je, kb, ke;
+    int ndim;            // 1, 2 or 3
+    int pitch;           // doubles per row
+    int nzs;             // stored z-planes
+    int kofs;            // reference k of stored plane 0
+    long long kstride;   // doubles per stored z-plane (pitch*leny)
+    long long vstride;   // doubles per variable slot (kstride*nzs)
+    // face arrays (generic path): rows leny+1, planes nzs+1
+    int fpitch;
+    long long fkstride, fvstride;
+    double dx, dy, dz, dxRec, dyRec, dzRec, drmin;
+};
+
+struct Phys {
+    double gamma, gm1, gm1Rec, gmRec, cq;  // cq = 0.5*(1+1/gamma) (hllc.cpp:55-58)
+    double cfl, dmin, pmin;
+    double grav[3];
+    int has_grav;
+    int integrator;   // 1, 2, 3
+    int plm;          // 1 = PLM, 0 = first order
+    int bc[6];        // effective ghost-fill type per side (after the z->y copy mapping)
+    int fill_z;       // 3D only: whether z sides are filled (per side bit 0/1)
+    int stepmax;
+};
+
+// Device-resident clock of Sim::Advance (sim.cpp:69-117).  Written by the
+// step epilogue (the last CTA of the CFL kernel) and by the begin kernel.
+struct DevTime {
+    double t, dt, tNext, dtUntilOutput;
+    double cmax_last;                 // CalCmax of the current state
+    unsigned long long cmax_acc;      // running max (bit pattern; values >= 0)
+    unsigned int done_ctas;           // last-CTA detection counter
+    int step;
+    int is_continue;                  // Sim::isContinue
+    int active;                       // the loop condition of the running call
+    int status;                       // error bits (STATUS_*)
+    int steps_left;                   // step budget (-1 = none)
+    int nlog, log_cap;
+    double* log;                      // dt of each step
+};
+
+enum { STATUS_NONFINITE = 1 };
+
+struct Ctx {
+    Geom g;
+    Phys ph;
+    DevTime* tm;
+    int has_vz;      // 2D: MTZ not identically zero -> generic path
+    int h2d_rows;    // fused 2D kernel: rows per CTA segment
+};
+
+// Kernel classes, for per-kernel profiling.
+enum KClass { K_BC = 0, K_C2P, K_FLUX, K_UPDATE, K_KICK, K_CFL, K_STAGE, K_BEGIN, K_NCLASS };
+static const char* const kClassNames[K_NCLASS] = {
+    "ghost_fill", "cons_to_prim", "flux", "update", "gravity_kick", "cfl_reduce",
+    "stage2d", "begin"};
+
+}  // namespace gk
+
+// One set of launchers per arithmetic mode (gk_kernels_parity.cu,
+// gk_kernels_fast.cu).  Same signatures, different namespaces.
+#define GK_DECLARE_KERNEL_SET(NS)                                                              \
+    namespace NS {                                                                             \
+    void launch_bc(const gk::Ctx& c, double* u, cudaStream_t s);                               \
+    void launch_c2p(const gk::Ctx& c, const double* u, double* prim, cudaStream_t s);          \
+    void launch_flux(const gk::Ctx& c, int dir, const double* prim, double* F, cudaStream_t s); \
+    void launch_update(const gk::Ctx& c, const double* u0, const double* uc, double* out,      \
+                       const double* F1, const double* F2, const double* F3, int three,        \
+                       double c1, double c2, double c3, cudaStream_t s);                       \
+    void launch_kick(const gk::Ctx& c, double* u, cudaStream_t s);                             \
+    void launch_cfl(const gk::Ctx& c, const double* u, int epilogue, cudaStream_t s);          \
+    void launch_stage2d(const gk::Ctx& c, const double* uc, const double* u0, double* out,     \
+                        int three, double c1, double c2, double c3, cudaStream_t s);           \
+    void launch_begin(const gk::Ctx& c, double dtoutput, int steps, cudaStream_t s);           \
+    void launch_mtz_check(const gk::Ctx& c, const double* u, int* flag, cudaStream_t s);       \
+    }
+
+GK_DECLARE_KERNEL_SET(gk_parity)
+GK_DECLARE_KERNEL_SET(gk_fast)

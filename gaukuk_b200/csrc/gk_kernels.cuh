@@ -1,0 +1,659 @@
+// gk_kernels.cuh -- the device kernels of one arithmetic mode.
+//
+// Included by gk_kernels_parity.cu (GK_NS = gk_parity, GK_SEL = false,
+// compiled with -fmad=false) and gk_kernels_fast.cu (GK_NS = gk_fast,
+// GK_SEL = true, FMA contraction allowed).
+//
+// Two implementations of one RK stage share the pointwise physics:
+//   * the generic path, one kernel per reference phase (ghost fill,
+//     ConsToPrim, one flux sweep per direction, UpdateCons), any dimension,
+//     five variables;
+//   * the fused 2D stage kernel (k_stage2d), which for a 2D run with vz = 0
+//     does ConsToPrim + PLM + HLLC in x and y + flux divergence + RK combine
+//     + floors in one pass, marching up columns.
+// Both end each step in k_cfl, whose last CTA runs the step epilogue of
+// Sim::Advance on the device clock (DevTime).
+#pragma once
+
+#include <cfloat>
+#include <cstdio>
+#include <math_constants.h>
+
+#include "gk_internal.h"
+
+#ifndef GK_NS
+#error "define GK_NS"
+#endif
+
+namespace GK_NS {
+
+#include "gk_physics.cuh"
+
+using gk::Ctx;
+using gk::DevTime;
+using gk::Geom;
+using gk::Phys;
+
+constexpr bool kSel = GK_SEL;
+
+__device__ __forceinline__ long long sidx(const Geom& g, int k, int j, int i) {
+    return (long long)(k - g.kofs) * g.kstride + (long long)j * g.pitch + i;
+}
+__device__ __forceinline__ long long fidx(const Geom& g, int k, int j, int i) {
+    return (long long)(k - g.kofs) * g.fkstride + (long long)j * g.fpitch + i;
+}
+
+// ---------------------------------------------------------------- ghost fill
+// Boundary::UpdateBD (boundary.cpp:127-142) with the routines of
+// boundary/{outflow_copy,periodic,reflective,outflow}.cpp.  Ghosts of active
+// rows/columns only; corners untouched.  With n >= nghost in every filled
+// direction each ghost depends on one active cell, so all sides fill in one
+// launch.  blockIdx.y = 2*dir + side.
+__global__ void k_bc(double* __restrict__ u, Geom g, Phys ph, const DevTime* __restrict__ tm) {
+    if (!tm->active) return;
+    const int dir = blockIdx.y >> 1, side = blockIdx.y & 1;
+    const int n3[3] = {g.nx, g.ny, g.nz};
+    if (n3[dir] <= 1) return;
+    if (dir == 2 && !((ph.fill_z >> side) & 1)) return;
+    const int type = ph.bc[blockIdx.y];
+    // transverse extents (active), ghost layers along dir
+    const int ta = dir == 0 ? g.ny : g.nx;
+    const int tb = dir == 2 ? g.ny : g.nz;
+    const long long count = (long long)g.ng * ta * tb;
+    long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= count) return;
+    const int gi = (int)(id % g.ng);
+    const long long r = id / g.ng;
+    const int a = (int)(r % ta), b = (int)(r / ta);
+    const int e = g.ng + n3[dir];
+    const int gc = side == 0 ? gi : e + gi;  // ghost coordinate along dir
+    int sc;                                  // source coordinate along dir
+    if (type == 1) sc = side == 0 ? gc + n3[dir] : gc - n3[dir];
+    else if (type == 0) sc = side == 0 ? g.ng : e - 1;
+    else sc = side == 0 ? (g.ng + g.ng - gc - 1) : (e + e - gc - 1);
+    int ci, cj, ck, si, sj, sk;
+    if (dir == 0) { ci = gc; si = sc; cj = sj = g.jb + a; ck = sk = g.kb + b; }
+    else if (dir == 1) { cj = gc; sj = sc; ci = si = g.ib + a; ck = sk = g.kb + b; }
+    else { ck = gc; sk = sc; ci = si = g.ib + a; cj = sj = g.jb + b; }
+    const long long dst = sidx(g, ck, cj, ci), src = sidx(g, sk, sj, si);
+    double q[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) q[v] = u[v * g.vstride + src];
+    const int mom = dir == 0 ? gk::S_MTX : (dir == 1 ? gk::S_MTY : gk::S_MTZ);
+    if (type == 2) {
+        q[mom] = -q[mom];
+    } else if (type == 3) {
+        // outflow.cpp:36-60: clamp inflow momentum, floor e_int at 1e-16.
+        double mt = q[mom];
+        double mc = side == 0 ? smin(mt, 0.0) : smax(mt, 0.0);
+        double rho = smax(q[gk::S_DEN], ph.dmin);
+        double rhoInv = 1.0 / rho;
+        double keOld = 0.5 * rhoInv * mt * mt;
+        double keNew = 0.5 * rhoInv * mc * mc;
+        double eint = q[gk::S_ENG] - keOld;
+        eint = smax(eint, 1e-16);
+        q[gk::S_DEN] = rho;
+        q[mom] = mc;
+        q[gk::S_ENG] = eint + keNew;
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) u[v * g.vstride + dst] = q[v];
+}
+
+// ------------------------------------------------------------ ConsToPrim
+// EquationOfState::ConsToPrim (adiabatic.cpp:18-61) over every stored cell.
+__device__ __forceinline__ void cons_to_prim5(double d, double mx, double my, double mz, double e,
+                                              const Phys& ph, double w[5]) {
+    d = smax(d, ph.dmin);
+    w[gk::P_RHO] = d;
+    double denInv = 1.0 / d;
+    w[gk::P_VX] = mx * denInv;
+    w[gk::P_VY] = my * denInv;
+    w[gk::P_VZ] = mz * denInv;
+    double engKin = 0.5 * denInv * (mx * mx + my * my + mz * mz);
+    double pre = ph.gm1 * (e - engKin);
+    w[gk::P_PRE] = (pre > ph.pmin) ? pre : ph.pmin;
+}
+
+__global__ void k_c2p(const double* __restrict__ u, double* __restrict__ w, Geom g, Phys ph,
+                      const DevTime* __restrict__ tm) {
+    if (!tm->active) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int k = g.kofs + blockIdx.z;
+    if (i >= g.lenx) return;
+    const long long c = sidx(g, k, j, i);
+    double q[5];
+    cons_to_prim5(u[gk::S_DEN * g.vstride + c], u[gk::S_MTX * g.vstride + c],
+                  u[gk::S_MTY * g.vstride + c], u[gk::S_MTZ * g.vstride + c],
+                  u[gk::S_ENG * g.vstride + c], ph, q);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) w[v * g.vstride + c] = q[v];
+}
+
+// ------------------------------------------------------------ flux sweeps
+// Flux::CalFlux (cal_flux.cpp:13-160): faces ib..ie along the sweep, active
+// in the other directions.  dir 0 = x (flx1), 1 = y (flx2), 2 = z (flx3).
+// For z the reference forms the face states with ReconstructYZPLM, whose
+// slope is along y (recon_piecewise_linear.cpp:29-50); that is kept.
+__global__ void k_flux(const double* __restrict__ w, double* __restrict__ F, Geom g, Phys ph,
+                       int dir, const DevTime* __restrict__ tm) {
+    if (!tm->active) return;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int bidx = blockIdx.y, cidx = blockIdx.z;
+    int i, j, k;
+    if (dir == 0) { i = g.ib + a; j = g.jb + bidx; k = g.kb + cidx; if (i > g.ie) return; }
+    else if (dir == 1) { i = g.ib + a; j = g.jb + bidx; k = g.kb + cidx; if (i >= g.ie) return; }
+    else { i = g.ib + a; j = g.jb + bidx; k = g.kb + cidx; if (i >= g.ie) return; }
+    // cells m (left of the face) and p (right); stencil offsets
+    double wl[5], wr[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        double l1, l2, l3, r1, r2, r3;
+        const double* p = w + v * g.vstride;
+        if (dir == 0) {
+            l1 = p[sidx(g, k, j, i - 2)]; l2 = p[sidx(g, k, j, i - 1)]; l3 = p[sidx(g, k, j, i)];
+            r1 = l2; r2 = l3; r3 = p[sidx(g, k, j, i + 1)];
+        } else if (dir == 1) {
+            l1 = p[sidx(g, k, j - 2, i)]; l2 = p[sidx(g, k, j - 1, i)]; l3 = p[sidx(g, k, j, i)];
+            r1 = l2; r2 = l3; r3 = p[sidx(g, k, j + 1, i)];
+        } else {
+            l1 = p[sidx(g, k - 1, j - 1, i)]; l2 = p[sidx(g, k - 1, j, i)];
+            l3 = p[sidx(g, k - 1, j + 1, i)];
+            r1 = p[sidx(g, k, j - 1, i)]; r2 = p[sidx(g, k, j, i)]; r3 = p[sidx(g, k, j + 1, i)];
+        }
+        if (ph.plm) {
+            wl[v] = l2 + 0.5 * vanleer(l2 - l1, l3 - l2);
+            wr[v] = r2 - 0.5 * vanleer(r2 - r1, r3 - r2);
+        } else {
+            wl[v] = l2;
+            wr[v] = r2;
+        }
+    }
+    // rotation (hllc.cpp:25-27): x (vx | vy, vz), y (vy | vz, vx), z (vz | vx, vy)
+    const int sn = dir == 0 ? gk::P_VX : (dir == 1 ? gk::P_VY : gk::P_VZ);
+    const int s1 = dir == 0 ? gk::P_VY : (dir == 1 ? gk::P_VZ : gk::P_VX);
+    const int s2 = dir == 0 ? gk::P_VZ : (dir == 1 ? gk::P_VX : gk::P_VY);
+    Flux5 f;
+    hllc<true, kSel>(wl[gk::P_RHO], wl[sn], wl[s1], wl[s2], wl[gk::P_PRE], wr[gk::P_RHO], wr[sn],
+                     wr[s1], wr[s2], wr[gk::P_PRE], ph, f);
+    // momentum slots of the rotated components (slot ids equal prim ids)
+    const long long c = fidx(g, k, j, i);
+    F[gk::S_DEN * g.fvstride + c] = f.d;
+    F[sn * g.fvstride + c] = f.n;
+    F[s1 * g.fvstride + c] = f.t1;
+    F[s2 * g.fvstride + c] = f.t2;
+    F[gk::S_ENG * g.fvstride + c] = f.e;
+}
+
+// ------------------------------------------------------------ UpdateCons
+// Sim::UpdateCons, both overloads (update_cons.cpp:11-133, 135-269).
+// update_cons.cpp:55-68, five slots (DEN, MTX, MTY, ENG, MTZ).
+__device__ __forceinline__ void floors5(double (&r)[5], const Phys& ph) {
+    if (r[gk::S_DEN] < ph.dmin) {
+        r[gk::S_DEN] = ph.dmin;
+        r[gk::S_MTX] = 0.0;
+        r[gk::S_MTY] = 0.0;
+        r[gk::S_MTZ] = 0.0;
+        r[gk::S_ENG] = ph.pmin / ph.gm1 + 0.0;
+    } else {
+        double inv_den = 1.0 / r[gk::S_DEN];
+        double ke = 0.5 * inv_den *
+                    (r[gk::S_MTX] * r[gk::S_MTX] + r[gk::S_MTY] * r[gk::S_MTY] +
+                     r[gk::S_MTZ] * r[gk::S_MTZ]);
+        double press = ph.gm1 * (r[gk::S_ENG] - ke);
+        if (press < ph.pmin) r[gk::S_ENG] = ph.pmin / ph.gm1 + ke;
+    }
+}
+
+// The same with mz = 0 (four slots DEN, MTX, MTY, ENG): the mz terms are
+// exact zeros.
+__device__ __forceinline__ void floors4(double (&r)[4], const Phys& ph) {
+    if (r[0] < ph.dmin) {
+        r[0] = ph.dmin;
+        r[1] = 0.0;
+        r[2] = 0.0;
+        r[3] = ph.pmin / ph.gm1 + 0.0;
+    } else {
+        double inv_den = 1.0 / r[0];
+        double ke = 0.5 * inv_den * (r[1] * r[1] + r[2] * r[2]);
+        double press = ph.gm1 * (r[3] - ke);
+        if (press < ph.pmin) r[3] = ph.pmin / ph.gm1 + ke;
+    }
+}
+
+__global__ void k_update(const double* u0, const double* uc, double* out,
+                         const double* __restrict__ F1, const double* __restrict__ F2,
+                         const double* __restrict__ F3, Geom g, Phys ph, int three, double c1,
+                         double c2, double c3, const DevTime* __restrict__ tm) {
+    if (!tm->active) return;
+    const int i = g.ib + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = g.jb + blockIdx.y;
+    const int k = g.kb + blockIdx.z;
+    if (i >= g.ie) return;
+    const double dt = tm->dt;
+    const double dtdx = dt * g.dxRec, dtdy = dt * g.dyRec, dtdz = dt * g.dzRec;
+    const long long c = sidx(g, k, j, i);
+    const long long fc = fidx(g, k, j, i);
+    double r[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        double dF = (F1[v * g.fvstride + fc + 1] - F1[v * g.fvstride + fc]) * dtdx;
+        if (g.ndim == 2) {
+            dF = dF + (F2[v * g.fvstride + fc + g.fpitch] - F2[v * g.fvstride + fc]) * dtdy;
+        } else if (g.ndim == 3) {
+            dF = dF + (F2[v * g.fvstride + fc + g.fpitch] - F2[v * g.fvstride + fc]) * dtdy +
+                 (F3[v * g.fvstride + fc + g.fkstride] - F3[v * g.fvstride + fc]) * dtdz;
+        }
+        if (three) r[v] = c1 * u0[v * g.vstride + c] + c2 * uc[v * g.vstride + c] - c3 * dF;
+        else r[v] = c1 * uc[v * g.vstride + c] - c2 * dF;
+    }
+    floors5(r, ph);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) out[v * g.vstride + c] = r[v];
+}
+
+// ------------------------------------------------------------ gravity kick
+// SourceTerm::ConstGravity (const_gravity.cpp:10-69) with dt/2, applied
+// before and after the integrator (sim.cpp:85-91): E += m*g*dt; m += rho*g*dt.
+__global__ void k_kick(double* __restrict__ u, Geom g, Phys ph, const DevTime* __restrict__ tm) {
+    if (!tm->active) return;
+    const int i = g.ib + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = g.jb + blockIdx.y;
+    const int k = g.kb + blockIdx.z;
+    if (i >= g.ie) return;
+    const double hdt = 0.5 * tm->dt;
+    const long long c = sidx(g, k, j, i);
+    const int moms[3] = {gk::S_MTX, gk::S_MTY, gk::S_MTZ};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double gd = ph.grav[d];
+        if (gd == 0) continue;
+        double& E = u[gk::S_ENG * g.vstride + c];
+        double& m = u[moms[d] * g.vstride + c];
+        E += m * gd * hdt;
+        m += u[gk::S_DEN * g.vstride + c] * gd * hdt;
+    }
+}
+
+// ------------------------------------------------------------ CFL + epilogue
+// EquationOfState::CalCmax (adiabatic.cpp:115-160) on the active cells,
+// reduced in registers -> warp shuffles -> shared memory -> one atomicMax per
+// CTA on the bit pattern (non-negative doubles order like their bits; NaN
+// and inf sort above every finite value, so they reach the check below).
+// With epilogue = 1 the last CTA to finish runs the tail of the Sim::Advance
+// loop body (sim.cpp:93-98) and the next step's dt (sim.cpp:77-81).
+__device__ __forceinline__ double cell_cmax(double d, double mx, double my, double mz, double e,
+                                            const Phys& ph, bool has_z) {
+    d = smax(d, ph.dmin);
+    double denInv = 1.0 / d;
+    double vx = mx * denInv, vy = my * denInv, vz = mz * denInv;
+    double engKin = has_z ? 0.5 * (vx * mx + vy * my + vz * mz) : 0.5 * (vx * mx + vy * my);
+    double pres = ph.gm1 * (e - engKin);
+    pres = (pres > ph.pmin) ? pres : ph.pmin;
+    double cs = sqrt(ph.gamma * pres * denInv);
+    double local = fabs(vx) + cs;
+    local = smax(local, fabs(vy) + cs);
+    if (has_z) local = smax(local, fabs(vz) + cs);
+    return local;
+}
+
+__device__ void step_epilogue(DevTime* tm, const Geom& g, const Phys& ph, int epilogue) {
+    unsigned long long bits = atomicAdd(&tm->cmax_acc, 0ull);
+    double cm = __longlong_as_double((long long)bits);
+    tm->cmax_acc = (unsigned long long)__double_as_longlong(1e-16);
+    tm->done_ctas = 0;
+    tm->cmax_last = cm;
+    if (!(cm <= DBL_MAX)) tm->status |= gk::STATUS_NONFINITE;
+    if (epilogue) {
+        tm->t += tm->dt;
+        tm->step += 1;
+        tm->dtUntilOutput = tm->tNext - tm->t;
+        if (ph.stepmax > 0 && tm->step >= ph.stepmax) tm->is_continue = 0;
+        if (tm->nlog < tm->log_cap) tm->log[tm->nlog] = tm->dt;
+        tm->nlog += 1;
+        if (tm->steps_left > 0) tm->steps_left -= 1;
+        int act = (fabs(tm->tNext - tm->t) > 1e-12) && tm->is_continue && tm->status == 0 &&
+                  tm->steps_left != 0;
+        if (act) {
+            double dt = ph.cfl * g.drmin / cm;
+            tm->dt = smin(dt, tm->dtUntilOutput);
+        }
+        tm->active = act;
+    }
+}
+
+template <bool HAS_Z>
+__global__ void __launch_bounds__(256) k_cfl(const double* __restrict__ u, Geom g, Phys ph,
+                                             DevTime* tm, int epilogue) {
+    if (epilogue && !tm->active) return;
+    unsigned long long best = 0ull;
+    const long long ncell = (long long)g.nx * g.ny * g.nz;
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < ncell;
+         id += (long long)gridDim.x * blockDim.x) {
+        const int i = g.ib + (int)(id % g.nx);
+        const long long r = id / g.nx;
+        const int j = g.jb + (int)(r % g.ny);
+        const int k = g.kb + (int)(r / g.ny);
+        const long long c = sidx(g, k, j, i);
+        double mz = HAS_Z ? u[gk::S_MTZ * g.vstride + c] : 0.0;
+        double local = cell_cmax(u[gk::S_DEN * g.vstride + c], u[gk::S_MTX * g.vstride + c],
+                                 u[gk::S_MTY * g.vstride + c], mz, u[gk::S_ENG * g.vstride + c],
+                                 ph, HAS_Z);
+        unsigned long long b = (unsigned long long)__double_as_longlong(local);
+        best = b > best ? b : best;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long x = __shfl_xor_sync(0xffffffffu, best, o);
+        best = x > best ? x : best;
+    }
+    __shared__ unsigned long long wmax[8];
+    __shared__ bool last;
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long m = wmax[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = wmax[w] > m ? wmax[w] : m;
+        atomicMax(&tm->cmax_acc, m);
+        __threadfence();
+        unsigned int prev = atomicAdd(&tm->done_ctas, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        step_epilogue(tm, g, ph, epilogue);
+    }
+}
+
+// Start of a Sim::Advance call (sim.cpp:70-72, 77-81) or of a fixed-count
+// run (steps > 0: no output time, step budget).
+__global__ void k_begin(DevTime* tm, Geom g, Phys ph, double dtoutput, int steps) {
+    if (steps > 0) {
+        tm->tNext = CUDART_INF;
+        tm->dtUntilOutput = CUDART_INF;
+        tm->steps_left = steps;
+    } else {
+        tm->tNext = tm->t + dtoutput;
+        tm->dtUntilOutput = dtoutput;
+        tm->steps_left = -1;
+    }
+    int act = (fabs(tm->tNext - tm->t) > 1e-12) && tm->is_continue && tm->status == 0;
+    if (act) {
+        double dt = ph.cfl * g.drmin / tm->cmax_last;
+        tm->dt = smin(dt, tm->dtUntilOutput);
+    }
+    tm->active = act;
+}
+
+__global__ void k_mtz_check(const double* __restrict__ u, Geom g, int* flag) {
+    const long long ncell = (long long)g.nx * g.ny * g.nz;
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < ncell;
+         id += (long long)gridDim.x * blockDim.x) {
+        const int i = g.ib + (int)(id % g.nx);
+        const long long r = id / g.nx;
+        const int j = g.jb + (int)(r % g.ny);
+        const int k = g.kb + (int)(r / g.ny);
+        if (u[gk::S_MTZ * g.vstride + sidx(g, k, j, i)] != 0.0) *flag = 1;
+    }
+}
+
+// ------------------------------------------------------------ fused 2D stage
+// One RK stage of a 2D run with vz = 0 (four variables) in one pass:
+// ConsToPrim (adiabatic.cpp:18-61) -> PLM (recon_piecewise_linear.cpp:8-50)
+// -> HLLC x and y (hllc.cpp:22-101) -> dF (update_cons.cpp:38-47) -> RK
+// combine -> floors (update_cons.cpp:55-68).
+//
+// A CTA of 128 threads owns buffer columns x0-2 .. x0+125 (124 updated
+// columns plus a 2-cell halo each side) and marches up rows y0 .. y1-1.
+// Along y everything stays in registers: each thread carries its column's
+// primitives, the left state of the next y face and the flux of the face
+// below.  Along x, neighbours exchange through shared memory once per row.
+// The raw row two ahead is prefetched so the global load overlaps a row of
+// arithmetic.
+constexpr int kStageThreads = 128;
+constexpr int kStageCols = kStageThreads - 4;
+
+struct W4 {
+    double r, vx, vy, p;
+};
+struct Q4 {
+    double d, mx, my, e;
+};
+
+__device__ __forceinline__ W4 c2p4(const Q4& q, const Phys& ph) {
+    W4 w;
+    double d = smax(q.d, ph.dmin);
+    w.r = d;
+    double denInv = 1.0 / d;
+    w.vx = q.mx * denInv;
+    w.vy = q.my * denInv;
+    double engKin = 0.5 * denInv * (q.mx * q.mx + q.my * q.my);
+    double pre = ph.gm1 * (q.e - engKin);
+    w.p = (pre > ph.pmin) ? pre : ph.pmin;
+    return w;
+}
+
+__device__ __forceinline__ W4 vl4(const W4& a, const W4& b, const W4& c) {
+    W4 s;
+    s.r = vanleer(b.r - a.r, c.r - b.r);
+    s.vx = vanleer(b.vx - a.vx, c.vx - b.vx);
+    s.vy = vanleer(b.vy - a.vy, c.vy - b.vy);
+    s.p = vanleer(b.p - a.p, c.p - b.p);
+    return s;
+}
+
+__device__ __forceinline__ W4 plus_half(const W4& u, const W4& s) {
+    return W4{u.r + 0.5 * s.r, u.vx + 0.5 * s.vx, u.vy + 0.5 * s.vy, u.p + 0.5 * s.p};
+}
+__device__ __forceinline__ W4 minus_half(const W4& u, const W4& s) {
+    return W4{u.r - 0.5 * s.r, u.vx - 0.5 * s.vx, u.vy - 0.5 * s.vy, u.p - 0.5 * s.p};
+}
+
+__device__ __forceinline__ Q4 ldq(const double* __restrict__ u, long long vs, long long c) {
+    return Q4{__ldg(u + c), __ldg(u + vs + c), __ldg(u + 2 * vs + c), __ldg(u + 3 * vs + c)};
+}
+
+template <bool THREE, bool PLM>
+__global__ void __launch_bounds__(kStageThreads, 3)
+    k_stage2d(const double* __restrict__ uc, const double* u0, double* out, Geom g, Phys ph, double c1, double c2, double c3,
+              const DevTime* __restrict__ tm, int rows) {
+    if (!tm->active) return;
+    __shared__ double sP[4][kStageThreads];
+    __shared__ double sXL[4][kStageThreads];
+    __shared__ double sF[4][kStageThreads];
+
+    const double dt = tm->dt;
+    const double dtdx = dt * g.dxRec, dtdy = dt * g.dyRec;
+    const int t = threadIdx.x;
+    const int xi = g.ib - 2 + blockIdx.x * kStageCols + t;
+    const int xl = xi < g.lenx ? xi : g.lenx - 1;  // clamped load column
+    const bool do_sx = t >= 1 && t <= kStageThreads - 2 && xi + 1 < g.lenx;
+    const bool do_fx = t >= 2 && t <= kStageThreads - 2 && xi <= g.ie;
+    const bool do_cell = t >= 2 && t <= kStageThreads - 3 && xi < g.ie;
+    const int y0 = g.jb + blockIdx.y * rows;
+    const int y1 = min(y0 + rows, g.je);
+    const long long vs = g.vstride;
+    const long long P = g.pitch;
+
+    // prologue: rows y0-2, y0-1, y0 (and y0+1 prefetched)
+    const long long cbase = sidx(g, g.kb, 0, xl);
+    W4 Pm2 = c2p4(ldq(uc, vs, cbase + (y0 - 2) * P), ph);
+    Q4 Qm1 = ldq(uc, vs, cbase + (y0 - 1) * P);
+    W4 Pm1 = c2p4(Qm1, ph);
+    Q4 Q0 = ldq(uc, vs, cbase + y0 * P);
+    W4 P0 = c2p4(Q0, ph);
+    Q4 Qn = ldq(uc, vs, cbase + (y0 + 1) * P);
+    // left state of face y0 (from cell y0-1)
+    W4 wlNext;
+    if (PLM) wlNext = plus_half(Pm1, vl4(Pm2, Pm1, P0));
+    else wlNext = Pm1;
+    Flux5 fyPrev{0, 0, 0, 0, 0};
+
+    for (int f = y0; f <= y1; ++f) {
+        const Q4 Q1 = Qn;  // raw row f+1
+        if (f + 2 <= y1 + 1) Qn = ldq(uc, vs, cbase + (f + 2) * P);
+        Q4 U0q;
+        if (THREE && f > y0 && do_cell) {
+            const long long c0 = cbase + (f - 1) * P;  // u0 may alias out: plain loads
+            U0q = Q4{u0[c0], u0[vs + c0], u0[2 * vs + c0], u0[3 * vs + c0]};
+        }
+        const W4 P1 = c2p4(Q1, ph);
+        // y face f between rows f-1 and f
+        W4 wr, wlNew;
+        if (PLM) {
+            const W4 s = vl4(Pm1, P0, P1);
+            wr = minus_half(P0, s);
+            wlNew = plus_half(P0, s);
+        } else {
+            wr = P0;
+            wlNew = P0;
+        }
+        Flux5 fy{0, 0, 0, 0, 0};
+        if (do_cell) {
+            // rotation for y: (vy | vz, vx) with vz = 0, so t1 carries vx
+            hllc<false, kSel>(wlNext.r, wlNext.vy, wlNext.vx, 0.0, wlNext.p, wr.r, wr.vy, wr.vx,
+                              0.0, wr.p, ph, fy);
+        }
+        if (f > y0) {
+            // x work for row f-1 (primitives Pm1)
+            sP[0][t] = Pm1.r; sP[1][t] = Pm1.vx; sP[2][t] = Pm1.vy; sP[3][t] = Pm1.p;
+            __syncthreads();
+            W4 xr = Pm1;
+            if (do_sx) {
+                if (PLM) {
+                    const W4 a{sP[0][t - 1], sP[1][t - 1], sP[2][t - 1], sP[3][t - 1]};
+                    const W4 c{sP[0][t + 1], sP[1][t + 1], sP[2][t + 1], sP[3][t + 1]};
+                    const W4 s = vl4(a, Pm1, c);
+                    const W4 xlft = plus_half(Pm1, s);
+                    xr = minus_half(Pm1, s);
+                    sXL[0][t] = xlft.r; sXL[1][t] = xlft.vx; sXL[2][t] = xlft.vy; sXL[3][t] = xlft.p;
+                } else {
+                    sXL[0][t] = Pm1.r; sXL[1][t] = Pm1.vx; sXL[2][t] = Pm1.vy; sXL[3][t] = Pm1.p;
+                }
+            }
+            __syncthreads();
+            Flux5 fx{0, 0, 0, 0, 0};
+            if (do_fx) {
+                hllc<false, kSel>(sXL[0][t - 1], sXL[1][t - 1], sXL[2][t - 1], 0.0, sXL[3][t - 1],
+                                  xr.r, xr.vx, xr.vy, 0.0, xr.p, ph, fx);
+                sF[0][t] = fx.d; sF[1][t] = fx.n; sF[2][t] = fx.t1; sF[3][t] = fx.e;
+            }
+            __syncthreads();
+            if (do_cell) {
+                // update_cons.cpp:38-53: (Fx(i+1)-Fx(i))*dtdx + (Fy(j+1)-Fy(j))*dtdy
+                double dF0 = (sF[0][t + 1] - fx.d) * dtdx + (fy.d - fyPrev.d) * dtdy;
+                double dF1 = (sF[1][t + 1] - fx.n) * dtdx + (fy.t1 - fyPrev.t1) * dtdy;
+                double dF2 = (sF[2][t + 1] - fx.t1) * dtdx + (fy.n - fyPrev.n) * dtdy;
+                double dF3 = (sF[3][t + 1] - fx.e) * dtdx + (fy.e - fyPrev.e) * dtdy;
+                double r[4];
+                if (THREE) {
+                    r[0] = c1 * U0q.d + c2 * Qm1.d - c3 * dF0;
+                    r[1] = c1 * U0q.mx + c2 * Qm1.mx - c3 * dF1;
+                    r[2] = c1 * U0q.my + c2 * Qm1.my - c3 * dF2;
+                    r[3] = c1 * U0q.e + c2 * Qm1.e - c3 * dF3;
+                } else {
+                    r[0] = c1 * Qm1.d - c2 * dF0;
+                    r[1] = c1 * Qm1.mx - c2 * dF1;
+                    r[2] = c1 * Qm1.my - c2 * dF2;
+                    r[3] = c1 * Qm1.e - c2 * dF3;
+                }
+                floors4(r, ph);
+                const long long oc = cbase + (f - 1) * P;
+                out[oc] = r[0];
+                out[vs + oc] = r[1];
+                out[2 * vs + oc] = r[2];
+                out[3 * vs + oc] = r[3];
+            }
+        }
+        fyPrev = fy;
+        wlNext = wlNew;
+        Pm1 = P0;
+        P0 = P1;
+        Qm1 = Q0;
+        Q0 = Q1;
+    }
+}
+
+// ------------------------------------------------------------ launchers
+static inline dim3 cell_grid(const Geom& g, int threads) {
+    return dim3((g.nx + threads - 1) / threads, g.ny, g.nz);
+}
+
+void launch_bc(const Ctx& c, double* u, cudaStream_t s) {
+    const Geom& g = c.g;
+    long long m = 0;
+    m = max(m, (long long)g.ng * g.ny * g.nz);
+    m = max(m, (long long)g.ng * g.nx * g.nz);
+    m = max(m, (long long)g.ng * g.nx * g.ny);
+    dim3 grid((unsigned)((m + 127) / 128), 6);
+    k_bc<<<grid, 128, 0, s>>>(u, g, c.ph, c.tm);
+}
+
+void launch_c2p(const Ctx& c, const double* u, double* w, cudaStream_t s) {
+    const Geom& g = c.g;
+    dim3 grid((g.lenx + 127) / 128, g.leny, g.nzs);
+    k_c2p<<<grid, 128, 0, s>>>(u, w, g, c.ph, c.tm);
+}
+
+void launch_flux(const Ctx& c, int dir, const double* w, double* F, cudaStream_t s) {
+    const Geom& g = c.g;
+    int na = dir == 0 ? g.nx + 1 : g.nx;
+    int nb = dir == 1 ? g.ny + 1 : g.ny;
+    int nc = dir == 2 ? g.nz + 1 : g.nz;
+    dim3 grid((na + 127) / 128, nb, nc);
+    k_flux<<<grid, 128, 0, s>>>(w, F, g, c.ph, dir, c.tm);
+}
+
+void launch_update(const Ctx& c, const double* u0, const double* uc, double* out,
+                   const double* F1, const double* F2, const double* F3, int three, double c1,
+                   double c2, double c3, cudaStream_t s) {
+    k_update<<<cell_grid(c.g, 128), 128, 0, s>>>(u0, uc, out, F1, F2, F3, c.g, c.ph, three, c1, c2,
+                                                 c3, c.tm);
+}
+
+void launch_kick(const Ctx& c, double* u, cudaStream_t s) {
+    k_kick<<<cell_grid(c.g, 128), 128, 0, s>>>(u, c.g, c.ph, c.tm);
+}
+
+void launch_cfl(const Ctx& c, const double* u, int epilogue, cudaStream_t s) {
+    const Geom& g = c.g;
+    long long ncell = (long long)g.nx * g.ny * g.nz;
+    int blocks = (int)min((ncell + 255) / 256, (long long)148 * 8);
+    if (c.has_vz || g.ndim == 3)
+        k_cfl<true><<<blocks, 256, 0, s>>>(u, g, c.ph, c.tm, epilogue);
+    else
+        k_cfl<false><<<blocks, 256, 0, s>>>(u, g, c.ph, c.tm, epilogue);
+}
+
+void launch_stage2d(const Ctx& c, const double* uc, const double* u0, double* out, int three,
+                    double c1, double c2, double c3, cudaStream_t s) {
+    const Geom& g = c.g;
+    const int rows = c.h2d_rows;
+    dim3 grid((g.nx + kStageCols - 1) / kStageCols, (g.ny + rows - 1) / rows);
+    if (three) {
+        if (c.ph.plm)
+            k_stage2d<true, true><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
+        else
+            k_stage2d<true, false><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
+    } else {
+        if (c.ph.plm)
+            k_stage2d<false, true><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
+        else
+            k_stage2d<false, false><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
+    }
+}
+
+void launch_begin(const Ctx& c, double dtoutput, int steps, cudaStream_t s) {
+    k_begin<<<1, 1, 0, s>>>(c.tm, c.g, c.ph, dtoutput, steps);
+}
+
+void launch_mtz_check(const Ctx& c, const double* u, int* flag, cudaStream_t s) {
+    const Geom& g = c.g;
+    long long ncell = (long long)g.nx * g.ny * g.nz;
+    int blocks = (int)min((ncell + 255) / 256, (long long)148 * 8);
+    k_mtz_check<<<blocks, 256, 0, s>>>(u, g, flag);
+}
+
+}  // namespace GK_NS

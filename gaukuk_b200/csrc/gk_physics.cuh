@@ -1,0 +1,105 @@
+// gk_physics.cuh -- pointwise device physics of the finite-volume update.
+//
+// Included inside the mode namespace (gk_parity / gk_fast).  Every
+// expression keeps the reference's association order; the parity unit is
+// compiled with -fmad=false so nothing is contracted, and IEEE double
+// division and sqrt are correctly rounded on the GPU as on the host, which
+// makes the results bit-identical to the reference built without
+// -ffast-math.  The fast unit lets the compiler contract to FMA.
+#pragma once
+
+// libstdc++ std::max / std::min: max(a,b) = (a<b)?b:a, min(a,b) = (b<a)?b:a.
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+
+// Reconstruction::VanLeer (reconstruction.hpp:36-42).  The quotient is only
+// formed when it is kept; the result is the same value in every case.
+__device__ __forceinline__ double vanleer(double a, double b) {
+    double multi = a * b;
+    return (multi <= 0.0) ? 0.0 : (2.0 * multi) / (a + b);
+}
+
+struct Flux5 {
+    double d, n, t1, t2, e;  // density, normal momentum, tangential 1/2, energy
+};
+
+// Flux::RiemannSolver for one face (hllc.cpp:22-101), HLLC after Toro
+// ch. 10 with the PVRS pressure estimate.  Velocities come as (normal,
+// tangential 1, tangential 2) in the reference's rotation
+// (IVLX, IVLY, IVLZ = hllc.cpp:25-27).  T2 = false drops the second
+// tangential component, which callers use only when it is exactly zero (2D
+// runs with vz = 0): every term it contributes is then an exact zero.
+// SEL = true evaluates only the side picked by ss >= 0 (the other side's
+// weight is 0.0); that changes results only where the reference's unused
+// side is not finite.
+template <bool T2, bool SEL>
+__device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double vzl, double prel,
+                                     double denr, double vxr, double vyr, double vzr, double prer,
+                                     const gk::Phys& ph, Flux5& f) {
+    const double gamma = ph.gamma;
+    // EquationOfState::SoundSpeed (eos.hpp:27-29)
+    double al = sqrt(gamma * prel / denl);
+    double ar = sqrt(gamma * prer / denr);
+    double prePVRS = 0.5 * (prel + prer) - 0.125 * (vxr - vxl) * (denl + denr) * (al + ar);
+    prePVRS = smax(prePVRS, 0.0);
+    // q = sqrt(1 + 0.5*(1+1/gamma)*max(p*/p - 1, 0)) is exactly 1 whenever
+    // p* <= p with p > 0, so the division and root are skipped there.
+    double ql = 1.0, qr = 1.0;
+    if (!(prePVRS <= prel && prel > 0.0)) {
+        double temp = smax(prePVRS / prel - 1, 0.0);
+        ql = sqrt(1 + ph.cq * temp);
+    }
+    if (!(prePVRS <= prer && prer > 0.0)) {
+        double temp = smax(prePVRS / prer - 1, 0.0);
+        qr = sqrt(1 + ph.cq * temp);
+    }
+    double sl = vxl - al * ql;
+    double sr = vxr + ar * qr;
+    double ss = (prer - prel + denl * vxl * (sl - vxl) - denr * vxr * (sr - vxr)) /
+                (denl * (sl - vxl) - denr * (sr - vxr));
+    // EquationOfState::EGas (eos.hpp:30-32) + kinetic energy
+    double kl = T2 ? (vxl * vxl + vyl * vyl + vzl * vzl) : (vxl * vxl + vyl * vyl);
+    double kr = T2 ? (vxr * vxr + vyr * vyr + vzr * vzr) : (vxr * vxr + vyr * vyr);
+    if (!SEL) {
+        double el = prel * ph.gm1Rec + 0.5 * denl * kl;
+        double er = prer * ph.gm1Rec + 0.5 * denr * kr;
+        double cl = smin(0.0, sl) * (ss - vxl) / (sl - ss);
+        double cr = smax(0.0, sr) * (ss - vxr) / (sr - ss);
+        double selectl = (ss >= 0) ? 1.0 : 0.0;
+        double selectr = 1.0 - selectl;
+        double fl1 = denl * (vxl + cl);
+        double fl2 = denl * (vxl * vxl + cl * sl) + prel;
+        double fl3 = fl1 * vyl;
+        double fl5 = (el + prel) * (vxl + cl) + denl * cl * ss * (sl - vxl);
+        double fr1 = denr * (vxr + cr);
+        double fr2 = denr * (vxr * vxr + cr * sr) + prer;
+        double fr3 = fr1 * vyr;
+        double fr5 = (er + prer) * (vxr + cr) + denr * cr * ss * (sr - vxr);
+        f.d = selectl * fl1 + selectr * fr1;
+        f.n = selectl * fl2 + selectr * fr2;
+        f.t1 = selectl * fl3 + selectr * fr3;
+        if (T2) {
+            double fl4 = fl1 * vzl;
+            double fr4 = fr1 * vzr;
+            f.t2 = selectl * fl4 + selectr * fr4;
+        } else {
+            f.t2 = 0.0;
+        }
+        f.e = selectl * fl5 + selectr * fr5;
+    } else {
+        // Only the selected side.
+        const bool left = (ss >= 0);
+        double d = left ? denl : denr, vn = left ? vxl : vxr, v1 = left ? vyl : vyr;
+        double v2 = left ? vzl : vzr, p = left ? prel : prer, s = left ? sl : sr;
+        double k = left ? kl : kr;
+        double e = p * ph.gm1Rec + 0.5 * d * k;
+        double sc = left ? smin(0.0, s) : smax(0.0, s);
+        double c = sc * (ss - vn) / (s - ss);
+        double f1 = d * (vn + c);
+        f.d = f1;
+        f.n = d * (vn * vn + c * s) + p;
+        f.t1 = f1 * v1;
+        f.t2 = T2 ? f1 * v2 : 0.0;
+        f.e = (e + p) * (vn + c) + d * c * ss * (s - vn);
+    }
+}

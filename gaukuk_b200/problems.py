@@ -33,8 +33,8 @@ def splitmix64(x: np.ndarray) -> np.ndarray:
 
 def uniform_pm1(seed: int, ids: np.ndarray) -> np.ndarray:
     """Counter-based U(-1, 1): one draw per global cell id, independent of tiling."""
-    key = np.uint64(seed) * np.uint64(0xD1B54A32D192ED03) & _M64
     with np.errstate(over="ignore"):
+        key = np.uint64(seed) * np.uint64(0xD1B54A32D192ED03) & _M64
         bits = splitmix64((ids.astype(np.uint64) ^ key) & _M64)
     u01 = (bits >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
     return 2.0 * u01 - 1.0

@@ -1,0 +1,180 @@
+"""Python front end of the device finite-volume update.
+
+``Sim`` mirrors the reference's ``Gaukuk::Sim`` (src/sim.hpp:23-58): it holds
+the state of one problem, ``advance(dtoutput)`` is ``Sim::Advance``
+(sim.cpp:69-117), ``get_time/get_dt/get_step`` and ``is_continue`` are the
+reference accessors, and ``run(tmax, dtoutput)`` is the output-cadence loop of
+main.cpp:44-52.  States cross the boundary in the reference's TArray layout,
+``cons[n][k][j][i]``.  All work runs in libgk_cuda.so; nothing here computes.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from . import _lib
+from .config import Params
+
+MODES = {"parity": _lib.GK_MODE_PARITY, "fast": _lib.GK_MODE_FAST}
+
+
+def _descs(p: Params, mode: int, device: int):
+    gd = _lib.GridDesc(p.nx, p.ny, p.nz, p.ng, p.xmin, p.xmax, p.ymin, p.ymax, p.zmin, p.zmax)
+    pd = _lib.PhysDesc()
+    pd.gamma, pd.cfl = p.gamma, p.cfl
+    pd.integrator, pd.rc_order = int(p.integrator), int(p.rc_order)
+    for i in range(6):
+        pd.bc[i] = int(p.bc[i])
+    for i in range(3):
+        pd.grav[i] = float(p.grav[i])
+    pd.dfloor, pd.pfloor = p.dfloor, p.pfloor
+    pd.stepmax = int(p.stepmax)
+    pd.mode = int(mode)
+    pd.device = int(device)
+    return gd, pd
+
+
+class Sim:
+    """One problem on one GPU.  ``mode`` is ``"parity"`` (bit-identical to the
+    reference built with strict IEEE flags) or ``"fast"``."""
+
+    def __init__(self, params: Params, cons: Optional[np.ndarray] = None, mode: str = "parity",
+                 device: int = 0):
+        self.params = params
+        self.mode = mode
+        self._L = _lib.load()
+        gd, pd = _descs(params, MODES[mode], device)
+        h = ctypes.c_void_p()
+        _lib.check(self._L.gk_create(ctypes.byref(gd), ctypes.byref(pd), ctypes.byref(h)))
+        self.h = h
+        if cons is not None:
+            self.upload(cons)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self._L.gk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- state -----------------------------------------------------------
+    def upload(self, cons: np.ndarray) -> None:
+        c = np.ascontiguousarray(cons, dtype=np.float64)
+        if c.shape != self.params.shape:
+            raise ValueError(f"state shape {c.shape} != {self.params.shape}")
+        _lib.check(self._L.gk_upload_cons(self.h, c.ctypes.data_as(ctypes.c_void_p)), self.h)
+
+    def download(self, out: Optional[np.ndarray] = None, planes_only: bool = False) -> np.ndarray:
+        """The state in the reference layout.  planes_only leaves the planes the
+        device does not hold (1D/2D: k != nghost) as they are in ``out``."""
+        if out is None:
+            out = np.empty(self.params.shape, dtype=np.float64)
+            planes_only = False
+        assert out.shape == self.params.shape and out.dtype == np.float64 and out.flags.c_contiguous
+        fn = self._L.gk_download_planes if planes_only else self._L.gk_download_cons
+        _lib.check(fn(self.h, out.ctypes.data_as(ctypes.c_void_p)), self.h)
+        return out
+
+    # -- time loop -------------------------------------------------------
+    def advance(self, dtoutput: float) -> Tuple[float, int, bool]:
+        t, step, cont = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(self._L.gk_advance(self.h, float(dtoutput), ctypes.byref(t), ctypes.byref(step),
+                                      ctypes.byref(cont)), self.h)
+        return t.value, step.value, bool(cont.value)
+
+    def run(self, tmax: Optional[float] = None, dtoutput: Optional[float] = None) -> None:
+        """main.cpp:44-52 without the frame writes."""
+        tmax = self.params.tmax if tmax is None else tmax
+        dtoutput = self.params.dtoutput if dtoutput is None else dtoutput
+        if not dtoutput or dtoutput <= 0:
+            dtoutput = tmax
+        t = self.get_time()
+        while abs(tmax - t) > 1e-12 and self.is_continue:
+            dtoutput = min(dtoutput, tmax - t)
+            t, _, _ = self.advance(dtoutput)
+
+    def run_steps(self, n: int) -> int:
+        done = ctypes.c_int()
+        _lib.check(self._L.gk_run_steps(self.h, int(n), ctypes.byref(done)), self.h)
+        return done.value
+
+    def enqueue_steps(self, n: int) -> None:
+        _lib.check(self._L.gk_enqueue_steps(self.h, int(n)), self.h)
+
+    def _time(self):
+        t, dt, step, cont = ctypes.c_double(), ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(self._L.gk_get_time(self.h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(step),
+                                       ctypes.byref(cont)), self.h)
+        return t.value, dt.value, step.value, bool(cont.value)
+
+    def get_time(self) -> float:
+        return self._time()[0]
+
+    def get_dt(self) -> float:
+        return self._time()[1]
+
+    def get_step(self) -> int:
+        return self._time()[2]
+
+    @property
+    def is_continue(self) -> bool:
+        return self._time()[3]
+
+    def set_time(self, t: float, step: int) -> None:
+        _lib.check(self._L.gk_set_time(self.h, float(t), int(step)), self.h)
+
+    def dt_log(self) -> List[float]:
+        n = ctypes.c_int()
+        _lib.check(self._L.gk_dt_log(self.h, None, 0, ctypes.byref(n)), self.h)
+        buf = np.empty(max(n.value, 1), dtype=np.float64)
+        _lib.check(self._L.gk_dt_log(self.h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     n.value, ctypes.byref(n)), self.h)
+        return buf[:n.value].tolist()
+
+    def cmax(self) -> float:
+        c = ctypes.c_double()
+        _lib.check(self._L.gk_cmax(self.h, ctypes.byref(c)), self.h)
+        return c.value
+
+    @property
+    def path(self) -> str:
+        p = ctypes.c_int()
+        _lib.check(self._L.gk_path(self.h, ctypes.byref(p)), self.h)
+        return {0: "generic", 1: "fused2d"}[p.value]
+
+    def graph_info(self) -> Tuple[int, int]:
+        """(whole steps per graph launch, kernel launches per step)."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _lib.check(self._L.gk_graph_info(self.h, ctypes.byref(a), ctypes.byref(b)), self.h)
+        return a.value, b.value
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _lib.check(self._L.gk_stream(self.h, ctypes.byref(s)), self.h)
+        return s.value or 0
+
+    def profile(self, nsteps: int) -> Dict[str, Tuple[float, int]]:
+        """Device milliseconds and launch counts per kernel class over nsteps
+        un-graphed steps (CUDA events on the handle's stream)."""
+        cap = 16
+        names = ctypes.create_string_buffer(512)
+        ms = (ctypes.c_double * cap)()
+        cnt = (ctypes.c_int * cap)()
+        n = ctypes.c_int()
+        _lib.check(self._L.gk_profile_steps(self.h, int(nsteps), names, 512, ms, cnt, cap,
+                                            ctypes.byref(n)), self.h)
+        keys = names.value.decode().split(";") if n.value else []
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(keys)}

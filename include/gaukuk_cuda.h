@@ -1,0 +1,167 @@
+/*
+ * gaukuk_cuda.h -- C ABI of the B200 finite-volume update (libgk_cuda.so).
+ *
+ * The reference (ShunqH/Gaukuk) is a C++ source-level API: a problem hook
+ * fills Sim::cons on the host and Sim::Advance runs the time loop.  This
+ * library takes over that loop.  The C++ host layer (gaukuk_b200/src) keeps
+ * the reference's classes and calls these entry points; Python reaches them
+ * through ctypes (gaukuk_b200/_lib.py).  Plain pointers and sizes only.
+ *
+ * Host arrays use the reference's TArray layout (template_array.hpp:67-72):
+ * cons[n][k][j][i], n = DEN,MTX,MTY,MTZ,ENG, lenx = nx + 2*nghost
+ * (grid.hpp:26-28), and lenz = nz + 2*nghost planes even in 2D (sim.cpp:49).
+ *
+ * Every function returns GK_OK (0) or a negative GK_ERR_* code; the text of
+ * the last failure on a handle is available from gk_last_error().
+ * One host thread per handle; work is ordered on the handle's CUDA stream and
+ * every entry point returns after that stream has synchronised, except where
+ * stated.
+ */
+#ifndef GAUKUK_CUDA_H
+#define GAUKUK_CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GK_ABI_VERSION 1
+
+enum gk_status {
+    GK_OK = 0,
+    GK_ERR_INVALID = -1,     /* bad argument or configuration */
+    GK_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+    GK_ERR_NONFINITE = -3,   /* the CFL reduction met a non-finite state */
+    GK_ERR_UNSUPPORTED = -4, /* valid for the reference, not implemented here */
+    GK_ERR_STATE = -5        /* call order (e.g. advance before upload) */
+};
+
+/* Arithmetic modes.  PARITY evaluates every expression in the reference's
+ * order with no FMA contraction: results are bit-identical to the reference
+ * compiled with strict IEEE flags (-ffp-contract=off, no -ffast-math),
+ * including the dt sequence.  FAST lets the compiler contract to FMA and
+ * evaluates only the selected HLLC side; it stays within 1e-12 relative of
+ * the reference over 100 steps. */
+enum gk_mode { GK_MODE_PARITY = 0, GK_MODE_FAST = 1 };
+
+/* Boundary types, as read from xleft..zright (boundary.cpp:13-125). */
+enum gk_bc { GK_BC_COPY = 0, GK_BC_PERIODIC = 1, GK_BC_REFLECTIVE = 2, GK_BC_OUTFLOW = 3,
+             GK_BC_FIXED = 4 };
+
+/* Grid + Domain: grid.hpp:18-41 and sim.cpp:16-42 (NX, NY, NZ, NGhost,
+ * xmin..zmax from the .in file). */
+typedef struct gk_grid_desc {
+    int nx, ny, nz, nghost;
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+} gk_grid_desc;
+
+/* Everything else Sim::Sim reads (sim.cpp:45-67, adiabatic.cpp:12-16,
+ * boundary.cpp:13-20), the gravity vector a setup hook enrolls
+ * (SourceTerm::EnrollConstGravityVector, source.cpp:23-31) and the floors
+ * fixed at build time (gaukuk.hpp:11-21, Makefile:47-48). */
+typedef struct gk_phys_desc {
+    double gamma;       /* adiabatic index */
+    double cfl;         /* CFL */
+    int integrator;     /* 1 Euler, 3 RK3, anything else RK2 (sim.cpp:59-66) */
+    int rc_order;       /* 1 first order, anything else PLM (cal_flux.cpp:24) */
+    int bc[6];          /* xleft xright yleft yright zleft zright */
+    double grav[3];     /* constant gravity; all zero = no source term */
+    double dfloor;      /* density floor (1e-16 in the reference build) */
+    double pfloor;      /* pressure floor (1e-16) */
+    int stepmax;        /* <= 0: unlimited (sim.cpp:58, 95-97) */
+    int mode;           /* enum gk_mode */
+    int device;         /* CUDA device ordinal */
+} gk_phys_desc;
+
+typedef struct gk_handle gk_handle;
+
+/* Replaces Sim::Sim (sim.cpp:45-67) with Boundary::Boundary (boundary.cpp:13-125)
+ * and EquationOfState::EquationOfState (adiabatic.cpp:12-16): validates the
+ * configuration and allocates the device state.  Time starts at t = 0,
+ * step = 0 (sim.cpp:45-46). */
+int gk_create(const gk_grid_desc* grid, const gk_phys_desc* phys, gk_handle** out);
+
+/* Releases the handle, its stream, graphs and device memory. */
+void gk_destroy(gk_handle* h);
+
+/* Number of doubles in one reference-layout state: 5*lenz*leny*lenx. */
+long long gk_state_size(const gk_handle* h);
+
+/* Loads Sim::cons from the host after the setup hook ran (main.cpp:25-30):
+ * the whole array, ghosts included, is copied to the device (the host array
+ * is not retained), the dt log is cleared and the CFL reduction of
+ * EquationOfState::CalCmax (adiabatic.cpp:115-160) is evaluated so that the
+ * next step's dt is ready. */
+int gk_upload_cons(gk_handle* h, const double* cons);
+
+/* Copies the device state back into a reference-layout host array, as
+ * Sim::WriteData reads it (write_sim.cpp:14-58).  Active cells are exactly
+ * the reference's.  In 1D/2D the planes k != nghost are written as zero.
+ * Ghost cells hold the boundary fill of the current state. */
+int gk_download_cons(gk_handle* h, double* cons);
+
+/* As gk_download_cons, but writes only the planes the device holds (in 1D/2D
+ * the active plane k = nghost) and leaves the caller's other planes as they
+ * are -- the copy Sim::WriteData needs when Sim::cons is reused between
+ * frames, since the reference never writes those planes. */
+int gk_download_planes(gk_handle* h, double* cons);
+
+/* Replaces Sim::Advance (sim.cpp:69-117, sim.hpp:39): runs time steps on the
+ * device until the output time t + dtoutput is reached (tolerance 1e-12),
+ * stepmax is hit, or the CFL reduction fails.  Each step: cmax -> dt =
+ * min(CFL*drmin/cmax, dtUntilOutput) -> gravity half kick -> integrator ->
+ * gravity half kick -> t += dt.  Outputs (any may be NULL): time, step count
+ * and the isContinue flag after the call. */
+int gk_advance(gk_handle* h, double dtoutput, double* t, int* step, int* is_continue);
+
+/* Runs exactly nsteps steps (fewer if stepmax stops the run) with no output
+ * time to clamp dt, i.e. Sim::Advance with an infinite dtoutput.  Returns
+ * after the stream synchronises; *done receives the steps taken. */
+int gk_run_steps(gk_handle* h, int nsteps, int* done);
+
+/* As gk_run_steps, but only enqueues the work on the handle's stream and
+ * returns at once: the steps beyond the run's end are no-ops on the device.
+ * Used to time a device-resident loop with events on gk_stream(). */
+int gk_enqueue_steps(gk_handle* h, int nsteps);
+
+/* Sim::GetTime / Getdt / GetStep and Sim::isContinue (sim.hpp:26,44-46). */
+int gk_get_time(gk_handle* h, double* t, double* dt, int* step, int* is_continue);
+
+/* Sets the simulation clock (restart from a written frame). */
+int gk_set_time(gk_handle* h, double t, int step);
+
+/* The dt of every step since the last upload, at full precision: the values
+ * Sim::Advance prints with 6 digits (sim.cpp:100-103).  Copies up to cap
+ * entries; *n receives the total count. */
+int gk_dt_log(gk_handle* h, double* buf, int cap, int* n);
+
+/* EquationOfState::CalCmax seeded with 1e-16 (sim.cpp:77-78) on the current
+ * device state. */
+int gk_cmax(gk_handle* h, double* cmax);
+
+/* The handle's CUDA stream (a cudaStream_t), for callers that time or order
+ * work around the library's launches. */
+int gk_stream(gk_handle* h, void** stream);
+
+/* Which device implementation the handle selected: 0 generic (unfused
+ * per-phase kernels, any dimension), 1 fused 2D stage kernel. */
+int gk_path(gk_handle* h, int* path);
+
+/* Launch accounting: whole time steps per graph launch, and kernel launches
+ * per time step on the selected path. */
+int gk_graph_info(gk_handle* h, int* steps_per_graph, int* launches_per_step);
+
+/* Device time of each kernel class over `nsteps` un-graphed steps, measured
+ * with CUDA events on the handle's stream: names (';'-separated, into
+ * `names`, size `names_cap`), per-class total milliseconds and launch counts
+ * (arrays of `cap` entries).  *n receives the number of classes. */
+int gk_profile_steps(gk_handle* h, int nsteps, char* names, int names_cap,
+                     double* total_ms, int* launches, int cap, int* n);
+
+/* Text for a status code, and the last failure message on a handle. */
+const char* gk_strerror(int status);
+const char* gk_last_error(const gk_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GAUKUK_CUDA_H */

@@ -14,7 +14,9 @@
 //   * --out FILE writes the final state as a raw array; --frames writes the
 //     reference's own cons_XXXXX files via Sim::WriteData;
 //   * wall time spent inside Sim::Advance only (no setup, no I/O) is
-//     reported as one JSON line on stderr.
+//     reported as one JSON line on stderr, with the time at which each
+//     per-step line was written (--step-times), so that the first steps,
+//     which also page in the reference's arrays, can be left out.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -27,6 +29,30 @@
 #include "gaukuk.hpp"
 #include "sim.hpp"
 
+namespace {
+
+// Forwards to std::cout's buffer and notes the time of every newline.
+class StampBuf : public std::streambuf {
+public:
+    explicit StampBuf(std::streambuf* out) : out_(out) {}
+    std::vector<double> stamps;
+
+protected:
+    int overflow(int c) override {
+        if (c == traits_type::eof()) return out_->pubsync() == 0 ? 0 : traits_type::eof();
+        if (c == '\n')
+            stamps.push_back(std::chrono::duration<double>(
+                                 std::chrono::steady_clock::now().time_since_epoch()).count());
+        return out_->sputc(static_cast<char>(c));
+    }
+    int sync() override { return out_->pubsync(); }
+
+private:
+    std::streambuf* out_;
+};
+
+}  // namespace
+
 #ifndef GK_DRIVER_HAS_SETUP
 // The problem hook is empty unless a setup file is linked: the state comes
 // from --ic.
@@ -36,7 +62,7 @@ void Gaukuk::Sim::Setup() {}
 int main(int argc, char** argv) {
     using namespace Gaukuk;
     std::string infile, icfile, outfile;
-    bool frames = false, quiet = false;
+    bool frames = false, quiet = false, step_times = false;
     double tmax_override = -1.0;
     for (int a = 1; a < argc; ++a) {
         std::string s = argv[a];
@@ -46,6 +72,7 @@ int main(int argc, char** argv) {
         else if (s == "--tmax" && a + 1 < argc) tmax_override = std::atof(argv[++a]);
         else if (s == "--frames") frames = true;
         else if (s == "--quiet") quiet = true;
+        else if (s == "--step-times") step_times = true;
         else {
             std::cerr << "usage: " << argv[0]
                       << " -i input.in [--ic state.bin] [--out state.bin] [--tmax T] [--frames] [--quiet]\n";
@@ -75,6 +102,9 @@ int main(int argc, char** argv) {
     if (gx != 0 || gy != 0 || gz != 0) sim.srcTerm.EnrollConstGravityVector(gx, gy, gz);
 
     std::cout.precision(17);
+    std::streambuf* const original = std::cout.rdbuf();
+    StampBuf stamp(original);
+    if (step_times) std::cout.rdbuf(&stamp);
     if (quiet) std::cout.setstate(std::ios_base::failbit);
 
     int outputStep = 0;
@@ -94,6 +124,8 @@ int main(int argc, char** argv) {
         if (frames) sim.WriteData(outputStep, DataType::Cons);
     }
     std::cout.clear();
+    std::cout.flush();
+    std::cout.rdbuf(original);  // the stamping buffer dies with main()
     if (!outfile.empty()) {
         FILE* f = std::fopen(outfile.c_str(), "wb");
         if (!f) { std::cerr << "cannot open " << outfile << "\n"; return 3; }
@@ -101,8 +133,16 @@ int main(int argc, char** argv) {
         std::fclose(f);
     }
     long long cells = (long long)sim.grid.nx * sim.grid.ny * sim.grid.nz;
+    std::string st = "[";
+    for (size_t n = 0; n < stamp.stamps.size(); ++n) {
+        char b[40];
+        std::snprintf(b, sizeof(b), "%s%.6f", n ? ", " : "", stamp.stamps[n] - stamp.stamps[0]);
+        st += b;
+    }
+    st += "]";
     std::fprintf(stderr,
-                 "{\"steps\": %d, \"t\": %.17g, \"advance_seconds\": %.6f, \"cells\": %lld}\n",
-                 sim.GetStep(), (double)sim.GetTime(), seconds, cells);
+                 "{\"steps\": %d, \"t\": %.17g, \"advance_seconds\": %.6f, \"cells\": %lld, "
+                 "\"step_stamps\": %s}\n",
+                 sim.GetStep(), (double)sim.GetTime(), seconds, cells, st.c_str());
     return 0;
 }

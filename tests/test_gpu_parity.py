@@ -1,0 +1,152 @@
+"""Parity of the CUDA path (libgk_cuda.so, through the C ABI) with the oracle.
+
+Parity mode must equal the oracle exactly -- every active conserved value
+(np.array_equal, so -0.0 == 0.0) and every dt.  Fast mode must stay within
+1e-12 relative L-infinity per conserved variable after 100 steps, the
+contract for the floating-point path.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from gaukuk_b200 import problems
+from gaukuk_b200.config import Params
+from helpers import active, golden_cases, load_golden, rel_linf
+
+pytestmark = pytest.mark.gpu
+gk_oracle = pytest.importorskip("gk_oracle")
+
+FAST_TOL = 1e-12
+
+
+def _sim(p, c, mode="parity"):
+    from gaukuk_b200.sim import Sim
+    return Sim(p, c, mode=mode)
+
+
+def _oracle_run(p, c):
+    o = gk_oracle.OracleSim(p, c)
+    dts = o.run(p.tmax, p.dtoutput)
+    return active(p, o.get_cons()), dts, o
+
+
+@pytest.mark.parametrize("name", sorted(golden_cases()))
+def test_golden_vectors_on_gpu(name):
+    p, cons, final, dts = load_golden(name)
+    s = _sim(p, cons)
+    s.run(p.tmax, p.dtoutput)
+    assert s.dt_log() == dts
+    assert np.array_equal(active(p, s.download()), final)
+
+
+def _cases():
+    p, c = problems.kh(64, seed=1)
+    yield "kh64_rk2", dataclasses.replace(p, stepmax=60), c
+    p, c = problems.kh(130, ny=70, seed=2, integrator=3)
+    yield "kh130x70_rk3", dataclasses.replace(p, stepmax=30), c
+    p, c = problems.kh(50, ny=300, seed=4, rc_order=1)
+    yield "kh50x300_rc1_tall", dataclasses.replace(p, stepmax=20), c
+    p, c = problems.kh(40, ny=40, integrator=1, cfl=0.2)
+    yield "kh40_euler", dataclasses.replace(p, stepmax=20), c
+    for bcs in [(2, 2, 3, 3, 1, 1), (3, 0, 2, 1, 1, 1), (0, 0, 0, 0, 1, 1)]:
+        p, c = problems.kh(37, ny=45, seed=5)
+        yield f"kh_bc{''.join(map(str, bcs[:4]))}", dataclasses.replace(p, bc=bcs, stepmax=25), c
+    p, c = problems.sod(256)
+    yield "sod256", p, c
+    p, c = problems.sod(256, integrator=3, bc=2)
+    yield "sod256_rk3_reflect", p, c
+    p, c = problems.rt(32, 96)
+    yield "rt32x96_gravity", dataclasses.replace(p, stepmax=40), c
+    p = Params(nx=16, ny=12, nz=10, bc=(1, 1, 2, 3, 0, 1), integrator=3, tmax=1.0, dtoutput=1.0,
+               stepmax=10)
+    yield "box16x12x10", p, problems.random_smooth(p, seed=3, with_vz=True)
+    p = Params(nx=24, ny=20, nz=1, integrator=2, tmax=1.0, dtoutput=1.0, stepmax=15)
+    yield "kh_with_vz", p, problems.random_smooth(p, seed=4, with_vz=True)
+
+
+@pytest.mark.parametrize("case", list(_cases()), ids=lambda c: c[0])
+def test_parity_mode_bitwise(case):
+    _, p, c = case
+    ref, ref_dts, _ = _oracle_run(p, c)
+    s = _sim(p, c)
+    s.run(p.tmax, p.dtoutput)
+    assert s.dt_log() == ref_dts
+    assert np.array_equal(active(p, s.download()), ref)
+
+
+def test_paths_selected():
+    p, c = problems.kh(32)
+    assert _sim(p, c).path == "fused2d"
+    p, c = problems.sod(64)
+    assert _sim(p, c).path == "generic"
+
+
+@pytest.mark.parametrize("n", [256])
+def test_fast_mode_within_tolerance_100_steps(n):
+    p, c = problems.kh(n)
+    p = dataclasses.replace(p, stepmax=100)
+    ref, ref_dts, _ = _oracle_run(p, c)
+    s = _sim(p, c, mode="fast")
+    s.run(p.tmax, p.dtoutput)
+    assert len(s.dt_log()) == 100
+    errs = rel_linf(active(p, s.download()), ref)
+    assert max(errs[v] for v in (0, 1, 2, 4)) <= FAST_TOL, errs
+
+
+def test_advance_semantics_match_reference_loop():
+    """Sim::Advance clamps the last dt to the output time and keeps t, step
+    and isContinue across calls (sim.cpp:69-117); stepmax stops the run."""
+    p, c = problems.kh(48)
+    p = dataclasses.replace(p, tmax=0.05, dtoutput=0.013, stepmax=-1)
+    o = gk_oracle.OracleSim(p, c)
+    s = _sim(p, c)
+    for _ in range(3):
+        o_dts = o.advance(0.013)
+        t, step, cont = s.advance(0.013)
+        assert t == o.time and step == o.step and cont == o.is_continue
+    assert s.dt_log()[-len(o_dts):] == o_dts
+    q = dataclasses.replace(p, stepmax=7)
+    s2 = _sim(q, c)
+    t, step, cont = s2.advance(1.0)
+    assert step == 7 and not cont
+    t2, step2, _ = s2.advance(1.0)
+    assert (t2, step2) == (t, step)
+
+
+def test_nonfinite_state_is_reported():
+    """A NaN injected on the host into the uploaded state is reported by the
+    CFL reduction as an error, not propagated silently."""
+    from gaukuk_b200._lib import GkError
+    p, c = problems.kh(32)
+    c = c.copy()
+    c[0, 2, 10, 10] = np.nan
+    with pytest.raises(GkError):
+        _sim(p, c)
+
+
+def test_kh4096_parity_vs_fast_and_conservation():
+    """Full size (4096^2): parity and fast modes agree to 1e-12 after a few
+    steps and both conserve mass and energy to round-off."""
+    p, c = problems.kh(4096)
+    s1 = _sim(p, c, "parity")
+    s2 = _sim(p, c, "fast")
+    assert s1.run_steps(4) == 4 and s2.run_steps(4) == 4
+    a, b = active(p, s1.download()), active(p, s2.download())
+    errs = rel_linf(b, a)
+    assert max(errs[v] for v in (0, 1, 2, 4)) < FAST_TOL, errs
+    m0 = active(p, c).sum(axis=(1, 2, 3))
+    for x in (a, b):
+        m = x.sum(axis=(1, 2, 3))
+        assert abs(m[0] - m0[0]) / m0[0] < 1e-13
+        assert abs(m[4] - m0[4]) / m0[4] < 1e-13
+
+
+def test_kh4096_two_steps_against_oracle():
+    p, c = problems.kh(4096)
+    p = dataclasses.replace(p, stepmax=2)
+    ref, ref_dts, _ = _oracle_run(p, c)
+    s = _sim(p, c)
+    s.run(p.tmax, p.dtoutput)
+    assert s.dt_log() == ref_dts
+    assert np.array_equal(active(p, s.download()), ref)
