@@ -56,6 +56,7 @@ SIGNATURES = {
     "gk_graph_info": (ctypes.c_int, [_vp, _ip, _ip]),
     "gk_profile_steps": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _dp,
                                         _ip, ctypes.c_int, _ip]),
+    "gk_fastmath_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_ulonglong, _dp]),
     "gk_strerror": (ctypes.c_char_p, [ctypes.c_int]),
     "gk_last_error": (ctypes.c_char_p, [_vp]),
 }

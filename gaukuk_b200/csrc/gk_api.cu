@@ -12,12 +12,17 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "gaukuk_cuda.h"
 #include "gk_internal.h"
+
+namespace gk_fast {
+int fastmath_check(int n, unsigned long long seed, double* host_worst3);
+}
 
 namespace {
 
@@ -217,14 +222,21 @@ int alloc_generic(gk_handle* h) {
     return GK_OK;
 }
 
-// Rows per CTA segment of the fused kernel: enough segments for about four
-// CTAs per SM, at least 8 rows each.
+int env_int(const char* name, int dflt) {
+    const char* v = std::getenv(name);
+    return v && *v ? std::atoi(v) : dflt;
+}
+
+// Rows per CTA segment of the fused kernel.  Short segments (16 rows) give
+// many waves of CTAs, so no partial last wave dominates (measured on 4096^2:
+// 16-32 rows beat one wave of long segments by 1.5x); small grids use down
+// to 4 rows so that every SM gets work.  GK_STAGE_ROWS overrides (tuning).
 int stage_rows(const gk::Geom& g) {
-    int strips = (g.nx + 123) / 124;
-    int target = 148 * 4;
-    int segs = std::max(1, (target + strips - 1) / strips);
-    int rows = (g.ny + segs - 1) / segs;
-    return std::max(8, rows);
+    int forced = env_int("GK_STAGE_ROWS", 0);
+    if (forced > 0) return forced;
+    long long strips = (g.nx + 123) / 124;
+    long long per_slot = (long long)g.ny * strips / (148 * 4);
+    return (int)std::max(4LL, std::min(16LL, per_slot));
 }
 
 // One time step.  Kernel order per RK stage follows Sim::RK2_/RK3_/
@@ -416,6 +428,7 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
     }
     h->path = (g.ndim == 2 && !h->ctx.has_vz && h->ctx.ph.integrator != 1) ? 1 : 0;
     h->ctx.h2d_rows = stage_rows(g);
+    h->ctx.stage_minb = env_int("GK_STAGE_MINB", 4) == 3 ? 3 : 4;
     if (h->path == 0) {
         int rc = alloc_generic(h);
         if (rc != GK_OK) return rc;
@@ -638,6 +651,11 @@ int gk_profile_steps(gk_handle* h, int nsteps, char* names, int names_cap, doubl
     }
     if (n) *n = m;
     return pull_time(h);
+}
+
+int gk_fastmath_check(int n, unsigned long long seed, double* worst3) {
+    if (n <= 0 || !worst3) return GK_ERR_INVALID;
+    return gk_fast::fastmath_check(n, seed, worst3) == 0 ? GK_OK : GK_ERR_CUDA;
 }
 
 const char* gk_strerror(int status) {

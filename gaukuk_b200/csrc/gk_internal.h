@@ -71,6 +71,7 @@ struct Ctx {
     DevTime* tm;
     int has_vz;      // 2D: MTZ not identically zero -> generic path
     int h2d_rows;    // fused 2D kernel: rows per CTA segment
+    int stage_minb;  // fused 2D kernel: CTAs per SM the register budget targets (3 or 4)
 };
 
 // Kernel classes, for per-kernel profiling.

@@ -106,7 +106,7 @@ __device__ __forceinline__ void cons_to_prim5(double d, double mx, double my, do
                                               const Phys& ph, double w[5]) {
     d = smax(d, ph.dmin);
     w[gk::P_RHO] = d;
-    double denInv = 1.0 / d;
+    double denInv = GK_RCP(d);
     w[gk::P_VX] = mx * denInv;
     w[gk::P_VY] = my * denInv;
     w[gk::P_VZ] = mz * denInv;
@@ -197,7 +197,7 @@ __device__ __forceinline__ void floors5(double (&r)[5], const Phys& ph) {
         r[gk::S_MTZ] = 0.0;
         r[gk::S_ENG] = ph.pmin / ph.gm1 + 0.0;
     } else {
-        double inv_den = 1.0 / r[gk::S_DEN];
+        double inv_den = GK_RCP(r[gk::S_DEN]);
         double ke = 0.5 * inv_den *
                     (r[gk::S_MTX] * r[gk::S_MTX] + r[gk::S_MTY] * r[gk::S_MTY] +
                      r[gk::S_MTZ] * r[gk::S_MTZ]);
@@ -215,7 +215,7 @@ __device__ __forceinline__ void floors4(double (&r)[4], const Phys& ph) {
         r[2] = 0.0;
         r[3] = ph.pmin / ph.gm1 + 0.0;
     } else {
-        double inv_den = 1.0 / r[0];
+        double inv_den = GK_RCP(r[0]);
         double ke = 0.5 * inv_den * (r[1] * r[1] + r[2] * r[2]);
         double press = ph.gm1 * (r[3] - ke);
         if (press < ph.pmin) r[3] = ph.pmin / ph.gm1 + ke;
@@ -410,8 +410,11 @@ __global__ void k_mtz_check(const double* __restrict__ u, Geom g, int* flag) {
 // Along y everything stays in registers: each thread carries its column's
 // primitives, the left state of the next y face and the flux of the face
 // below.  Along x, neighbours exchange through shared memory once per row.
-// The raw row two ahead is prefetched so the global load overlaps a row of
-// arithmetic.
+// Every lane runs the same straight-line body (halo lanes read clamped
+// neighbours and discard their results); the x-face and the y-face Riemann
+// problems of a row are independent, so they sit side by side between the
+// same barriers and their instruction streams interleave.  Raw rows are
+// prefetched two rows ahead, the RK base state u0 one row ahead.
 constexpr int kStageThreads = 128;
 constexpr int kStageCols = kStageThreads - 4;
 
@@ -426,7 +429,7 @@ __device__ __forceinline__ W4 c2p4(const Q4& q, const Phys& ph) {
     W4 w;
     double d = smax(q.d, ph.dmin);
     w.r = d;
-    double denInv = 1.0 / d;
+    double denInv = GK_RCP(d);
     w.vx = q.mx * denInv;
     w.vy = q.my * denInv;
     double engKin = 0.5 * denInv * (q.mx * q.mx + q.my * q.my);
@@ -455,10 +458,19 @@ __device__ __forceinline__ Q4 ldq(const double* __restrict__ u, long long vs, lo
     return Q4{__ldg(u + c), __ldg(u + vs + c), __ldg(u + 2 * vs + c), __ldg(u + 3 * vs + c)};
 }
 
-template <bool THREE, bool PLM>
-__global__ void __launch_bounds__(kStageThreads, 3)
-    k_stage2d(const double* __restrict__ uc, const double* u0, double* out, Geom g, Phys ph, double c1, double c2, double c3,
-              const DevTime* __restrict__ tm, int rows) {
+// y face: rotation (vy | vz, vx) with vz = 0, so tangential 1 carries vx.
+__device__ __forceinline__ void hllc_y(const W4& l, const W4& r, const Phys& ph, Flux5& f) {
+    hllc<false, kSel>(l.r, l.vy, l.vx, 0.0, l.p, r.r, r.vy, r.vx, 0.0, r.p, ph, f);
+}
+// x face: rotation (vx | vy, vz).
+__device__ __forceinline__ void hllc_x(const W4& l, const W4& r, const Phys& ph, Flux5& f) {
+    hllc<false, kSel>(l.r, l.vx, l.vy, 0.0, l.p, r.r, r.vx, r.vy, 0.0, r.p, ph, f);
+}
+
+template <bool THREE, bool PLM, int MINB>
+__global__ void __launch_bounds__(kStageThreads, MINB)
+    k_stage2d(const double* __restrict__ uc, const double* u0, double* out, Geom g, Phys ph,
+              double c1, double c2, double c3, const DevTime* __restrict__ tm, int rows) {
     if (!tm->active) return;
     __shared__ double sP[4][kStageThreads];
     __shared__ double sXL[4][kStageThreads];
@@ -467,105 +479,112 @@ __global__ void __launch_bounds__(kStageThreads, 3)
     const double dt = tm->dt;
     const double dtdx = dt * g.dxRec, dtdy = dt * g.dyRec;
     const int t = threadIdx.x;
+    const int tl = t > 0 ? t - 1 : 0;                       // clamped neighbours
+    const int tr = t < kStageThreads - 1 ? t + 1 : t;
     const int xi = g.ib - 2 + blockIdx.x * kStageCols + t;
-    const int xl = xi < g.lenx ? xi : g.lenx - 1;  // clamped load column
-    const bool do_sx = t >= 1 && t <= kStageThreads - 2 && xi + 1 < g.lenx;
-    const bool do_fx = t >= 2 && t <= kStageThreads - 2 && xi <= g.ie;
+    const int xl = xi < g.lenx ? xi : g.lenx - 1;           // clamped load column
     const bool do_cell = t >= 2 && t <= kStageThreads - 3 && xi < g.ie;
     const int y0 = g.jb + blockIdx.y * rows;
     const int y1 = min(y0 + rows, g.je);
     const long long vs = g.vstride;
     const long long P = g.pitch;
-
-    // prologue: rows y0-2, y0-1, y0 (and y0+1 prefetched)
     const long long cbase = sidx(g, g.kb, 0, xl);
-    W4 Pm2 = c2p4(ldq(uc, vs, cbase + (y0 - 2) * P), ph);
-    Q4 Qm1 = ldq(uc, vs, cbase + (y0 - 1) * P);
-    W4 Pm1 = c2p4(Qm1, ph);
+
+    // prologue: primitives of rows y0-2, y0-1, y0; raw row y0+1 in flight
+    const W4 Pm2 = c2p4(ldq(uc, vs, cbase + (y0 - 2) * P), ph);
+    W4 Pm1 = c2p4(ldq(uc, vs, cbase + (y0 - 1) * P), ph);
     Q4 Q0 = ldq(uc, vs, cbase + y0 * P);
     W4 P0 = c2p4(Q0, ph);
     Q4 Qn = ldq(uc, vs, cbase + (y0 + 1) * P);
-    // left state of face y0 (from cell y0-1)
-    W4 wlNext;
-    if (PLM) wlNext = plus_half(Pm1, vl4(Pm2, Pm1, P0));
-    else wlNext = Pm1;
-    Flux5 fyPrev{0, 0, 0, 0, 0};
-
-    for (int f = y0; f <= y1; ++f) {
-        const Q4 Q1 = Qn;  // raw row f+1
-        if (f + 2 <= y1 + 1) Qn = ldq(uc, vs, cbase + (f + 2) * P);
-        Q4 U0q;
-        if (THREE && f > y0 && do_cell) {
-            const long long c0 = cbase + (f - 1) * P;  // u0 may alias out: plain loads
-            U0q = Q4{u0[c0], u0[vs + c0], u0[2 * vs + c0], u0[3 * vs + c0]};
+    Q4 Qm1;
+    Q4 U0n{0, 0, 0, 0};
+    // left state of y face y0 (cell y0-1)
+    W4 wlNext = PLM ? plus_half(Pm1, vl4(Pm2, Pm1, P0)) : Pm1;
+    Flux5 fyPrev;
+    {
+        // y face y0 (no cell of this segment is complete yet)
+        const Q4 Q1 = Qn;
+        Qn = ldq(uc, vs, cbase + (y0 + 2) * P);
+        if (THREE) {
+            const long long c0 = cbase + y0 * P;  // u0 may alias out: plain loads
+            U0n = Q4{u0[c0], u0[vs + c0], u0[2 * vs + c0], u0[3 * vs + c0]};
         }
         const W4 P1 = c2p4(Q1, ph);
-        // y face f between rows f-1 and f
-        W4 wr, wlNew;
+        W4 wr = P0, wlNew = P0;
         if (PLM) {
             const W4 s = vl4(Pm1, P0, P1);
             wr = minus_half(P0, s);
             wlNew = plus_half(P0, s);
+        }
+        hllc_y(wlNext, wr, ph, fyPrev);
+        wlNext = wlNew;
+        Pm1 = P0;
+        P0 = P1;
+        Qm1 = Q0;
+        Q0 = Q1;
+    }
+
+    for (int f = y0 + 1; f <= y1; ++f) {
+        // loads in flight across the arithmetic of this row
+        const Q4 Q1 = Qn;  // raw row f+1
+        if (f + 2 <= y1 + 1) Qn = ldq(uc, vs, cbase + (f + 2) * P);
+        const Q4 U0 = U0n;  // base state of row f-1
+        if (THREE && f <= y1 - 1) {
+            const long long c0 = cbase + f * P;
+            U0n = Q4{u0[c0], u0[vs + c0], u0[2 * vs + c0], u0[3 * vs + c0]};
+        }
+        const W4 P1 = c2p4(Q1, ph);
+
+        // x neighbours of row f-1
+        sP[0][t] = Pm1.r; sP[1][t] = Pm1.vx; sP[2][t] = Pm1.vy; sP[3][t] = Pm1.p;
+        __syncthreads();
+        W4 xr = Pm1, wr = P0, wlNew = P0;
+        if (PLM) {
+            const W4 a{sP[0][tl], sP[1][tl], sP[2][tl], sP[3][tl]};
+            const W4 c{sP[0][tr], sP[1][tr], sP[2][tr], sP[3][tr]};
+            const W4 sx = vl4(a, Pm1, c);
+            const W4 sy = vl4(Pm1, P0, P1);
+            const W4 xlft = plus_half(Pm1, sx);
+            xr = minus_half(Pm1, sx);
+            wr = minus_half(P0, sy);
+            wlNew = plus_half(P0, sy);
+            sXL[0][t] = xlft.r; sXL[1][t] = xlft.vx; sXL[2][t] = xlft.vy; sXL[3][t] = xlft.p;
         } else {
-            wr = P0;
-            wlNew = P0;
+            sXL[0][t] = Pm1.r; sXL[1][t] = Pm1.vx; sXL[2][t] = Pm1.vy; sXL[3][t] = Pm1.p;
         }
-        Flux5 fy{0, 0, 0, 0, 0};
+        __syncthreads();
+        // the two Riemann problems of this row: x face at the left of cell
+        // (f-1, xi) and y face f below cell (f, xi)
+        const W4 xl_state{sXL[0][tl], sXL[1][tl], sXL[2][tl], sXL[3][tl]};
+        Flux5 fx, fy;
+        hllc_x(xl_state, xr, ph, fx);
+        hllc_y(wlNext, wr, ph, fy);
+        sF[0][t] = fx.d; sF[1][t] = fx.n; sF[2][t] = fx.t1; sF[3][t] = fx.e;
+        __syncthreads();
         if (do_cell) {
-            // rotation for y: (vy | vz, vx) with vz = 0, so t1 carries vx
-            hllc<false, kSel>(wlNext.r, wlNext.vy, wlNext.vx, 0.0, wlNext.p, wr.r, wr.vy, wr.vx,
-                              0.0, wr.p, ph, fy);
-        }
-        if (f > y0) {
-            // x work for row f-1 (primitives Pm1)
-            sP[0][t] = Pm1.r; sP[1][t] = Pm1.vx; sP[2][t] = Pm1.vy; sP[3][t] = Pm1.p;
-            __syncthreads();
-            W4 xr = Pm1;
-            if (do_sx) {
-                if (PLM) {
-                    const W4 a{sP[0][t - 1], sP[1][t - 1], sP[2][t - 1], sP[3][t - 1]};
-                    const W4 c{sP[0][t + 1], sP[1][t + 1], sP[2][t + 1], sP[3][t + 1]};
-                    const W4 s = vl4(a, Pm1, c);
-                    const W4 xlft = plus_half(Pm1, s);
-                    xr = minus_half(Pm1, s);
-                    sXL[0][t] = xlft.r; sXL[1][t] = xlft.vx; sXL[2][t] = xlft.vy; sXL[3][t] = xlft.p;
-                } else {
-                    sXL[0][t] = Pm1.r; sXL[1][t] = Pm1.vx; sXL[2][t] = Pm1.vy; sXL[3][t] = Pm1.p;
-                }
+            // update_cons.cpp:38-53: (Fx(i+1)-Fx(i))*dtdx + (Fy(j+1)-Fy(j))*dtdy
+            double dF0 = (sF[0][tr] - fx.d) * dtdx + (fy.d - fyPrev.d) * dtdy;
+            double dF1 = (sF[1][tr] - fx.n) * dtdx + (fy.t1 - fyPrev.t1) * dtdy;
+            double dF2 = (sF[2][tr] - fx.t1) * dtdx + (fy.n - fyPrev.n) * dtdy;
+            double dF3 = (sF[3][tr] - fx.e) * dtdx + (fy.e - fyPrev.e) * dtdy;
+            double r[4];
+            if (THREE) {
+                r[0] = c1 * U0.d + c2 * Qm1.d - c3 * dF0;
+                r[1] = c1 * U0.mx + c2 * Qm1.mx - c3 * dF1;
+                r[2] = c1 * U0.my + c2 * Qm1.my - c3 * dF2;
+                r[3] = c1 * U0.e + c2 * Qm1.e - c3 * dF3;
+            } else {
+                r[0] = c1 * Qm1.d - c2 * dF0;
+                r[1] = c1 * Qm1.mx - c2 * dF1;
+                r[2] = c1 * Qm1.my - c2 * dF2;
+                r[3] = c1 * Qm1.e - c2 * dF3;
             }
-            __syncthreads();
-            Flux5 fx{0, 0, 0, 0, 0};
-            if (do_fx) {
-                hllc<false, kSel>(sXL[0][t - 1], sXL[1][t - 1], sXL[2][t - 1], 0.0, sXL[3][t - 1],
-                                  xr.r, xr.vx, xr.vy, 0.0, xr.p, ph, fx);
-                sF[0][t] = fx.d; sF[1][t] = fx.n; sF[2][t] = fx.t1; sF[3][t] = fx.e;
-            }
-            __syncthreads();
-            if (do_cell) {
-                // update_cons.cpp:38-53: (Fx(i+1)-Fx(i))*dtdx + (Fy(j+1)-Fy(j))*dtdy
-                double dF0 = (sF[0][t + 1] - fx.d) * dtdx + (fy.d - fyPrev.d) * dtdy;
-                double dF1 = (sF[1][t + 1] - fx.n) * dtdx + (fy.t1 - fyPrev.t1) * dtdy;
-                double dF2 = (sF[2][t + 1] - fx.t1) * dtdx + (fy.n - fyPrev.n) * dtdy;
-                double dF3 = (sF[3][t + 1] - fx.e) * dtdx + (fy.e - fyPrev.e) * dtdy;
-                double r[4];
-                if (THREE) {
-                    r[0] = c1 * U0q.d + c2 * Qm1.d - c3 * dF0;
-                    r[1] = c1 * U0q.mx + c2 * Qm1.mx - c3 * dF1;
-                    r[2] = c1 * U0q.my + c2 * Qm1.my - c3 * dF2;
-                    r[3] = c1 * U0q.e + c2 * Qm1.e - c3 * dF3;
-                } else {
-                    r[0] = c1 * Qm1.d - c2 * dF0;
-                    r[1] = c1 * Qm1.mx - c2 * dF1;
-                    r[2] = c1 * Qm1.my - c2 * dF2;
-                    r[3] = c1 * Qm1.e - c2 * dF3;
-                }
-                floors4(r, ph);
-                const long long oc = cbase + (f - 1) * P;
-                out[oc] = r[0];
-                out[vs + oc] = r[1];
-                out[2 * vs + oc] = r[2];
-                out[3 * vs + oc] = r[3];
-            }
+            floors4(r, ph);
+            const long long oc = cbase + (f - 1) * P;
+            out[oc] = r[0];
+            out[vs + oc] = r[1];
+            out[2 * vs + oc] = r[2];
+            out[3 * vs + oc] = r[3];
         }
         fyPrev = fy;
         wlNext = wlNew;
@@ -576,6 +595,7 @@ __global__ void __launch_bounds__(kStageThreads, 3)
     }
 }
 
+
 // ------------------------------------------------------------ launchers
 static inline dim3 cell_grid(const Geom& g, int threads) {
     return dim3((g.nx + threads - 1) / threads, g.ny, g.nz);
@@ -583,11 +603,14 @@ static inline dim3 cell_grid(const Geom& g, int threads) {
 
 void launch_bc(const Ctx& c, double* u, cudaStream_t s) {
     const Geom& g = c.g;
+    // size the grid for the directions that are filled only
     long long m = 0;
-    m = max(m, (long long)g.ng * g.ny * g.nz);
-    m = max(m, (long long)g.ng * g.nx * g.nz);
-    m = max(m, (long long)g.ng * g.nx * g.ny);
-    dim3 grid((unsigned)((m + 127) / 128), 6);
+    if (g.nx > 1) m = max(m, (long long)g.ng * g.ny * g.nz);
+    if (g.ny > 1) m = max(m, (long long)g.ng * g.nx * g.nz);
+    if (g.nz > 1 && c.ph.fill_z) m = max(m, (long long)g.ng * g.nx * g.ny);
+    if (m == 0) return;
+    const int sides = (g.nz > 1 && c.ph.fill_z) ? 6 : 4;
+    dim3 grid((unsigned)((m + 127) / 128), sides);
     k_bc<<<grid, 128, 0, s>>>(u, g, c.ph, c.tm);
 }
 
@@ -627,22 +650,30 @@ void launch_cfl(const Ctx& c, const double* u, int epilogue, cudaStream_t s) {
         k_cfl<false><<<blocks, 256, 0, s>>>(u, g, c.ph, c.tm, epilogue);
 }
 
-void launch_stage2d(const Ctx& c, const double* uc, const double* u0, double* out, int three,
-                    double c1, double c2, double c3, cudaStream_t s) {
+template <int MINB>
+static void launch_stage2d_minb(const Ctx& c, const double* uc, const double* u0, double* out,
+                                int three, double c1, double c2, double c3, cudaStream_t s) {
     const Geom& g = c.g;
     const int rows = c.h2d_rows;
     dim3 grid((g.nx + kStageCols - 1) / kStageCols, (g.ny + rows - 1) / rows);
     if (three) {
         if (c.ph.plm)
-            k_stage2d<true, true><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
+            k_stage2d<true, true, MINB><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
         else
-            k_stage2d<true, false><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
+            k_stage2d<true, false, MINB><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
     } else {
         if (c.ph.plm)
-            k_stage2d<false, true><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
+            k_stage2d<false, true, MINB><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
         else
-            k_stage2d<false, false><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
+            k_stage2d<false, false, MINB><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
     }
+}
+
+// Occupancy target: 3 CTAs/SM (no register cap below 170) or 4 (128 registers).
+void launch_stage2d(const Ctx& c, const double* uc, const double* u0, double* out, int three,
+                    double c1, double c2, double c3, cudaStream_t s) {
+    if (c.stage_minb == 3) launch_stage2d_minb<3>(c, uc, u0, out, three, c1, c2, c3, s);
+    else launch_stage2d_minb<4>(c, uc, u0, out, three, c1, c2, c3, s);
 }
 
 void launch_begin(const Ctx& c, double dtoutput, int steps, cudaStream_t s) {

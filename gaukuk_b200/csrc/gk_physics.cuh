@@ -1,22 +1,70 @@
 // gk_physics.cuh -- pointwise device physics of the finite-volume update.
 //
 // Included inside the mode namespace (gk_parity / gk_fast).  Every
-// expression keeps the reference's association order; the parity unit is
-// compiled with -fmad=false so nothing is contracted, and IEEE double
-// division and sqrt are correctly rounded on the GPU as on the host, which
-// makes the results bit-identical to the reference built without
-// -ffast-math.  The fast unit lets the compiler contract to FMA.
+// expression keeps the reference's association order.  The parity unit is
+// compiled with -fmad=false and uses IEEE division and square root, which
+// are correctly rounded on the GPU as on the host: results are bit-identical
+// to the reference built without -ffast-math.  The fast unit (GK_FASTMATH)
+// lets the compiler contract to FMA and replaces division, reciprocal and
+// square root by the branch-free refinements below.
 #pragma once
 
 // libstdc++ std::max / std::min: max(a,b) = (a<b)?b:a, min(a,b) = (b<a)?b:a.
 __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
 __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
 
-// Reconstruction::VanLeer (reconstruction.hpp:36-42).  The quotient is only
-// formed when it is kept; the result is the same value in every case.
+#if GK_FASTMATH
+// Reciprocal, quotient and square root for finite, positive, normal
+// arguments (densities, pressures, sound speeds, wave-speed differences).
+// Each starts from the hardware approximation (PTX rcp.approx.ftz.f64 /
+// rsqrt.approx.ftz.f64, about 2^-22 relative error) and applies two
+// Newton-Raphson steps, which square the relative error each time:
+//   reciprocal  y' = y + y*(1 - b*y)
+//   rsqrt       y' = y + y*(1/2 - (x/2)*y*y)
+// The square root is x*rsqrt(x) with one Newton correction of the residual
+// x - s*s (Markstein, IBM J. Res. Dev. 34(1), 1990).  The result is within a
+// few ulp of the IEEE value; there is no slow path and no branch.
+__device__ __forceinline__ double rcp_nr(double b) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+    double e = fma(-b, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-b, y, 1.0);
+    return fma(y, e, y);
+}
+__device__ __forceinline__ double rsqrt_nr(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double h = 0.5 * x;
+    double r = fma(-h, y * y, 0.5);
+    y = fma(y, r, y);
+    r = fma(-h, y * y, 0.5);
+    return fma(y, r, y);
+}
+__device__ __forceinline__ double sqrt_nr(double x) {
+    const double y = rsqrt_nr(x);
+    const double s = x * y;
+    const double r = fma(-s, s, x);
+    return fma(r, 0.5 * y, s);
+}
+#define GK_DIV(a, b) ((a) * rcp_nr(b))
+#define GK_RCP(b) rcp_nr(b)
+#define GK_SQRT(x) sqrt_nr(x)
+#else
+#define GK_DIV(a, b) ((a) / (b))
+#define GK_RCP(b) (1.0 / (b))
+#define GK_SQRT(x) sqrt(x)
+#endif
+
+// Reconstruction::VanLeer (reconstruction.hpp:36-42).
 __device__ __forceinline__ double vanleer(double a, double b) {
     double multi = a * b;
+#if GK_FASTMATH
+    double sigma = GK_DIV(2.0 * multi, a + b);
+    return (multi <= 0.0) ? 0.0 : sigma;
+#else
     return (multi <= 0.0) ? 0.0 : (2.0 * multi) / (a + b);
+#endif
 }
 
 struct Flux5 {
@@ -37,14 +85,27 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
                                      double denr, double vxr, double vyr, double vzr, double prer,
                                      const gk::Phys& ph, Flux5& f) {
     const double gamma = ph.gamma;
+#if GK_FASTMATH
+    // sqrt(gamma*p/rho) = (gamma*p) * rsqrt(gamma*p*rho): one root, no quotient
+    const double gpl = gamma * prel, gpr = gamma * prer;
+    double al = gpl * rsqrt_nr(gpl * denl);
+    double ar = gpr * rsqrt_nr(gpr * denr);
+#else
     // EquationOfState::SoundSpeed (eos.hpp:27-29)
     double al = sqrt(gamma * prel / denl);
     double ar = sqrt(gamma * prer / denr);
+#endif
     double prePVRS = 0.5 * (prel + prer) - 0.125 * (vxr - vxl) * (denl + denr) * (al + ar);
     prePVRS = smax(prePVRS, 0.0);
+    double ql, qr;
+#if GK_FASTMATH
+    ql = sqrt_nr(1 + ph.cq * smax(prePVRS * rcp_nr(prel) - 1, 0.0));
+    qr = sqrt_nr(1 + ph.cq * smax(prePVRS * rcp_nr(prer) - 1, 0.0));
+#else
     // q = sqrt(1 + 0.5*(1+1/gamma)*max(p*/p - 1, 0)) is exactly 1 whenever
     // p* <= p with p > 0, so the division and root are skipped there.
-    double ql = 1.0, qr = 1.0;
+    ql = 1.0;
+    qr = 1.0;
     if (!(prePVRS <= prel && prel > 0.0)) {
         double temp = smax(prePVRS / prel - 1, 0.0);
         ql = sqrt(1 + ph.cq * temp);
@@ -53,18 +114,19 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
         double temp = smax(prePVRS / prer - 1, 0.0);
         qr = sqrt(1 + ph.cq * temp);
     }
+#endif
     double sl = vxl - al * ql;
     double sr = vxr + ar * qr;
-    double ss = (prer - prel + denl * vxl * (sl - vxl) - denr * vxr * (sr - vxr)) /
-                (denl * (sl - vxl) - denr * (sr - vxr));
+    double ss = GK_DIV(prer - prel + denl * vxl * (sl - vxl) - denr * vxr * (sr - vxr),
+                       denl * (sl - vxl) - denr * (sr - vxr));
     // EquationOfState::EGas (eos.hpp:30-32) + kinetic energy
     double kl = T2 ? (vxl * vxl + vyl * vyl + vzl * vzl) : (vxl * vxl + vyl * vyl);
     double kr = T2 ? (vxr * vxr + vyr * vyr + vzr * vzr) : (vxr * vxr + vyr * vyr);
     if (!SEL) {
         double el = prel * ph.gm1Rec + 0.5 * denl * kl;
         double er = prer * ph.gm1Rec + 0.5 * denr * kr;
-        double cl = smin(0.0, sl) * (ss - vxl) / (sl - ss);
-        double cr = smax(0.0, sr) * (ss - vxr) / (sr - ss);
+        double cl = GK_DIV(smin(0.0, sl) * (ss - vxl), sl - ss);
+        double cr = GK_DIV(smax(0.0, sr) * (ss - vxr), sr - ss);
         double selectl = (ss >= 0) ? 1.0 : 0.0;
         double selectr = 1.0 - selectl;
         double fl1 = denl * (vxl + cl);
@@ -94,7 +156,7 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
         double k = left ? kl : kr;
         double e = p * ph.gm1Rec + 0.5 * d * k;
         double sc = left ? smin(0.0, s) : smax(0.0, s);
-        double c = sc * (ss - vn) / (s - ss);
+        double c = GK_DIV(sc * (ss - vn), s - ss);
         double f1 = d * (vn + c);
         f.d = f1;
         f.n = d * (vn * vn + c * s) + p;

@@ -157,6 +157,13 @@ int gk_graph_info(gk_handle* h, int* steps_per_graph, int* launches_per_step);
 int gk_profile_steps(gk_handle* h, int nsteps, char* names, int names_cap,
                      double* total_ms, int* launches, int cap, int* n);
 
+/* Diagnostic of the FAST mode arithmetic: the largest error, in ulp of the
+ * IEEE result, of its refined reciprocal, square root and reciprocal square
+ * root against CUDA's IEEE division and sqrt, over n arguments spread over
+ * [2^-60, 2^60] (worst3 = {reciprocal, sqrt, rsqrt}).  Runs on the current
+ * device. */
+int gk_fastmath_check(int n, unsigned long long seed, double* worst3);
+
 /* Text for a status code, and the last failure message on a handle. */
 const char* gk_strerror(int status);
 const char* gk_last_error(const gk_handle* h);

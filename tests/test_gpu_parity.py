@@ -150,3 +150,14 @@ def test_kh4096_two_steps_against_oracle():
     s.run(p.tmax, p.dtoutput)
     assert s.dt_log() == ref_dts
     assert np.array_equal(active(p, s.download()), ref)
+
+
+def test_fastmath_refinements_within_error_bound():
+    """The fast mode's reciprocal / sqrt / rsqrt refinements stay within a few
+    ulp of CUDA's IEEE results over [2^-60, 2^60]."""
+    import ctypes
+    from gaukuk_b200 import _lib
+    L = _lib.load()
+    w = (ctypes.c_double * 3)()
+    _lib.check(L.gk_fastmath_check(1 << 22, 12345, w))
+    assert w[0] <= 2.0 and w[1] <= 2.0 and w[2] <= 2.0, list(w)
