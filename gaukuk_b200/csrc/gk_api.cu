@@ -268,40 +268,42 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
     const double frac13 = 1.0 / 3.0;
     if (c.ph.has_grav) GK_L(gk::K_KICK, k.kick(c, A, s));
     if (h->path == 1) {
+        // the last stage also applies the second half kick, the CFL
+        // reduction and the step epilogue
         GK_L(gk::K_BC, k.bc(c, A, s));
         GK_L(gk::K_STAGE, k.stage2d(c, A, nullptr, B, 0, 1.0, 1.0, 0.0, s));
         GK_L(gk::K_BC, k.bc(c, B, s));
         if (integ == 3) {
             GK_L(gk::K_STAGE, k.stage2d(c, B, A, Cb, 1, 0.75, 0.25, 0.25, s));
             GK_L(gk::K_BC, k.bc(c, Cb, s));
-            GK_L(gk::K_STAGE, k.stage2d(c, Cb, A, A, 1, frac13, 2 * frac13, 2 * frac13, s));
+            GK_L(gk::K_STAGE, k.stage2d(c, Cb, A, A, 2, frac13, 2 * frac13, 2 * frac13, s));
         } else {
-            GK_L(gk::K_STAGE, k.stage2d(c, B, A, A, 1, 0.5, 0.5, 0.5, s));
+            GK_L(gk::K_STAGE, k.stage2d(c, B, A, A, 2, 0.5, 0.5, 0.5, s));
         }
+        return;
+    }
+    auto fluxes = [&](const double* u) {
+        GK_L(gk::K_C2P, k.c2p(c, u, h->W, s));
+        GK_L(gk::K_FLUX, k.flux(c, 0, h->W, h->F1, s));
+        if (c.g.ndim >= 2) GK_L(gk::K_FLUX, k.flux(c, 1, h->W, h->F2, s));
+        if (c.g.ndim == 3) GK_L(gk::K_FLUX, k.flux(c, 2, h->W, h->F3, s));
+    };
+    GK_L(gk::K_BC, k.bc(c, A, s));
+    fluxes(A);
+    if (integ == 1) {
+        GK_L(gk::K_UPDATE, k.update(c, nullptr, A, A, h->F1, h->F2, h->F3, 0, 1.0, 1.0, 0.0, s));
     } else {
-        auto fluxes = [&](const double* u) {
-            GK_L(gk::K_C2P, k.c2p(c, u, h->W, s));
-            GK_L(gk::K_FLUX, k.flux(c, 0, h->W, h->F1, s));
-            if (c.g.ndim >= 2) GK_L(gk::K_FLUX, k.flux(c, 1, h->W, h->F2, s));
-            if (c.g.ndim == 3) GK_L(gk::K_FLUX, k.flux(c, 2, h->W, h->F3, s));
-        };
-        GK_L(gk::K_BC, k.bc(c, A, s));
-        fluxes(A);
-        if (integ == 1) {
-            GK_L(gk::K_UPDATE, k.update(c, nullptr, A, A, h->F1, h->F2, h->F3, 0, 1.0, 1.0, 0.0, s));
-        } else {
-            GK_L(gk::K_UPDATE, k.update(c, nullptr, A, B, h->F1, h->F2, h->F3, 0, 1.0, 1.0, 0.0, s));
+        GK_L(gk::K_UPDATE, k.update(c, nullptr, A, B, h->F1, h->F2, h->F3, 0, 1.0, 1.0, 0.0, s));
+        GK_L(gk::K_BC, k.bc(c, B, s));
+        fluxes(B);
+        if (integ == 3) {
+            GK_L(gk::K_UPDATE, k.update(c, A, B, B, h->F1, h->F2, h->F3, 1, 0.75, 0.25, 0.25, s));
             GK_L(gk::K_BC, k.bc(c, B, s));
             fluxes(B);
-            if (integ == 3) {
-                GK_L(gk::K_UPDATE, k.update(c, A, B, B, h->F1, h->F2, h->F3, 1, 0.75, 0.25, 0.25, s));
-                GK_L(gk::K_BC, k.bc(c, B, s));
-                fluxes(B);
-                GK_L(gk::K_UPDATE, k.update(c, A, B, A, h->F1, h->F2, h->F3, 1, frac13, 2 * frac13,
-                                            2 * frac13, s));
-            } else {
-                GK_L(gk::K_UPDATE, k.update(c, A, B, A, h->F1, h->F2, h->F3, 1, 0.5, 0.5, 0.5, s));
-            }
+            GK_L(gk::K_UPDATE, k.update(c, A, B, A, h->F1, h->F2, h->F3, 1, frac13, 2 * frac13,
+                                        2 * frac13, s));
+        } else {
+            GK_L(gk::K_UPDATE, k.update(c, A, B, A, h->F1, h->F2, h->F3, 1, 0.5, 0.5, 0.5, s));
         }
     }
     if (c.ph.has_grav) GK_L(gk::K_KICK, k.kick(c, A, s));
@@ -426,9 +428,10 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
         GK_CUDA(h, cudaStreamSynchronize(h->stream));
         h->ctx.has_vz = flag;
     }
-    h->path = (g.ndim == 2 && !h->ctx.has_vz && h->ctx.ph.integrator != 1) ? 1 : 0;
+    // (gz != 0 would make MTZ non-zero in the kick, so it also needs the generic path)
+    h->path = (g.ndim == 2 && !h->ctx.has_vz && h->ctx.ph.integrator != 1 &&
+               h->ctx.ph.grav[2] == 0) ? 1 : 0;
     h->ctx.h2d_rows = stage_rows(g);
-    h->ctx.stage_minb = env_int("GK_STAGE_MINB", 4) == 3 ? 3 : 4;
     if (h->path == 0) {
         int rc = alloc_generic(h);
         if (rc != GK_OK) return rc;
@@ -607,10 +610,12 @@ int gk_graph_info(gk_handle* h, int* steps_per_graph, int* launches_per_step) {
     if (!h) return GK_ERR_INVALID;
     const gk::Ctx& c = h->ctx;
     const int stages = c.ph.integrator;  // 1, 2 or 3 stages
-    int per = c.ph.has_grav ? 2 : 0;
-    if (h->path == 1) per += 2 * stages;
-    else per += stages * (3 + c.g.ndim);
-    per += 1;  // CFL + epilogue
+    int per;
+    if (h->path == 1) {
+        per = (c.ph.has_grav ? 1 : 0) + 2 * stages;  // kick, (ghost fill + stage) per stage
+    } else {
+        per = (c.ph.has_grav ? 2 : 0) + stages * (3 + c.g.ndim) + 1;  // + CFL/epilogue
+    }
     if (steps_per_graph) *steps_per_graph = steps_per_graph_of(c.g);
     if (launches_per_step) *launches_per_step = per;
     return GK_OK;

@@ -71,7 +71,6 @@ struct Ctx {
     DevTime* tm;
     int has_vz;      // 2D: MTZ not identically zero -> generic path
     int h2d_rows;    // fused 2D kernel: rows per CTA segment
-    int stage_minb;  // fused 2D kernel: CTAs per SM the register budget targets (3 or 4)
 };
 
 // Kernel classes, for per-kernel profiling.
@@ -95,7 +94,7 @@ static const char* const kClassNames[K_NCLASS] = {
     void launch_kick(const gk::Ctx& c, double* u, cudaStream_t s);                             \
     void launch_cfl(const gk::Ctx& c, const double* u, int epilogue, cudaStream_t s);          \
     void launch_stage2d(const gk::Ctx& c, const double* uc, const double* u0, double* out,     \
-                        int three, double c1, double c2, double c3, cudaStream_t s);           \
+                        int kind, double c1, double c2, double c3, cudaStream_t s);            \
     void launch_begin(const gk::Ctx& c, double dtoutput, int steps, cudaStream_t s);           \
     void launch_mtz_check(const gk::Ctx& c, const double* u, int* flag, cudaStream_t s);       \
     }

@@ -467,11 +467,19 @@ __device__ __forceinline__ void hllc_x(const W4& l, const W4& r, const Phys& ph,
     hllc<false, kSel>(l.r, l.vx, l.vy, 0.0, l.p, r.r, r.vx, r.vy, 0.0, r.p, ph, f);
 }
 
-template <bool THREE, bool PLM, int MINB>
-__global__ void __launch_bounds__(kStageThreads, MINB)
+// KIND 0: u' = c1*uc - c2*dF (stage 1); 1: u' = c1*u0 + c2*uc - c3*dF
+// (later stages); 2: as 1 and the last stage of the step, which also applies
+// the gravity half kick (sim.cpp:89-91), reduces the CFL speed of the new
+// state and, in its last CTA, runs the step epilogue -- the separate kick and
+// CFL passes over the state disappear.
+template <int KIND, bool PLM>
+__global__ void __launch_bounds__(kStageThreads, 3)
     k_stage2d(const double* __restrict__ uc, const double* u0, double* out, Geom g, Phys ph,
-              double c1, double c2, double c3, const DevTime* __restrict__ tm, int rows) {
+              double c1, double c2, double c3, DevTime* tm, int rows) {
+    constexpr bool THREE = KIND >= 1;
+    constexpr bool LAST = KIND == 2;
     if (!tm->active) return;
+    unsigned long long cbest = 0ull;  // CFL speed of this thread's cells (bit pattern)
     __shared__ double sP[4][kStageThreads];
     __shared__ double sXL[4][kStageThreads];
     __shared__ double sF[4][kStageThreads];
@@ -580,6 +588,23 @@ __global__ void __launch_bounds__(kStageThreads, MINB)
                 r[3] = c1 * Qm1.e - c2 * dF3;
             }
             floors4(r, ph);
+            if (LAST) {
+                if (ph.has_grav) {
+                    // SourceTerm::ConstGravity with dt/2 (const_gravity.cpp:28-46)
+                    const double hdt = 0.5 * dt;
+                    if (ph.grav[0] != 0) {
+                        r[3] += r[1] * ph.grav[0] * hdt;
+                        r[1] += r[0] * ph.grav[0] * hdt;
+                    }
+                    if (ph.grav[1] != 0) {
+                        r[3] += r[2] * ph.grav[1] * hdt;
+                        r[2] += r[0] * ph.grav[1] * hdt;
+                    }
+                }
+                const double local = cell_cmax(r[0], r[1], r[2], 0.0, r[3], ph, false);
+                const unsigned long long b = (unsigned long long)__double_as_longlong(local);
+                cbest = b > cbest ? b : cbest;
+            }
             const long long oc = cbase + (f - 1) * P;
             out[oc] = r[0];
             out[vs + oc] = r[1];
@@ -592,6 +617,30 @@ __global__ void __launch_bounds__(kStageThreads, MINB)
         P0 = P1;
         Qm1 = Q0;
         Q0 = Q1;
+    }
+    if (LAST) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long x = __shfl_xor_sync(0xffffffffu, cbest, o);
+            cbest = x > cbest ? x : cbest;
+        }
+        __shared__ unsigned long long wmax[kStageThreads / 32];
+        __shared__ bool last;
+        if ((t & 31) == 0) wmax[t >> 5] = cbest;
+        __syncthreads();
+        if (t == 0) {
+            unsigned long long m = wmax[0];
+            for (int w = 1; w < kStageThreads / 32; ++w) m = wmax[w] > m ? wmax[w] : m;
+            atomicMax(&tm->cmax_acc, m);
+            __threadfence();
+            const unsigned int prev = atomicAdd(&tm->done_ctas, 1u);
+            last = (prev == gridDim.x * gridDim.y - 1);
+        }
+        __syncthreads();
+        if (last && t == 0) {
+            __threadfence();
+            step_epilogue(tm, g, ph, 1);
+        }
     }
 }
 
@@ -650,30 +699,22 @@ void launch_cfl(const Ctx& c, const double* u, int epilogue, cudaStream_t s) {
         k_cfl<false><<<blocks, 256, 0, s>>>(u, g, c.ph, c.tm, epilogue);
 }
 
-template <int MINB>
-static void launch_stage2d_minb(const Ctx& c, const double* uc, const double* u0, double* out,
-                                int three, double c1, double c2, double c3, cudaStream_t s) {
+void launch_stage2d(const Ctx& c, const double* uc, const double* u0, double* out, int kind,
+                    double c1, double c2, double c3, cudaStream_t s) {
     const Geom& g = c.g;
     const int rows = c.h2d_rows;
     dim3 grid((g.nx + kStageCols - 1) / kStageCols, (g.ny + rows - 1) / rows);
-    if (three) {
-        if (c.ph.plm)
-            k_stage2d<true, true, MINB><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
-        else
-            k_stage2d<true, false, MINB><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
+#define GK_STAGE(K, PL) k_stage2d<K, PL><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows)
+    if (c.ph.plm) {
+        if (kind == 0) GK_STAGE(0, true);
+        else if (kind == 1) GK_STAGE(1, true);
+        else GK_STAGE(2, true);
     } else {
-        if (c.ph.plm)
-            k_stage2d<false, true, MINB><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
-        else
-            k_stage2d<false, false, MINB><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows);
+        if (kind == 0) GK_STAGE(0, false);
+        else if (kind == 1) GK_STAGE(1, false);
+        else GK_STAGE(2, false);
     }
-}
-
-// Occupancy target: 3 CTAs/SM (no register cap below 170) or 4 (128 registers).
-void launch_stage2d(const Ctx& c, const double* uc, const double* u0, double* out, int three,
-                    double c1, double c2, double c3, cudaStream_t s) {
-    if (c.stage_minb == 3) launch_stage2d_minb<3>(c, uc, u0, out, three, c1, c2, c3, s);
-    else launch_stage2d_minb<4>(c, uc, u0, out, three, c1, c2, c3, s);
+#undef GK_STAGE
 }
 
 void launch_begin(const Ctx& c, double dtoutput, int steps, cudaStream_t s) {
