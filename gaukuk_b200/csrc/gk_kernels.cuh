@@ -286,12 +286,12 @@ __global__ void k_kick(double* __restrict__ u, Geom g, Phys ph, const DevTime* _
 __device__ __forceinline__ double cell_cmax(double d, double mx, double my, double mz, double e,
                                             const Phys& ph, bool has_z) {
     d = smax(d, ph.dmin);
-    double denInv = 1.0 / d;
+    double denInv = GK_RCP(d);
     double vx = mx * denInv, vy = my * denInv, vz = mz * denInv;
     double engKin = has_z ? 0.5 * (vx * mx + vy * my + vz * mz) : 0.5 * (vx * mx + vy * my);
     double pres = ph.gm1 * (e - engKin);
     pres = (pres > ph.pmin) ? pres : ph.pmin;
-    double cs = sqrt(ph.gamma * pres * denInv);
+    double cs = GK_SQRT(ph.gamma * pres * denInv);
     double local = fabs(vx) + cs;
     local = smax(local, fabs(vy) + cs);
     if (has_z) local = smax(local, fabs(vz) + cs);
