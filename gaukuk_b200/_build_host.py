@@ -1,0 +1,78 @@
+"""Builds the C++ host layer (gaukuk_b200/src) and one driver per problem hook.
+
+* ``lib/libgaukuk_host.a`` -- Config, Grid/Domain, EquationOfState,
+  Boundary, SourceTerm, Sim (whose Advance calls libgk_cuda.so), WriteData.
+* ``bin/gaukuk_<name>.sim`` -- main.cpp + the host library + one problem hook
+  ``src/setup/setup_<name>.cpp``, linked against lib/libgk_cuda.so: the
+  reference's ``gaukuk.sim -i file.in`` with the time loop on the GPU.
+
+The host code is compiled without FMA contraction or fast-math, so a hook
+computes the same initial state bits as the reference built with strict IEEE
+flags.  ``build_hook(path)`` builds a driver for any hook file written for
+the reference -- the hook's own ``#include "../sim.hpp"`` resolves to this
+layer's headers (``-I-`` stops the compiler from looking next to the hook).
+"""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+from typing import List, Optional
+
+from ._build import BIN, CUDA_LIB, INCLUDE, LIB, OBJ, PKG, _newer, _run, build_cuda
+
+SRC = os.path.join(PKG, "src")
+SETUP = os.path.join(SRC, "setup")
+HOST_LIB = os.path.join(LIB, "libgaukuk_host.a")
+CXX = "g++"
+CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
+            "-Wno-unused-variable", "-I" + INCLUDE, "-I" + SRC]
+HOST_SRCS = ["sim.cpp", "utils/read_config.cpp", "utils/write_sim.cpp", "eos/adiabatic.cpp",
+             "boundary/boundary.cpp", "source_term/source.cpp"]
+
+
+def _headers() -> List[str]:
+    return glob.glob(os.path.join(SRC, "**", "*.hpp"), recursive=True) + \
+        glob.glob(os.path.join(INCLUDE, "*.h"))
+
+
+def build_host_lib(verbose: bool = False, force: bool = False) -> str:
+    odir = os.path.join(OBJ, "host")
+    os.makedirs(odir, exist_ok=True)
+    objs = []
+    for rel in HOST_SRCS + ["main.cpp"]:
+        src = os.path.join(SRC, rel)
+        obj = os.path.join(odir, rel.replace("/", "_").replace(".cpp", ".o"))
+        if force or _newer(obj, [src] + _headers()):
+            _run([CXX] + CXXFLAGS + ["-c", src, "-o", obj], verbose)
+        if rel != "main.cpp":
+            objs.append(obj)
+    if force or _newer(HOST_LIB, objs):
+        if os.path.exists(HOST_LIB):
+            os.remove(HOST_LIB)
+        _run(["ar", "rcs", HOST_LIB] + objs, verbose)
+    return HOST_LIB
+
+
+def build_hook(hook_src: str, name: Optional[str] = None, verbose: bool = False,
+               force: bool = False, out_dir: str = BIN) -> str:
+    """Links bin/gaukuk_<name>.sim from main.cpp, the host library and a hook."""
+    build_cuda(verbose=verbose)
+    build_host_lib(verbose=verbose)
+    name = name or os.path.basename(hook_src)[len("setup_"):-len(".cpp")]
+    os.makedirs(out_dir, exist_ok=True)
+    exe = os.path.join(out_dir, f"gaukuk_{name}.sim")
+    main_obj = os.path.join(OBJ, "host", "main.o")
+    if force or _newer(exe, [hook_src, main_obj, HOST_LIB, CUDA_LIB]):
+        # -I- : quote includes of the hook are looked up in -I directories
+        # only, so "../sim.hpp" from a hook file anywhere resolves to src/.
+        cmd = [CXX] + CXXFLAGS + ["-I-", "-I" + SETUP, "-o", exe, hook_src, main_obj, HOST_LIB,
+                                  "-L" + LIB, "-lgk_cuda", "-Wl,-rpath," + LIB]
+        _run(cmd, verbose)
+    return exe
+
+
+def build_host(verbose: bool = False, force: bool = False) -> None:
+    build_host_lib(verbose=verbose, force=force)
+    for hook in sorted(glob.glob(os.path.join(SETUP, "setup_*.cpp"))):
+        build_hook(hook, verbose=verbose, force=force)

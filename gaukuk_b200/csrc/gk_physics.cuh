@@ -99,13 +99,11 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
     prePVRS = smax(prePVRS, 0.0);
     double ql, qr;
 #if GK_FASTMATH
-    // q is 1 unless p* exceeds that side's pressure; neighbouring faces
-    // usually agree (compression vs expansion), so the branch is mostly
-    // uniform across a warp.
-    ql = 1.0;
-    qr = 1.0;
-    if (prePVRS > prel) ql = sqrt_nr(1 + ph.cq * smax(prePVRS * rcp_nr(prel) - 1, 0.0));
-    if (prePVRS > prer) qr = sqrt_nr(1 + ph.cq * smax(prePVRS * rcp_nr(prer) - 1, 0.0));
+    // Branch-free on purpose: a skip when p* <= p (as in parity mode) was
+    // measured slower, because it splits the straight-line code in which the
+    // x- and y-face solves of a row interleave.
+    ql = sqrt_nr(1 + ph.cq * smax(prePVRS * rcp_nr(prel) - 1, 0.0));
+    qr = sqrt_nr(1 + ph.cq * smax(prePVRS * rcp_nr(prer) - 1, 0.0));
 #else
     // q = sqrt(1 + 0.5*(1+1/gamma)*max(p*/p - 1, 0)) is exactly 1 whenever
     // p* <= p with p > 0, so the division and root are skipped there.

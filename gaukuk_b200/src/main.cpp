@@ -1,0 +1,57 @@
+// main.cpp -- gaukuk.sim, the command-line driver, with the reference's
+// interface and output cadence (src/main.cpp:12-65):
+//     gaukuk.sim -i input.in
+// Setup hook -> ghost fill -> frame 0 -> {Advance(dtoutput); frame n} until
+// tmax, then the step count and timings.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <ctime>
+#include <iomanip>
+#include <iostream>
+#include <string>
+
+#include "gaukuk.hpp"
+#include "sim.hpp"
+
+int main(int argc, char* argv[]) {
+    using namespace Gaukuk;
+    if (argc < 3 || std::string(argv[1]) != "-i") {
+        std::cerr << "Usage: " << argv[0] << " -i input.in" << std::endl;
+        return 1;
+    }
+    Config::getInstance().loadFromFile(argv[2]);
+    Real tmax = Config::getInstance().get("tmax");
+    Real dtoutput = Config::getInstance().get("dtoutput");
+
+    Sim sim;
+    sim.Setup();
+    int outputStep = 0;
+    Real tnow = sim.GetTime();
+    sim.boundary.UpdateBD(sim.cons, sim.grid, sim.domain, sim.eos);
+    DataType outputType = DataType::Cons;
+    if (static_cast<int>(Config::getInstance().get("dataType")) == 1) outputType = DataType::Prim;
+    sim.WriteData(outputStep, outputType);
+
+    auto time0 = std::chrono::high_resolution_clock::now();
+    clock_t cpu0 = clock();
+    while (std::abs(tmax - tnow) > 1e-12 && sim.isContinue) {
+        dtoutput = std::min(dtoutput, tmax - tnow);
+        sim.Advance(dtoutput);
+        tnow = sim.GetTime();
+        outputStep++;
+        sim.WriteData(outputStep, outputType);
+        std::cout << "output " << outputStep << std::endl;
+    }
+    auto time1 = std::chrono::high_resolution_clock::now();
+    clock_t cpu1 = clock();
+    Real wall = std::chrono::duration<Real>(time1 - time0).count();
+    Real cpu = double(cpu1 - cpu0) / CLOCKS_PER_SEC;
+    std::cout << std::right << "Finish! "
+              << "\n    total steps = " << std::setw(6) << sim.GetStep()
+              << " , \n    walltime = " << std::setw(8) << std::fixed << std::setprecision(3) << wall
+              << " s, \n    cputime = " << std::setw(8) << std::fixed << std::setprecision(3) << cpu
+              << " s"
+              << "\n-----------------------------------------------------------" << std::endl;
+    return 0;
+}

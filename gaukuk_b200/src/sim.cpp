@@ -1,0 +1,133 @@
+// sim.cpp -- Domain and Sim of the host interface.
+//
+// Domain geometry is the reference's (src/sim.cpp:16-42).  Sim::Sim reads
+// the same keys (sim.cpp:45-67).  Sim::Advance replaces the reference's host
+// loop (sim.cpp:69-117) with one call into libgk_cuda.so: the state is
+// uploaded, the device runs every step up to the output time, and the state
+// comes back into cons.  The per-step log lines the reference prints
+// (sim.cpp:100-103) are printed afterwards from the device's dt log, with
+// t accumulated in the same order, so they read the same.
+#include <algorithm>
+#include <iostream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "gaukuk_cuda.h"
+#include "sim.hpp"
+#include "utils/utils.hpp"
+
+namespace Gaukuk {
+
+Domain::Domain(const Grid& grid)
+    : xmin(Config::getInstance().get("xmin")),
+      xmax(Config::getInstance().get("xmax")),
+      ymin(Config::getInstance().get("ymin")),
+      ymax(Config::getInstance().get("ymax")),
+      zmin(Config::getInstance().get("zmin")),
+      zmax(Config::getInstance().get("zmax")) {
+    dx = (xmax - xmin) / grid.nx;
+    dy = (ymax - ymin) / grid.ny;
+    dz = (zmax - zmin) / grid.nz;
+    dxRec = 1. / dx;
+    dyRec = 1. / dy;
+    dzRec = 1. / dz;
+    if (grid.ny <= 1) dyRec = 0;
+    if (grid.nz <= 1) dzRec = 0;
+    drmin = std::min(std::min(dx, dy), dz);
+    xc.NewArray(grid.lenx);
+    yc.NewArray(grid.leny);
+    zc.NewArray(grid.lenz);
+    for (int i = 0; i < grid.lenx; i++) xc(i) = xmin - grid.nGhost * dx + 0.5 * dx + i * dx;
+    for (int j = 0; j < grid.leny; j++) yc(j) = ymin - grid.nGhost * dy + 0.5 * dy + j * dy;
+    for (int k = 0; k < grid.lenz; k++) zc(k) = zmin - grid.nGhost * dz + 0.5 * dz + k * dz;
+}
+
+Sim::Sim()
+    : isContinue(true), domain(grid), flux(grid.lenx), step(0), t(0), dt(1e10),
+      dtUntilOutput(1e10), cmax(1e-16) {
+    Config& c = Config::getInstance();
+    CFL = c.get("CFL");
+    cons.NewArray(NVar, grid.lenz, grid.leny, grid.lenx);
+    prim.NewArray(NVar, grid.lenz, grid.leny, grid.lenx);
+    integratorType = static_cast<int>(c.get("integrator", 2));
+    rcOrder = static_cast<int>(c.get("RcOrder", 1));
+    stepMax = static_cast<int>(c.get("stepmax", -1));
+    gpuMode_ = static_cast<int>(c.get("gpuMode", 0));
+    gpuDevice_ = static_cast<int>(c.get("gpuDevice", 0));
+}
+
+Sim::~Sim() { gk_destroy(dev_); }
+
+namespace {
+
+void Check(gk_handle* h, int rc, const char* what) {
+    if (rc == GK_OK) return;
+    std::string msg = std::string(what) + ": " + gk_strerror(rc);
+    if (h && *gk_last_error(h)) msg += std::string(" (") + gk_last_error(h) + ")";
+    if (rc == GK_ERR_INVALID) throw std::invalid_argument(msg);
+    throw std::runtime_error(msg);
+}
+
+}  // namespace
+
+void Sim::EnsureDevice() {
+    if (dev_) return;
+    const char* why = boundary.DeviceBlocker();
+    if (*why) throw std::runtime_error(why);
+    if (srcTerm.HasPointGravity())
+        throw std::runtime_error("point/binary gravity is not implemented on the device");
+    gk_grid_desc gd{};
+    gd.nx = grid.nx; gd.ny = grid.ny; gd.nz = grid.nz; gd.nghost = grid.nGhost;
+    gd.xmin = domain.xmin; gd.xmax = domain.xmax;
+    gd.ymin = domain.ymin; gd.ymax = domain.ymax;
+    gd.zmin = domain.zmin; gd.zmax = domain.zmax;
+    gk_phys_desc pd{};
+    pd.gamma = eos.GetGamma();
+    pd.cfl = CFL;
+    pd.integrator = integratorType;
+    pd.rc_order = rcOrder;
+    for (int s = 0; s < 6; ++s) pd.bc[s] = boundary.Type(s);
+    pd.grav[0] = srcTerm.Gx();
+    pd.grav[1] = srcTerm.Gy();
+    pd.grav[2] = srcTerm.Gz();
+    pd.dfloor = DENSITY_FLOOR;
+    pd.pfloor = PRESSURE_FLOOR;
+    pd.stepmax = stepMax;
+    pd.mode = gpuMode_ == 1 ? GK_MODE_FAST : GK_MODE_PARITY;
+    pd.device = gpuDevice_;
+    Check(nullptr, gk_create(&gd, &pd, &dev_), "gk_create");
+}
+
+void Sim::Advance(Real dtoutput) {
+    EnsureDevice();
+    const int step0 = step;
+    const Real t0 = t;
+    Check(dev_, gk_set_time(dev_, t, step), "gk_set_time");
+    Check(dev_, gk_upload_cons(dev_, cons.data()), "gk_upload_cons");
+    double tt = t;
+    int st = step, cont = 1;
+    const int rc = gk_advance(dev_, dtoutput, &tt, &st, &cont);
+    int n = 0;
+    Check(dev_, gk_dt_log(dev_, nullptr, 0, &n), "gk_dt_log");
+    std::vector<double> dts(n);
+    if (n > 0) Check(dev_, gk_dt_log(dev_, dts.data(), n, &n), "gk_dt_log");
+    Real tp = t0;
+    for (int k = 0; k < (int)dts.size(); ++k) {
+        tp += dts[k];
+        std::cout << "step = " << step0 + k + 1 << ", t = " << tp << ", dt = " << dts[k]
+                  << std::endl;
+    }
+    Check(dev_, rc, "gk_advance");
+    Check(dev_, gk_download_cons(dev_, cons.data()), "gk_download_cons");
+    double tdev = 0, dtdev = 0;
+    int sdev = 0, cdev = 1;
+    Check(dev_, gk_get_time(dev_, &tdev, &dtdev, &sdev, &cdev), "gk_get_time");
+    t = tt;
+    step = st;
+    dt = dtdev;
+    isContinue = cont != 0;
+    dtUntilOutput = (t0 + dtoutput) - t;
+}
+
+}  // namespace Gaukuk

@@ -1,0 +1,68 @@
+// sim.hpp -- Sim, the problem object of the host interface.
+//
+// Public members and methods as in the reference (src/sim.hpp:23-58): a
+// setup hook fills prim/cons using grid and domain and may enroll sources
+// or boundaries; main drives Advance / WriteData.  Advance runs the whole
+// time loop on the GPU through the C ABI of include/gaukuk_cuda.h: the state
+// goes to the device at the start of the call and comes back at the end, so
+// cons always holds the current state between calls.
+//
+// Two .in keys beyond the reference's select the device: gpuMode (0 =
+// bit-identical to the reference built with strict IEEE flags, the default;
+// 1 = fast mode, within 1e-12) and gpuDevice (CUDA ordinal, default 0).
+#pragma once
+
+#include <cstddef>
+
+#include "boundary/boundary.hpp"
+#include "eos/eos.hpp"
+#include "flux/flux.hpp"
+#include "gaukuk.hpp"
+#include "grid.hpp"
+#include "source_term/source.hpp"
+#include "template_array.hpp"
+
+struct gk_handle;
+
+namespace Gaukuk {
+
+enum class DataType { Prim, Cons };
+
+class Sim {
+public:
+    Sim();
+    ~Sim();
+    Sim(const Sim&) = delete;
+    Sim& operator=(const Sim&) = delete;
+
+    bool isContinue;
+    const Grid grid;
+    const Domain domain;
+    Flux flux;
+
+    TArray<Real> cons, prim;
+    // Face fluxes live on the device; these stay unallocated.
+    TArray<Real> flx1, flx2, flx3;
+
+    EquationOfState eos;
+    Boundary boundary;
+    SourceTerm srcTerm;
+
+    void Setup();
+    void Advance(Real dtoutput);
+    void WriteData(const int outputID, DataType dType);
+
+    Real GetTime() { return t; }
+    Real Getdt() { return dt; }
+    int GetStep() { return step; }
+
+private:
+    int step, stepMax;
+    Real t, dt, dtUntilOutput, cmax, CFL;
+    int rcOrder, integratorType;
+    int gpuMode_, gpuDevice_;
+    gk_handle* dev_ = nullptr;
+    void EnsureDevice();
+};
+
+}  // namespace Gaukuk
