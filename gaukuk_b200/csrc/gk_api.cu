@@ -77,6 +77,7 @@ struct gk_handle {
     int* dflag = nullptr;
     int path = 0;  // 0 generic, 1 fused 2D
     bool uploaded = false;
+    int upload_step = 0;  // clock step at the last upload
     cudaGraphExec_t gexec = nullptr;
     int graph_steps = 0;
     int graph_path = -1;
@@ -453,6 +454,7 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
     rc = pull_time(h);
     if (rc != GK_OK) return rc;
     h->uploaded = true;
+    h->upload_step = h->htm->step;
     if (h->htm->status) return fail(h, GK_ERR_NONFINITE, "non-finite state in the uploaded array");
     return GK_OK;
 }
@@ -461,6 +463,8 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
     int rc = check_ready(h);
     if (rc != GK_OK) return rc;
     if (!cons) return GK_ERR_INVALID;
+    rc = pull_time(h);
+    if (rc != GK_OK) return rc;
     const gk::Geom& g = h->ctx.g;
     for (int n = 0; n < 5; ++n) {
         for (int kk = 0; kk < g.nzs; ++kk) {
@@ -470,6 +474,59 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
             GK_CUDA(h, cudaMemcpy2DAsync(dst, sizeof(double) * g.lenx, src, sizeof(double) * g.pitch,
                                          sizeof(double) * g.lenx, g.leny, cudaMemcpyDeviceToHost,
                                          h->stream));
+        }
+    }
+    // Ghost strips as the reference leaves them after a step: Sim's integrators
+    // end with cons.Swap(consTemp) (rk2.cpp:21, rk3.cpp:27), so the written
+    // array carries the ghost fill of the last intermediate stage state.  That
+    // fill sits in the stage buffer (B, or C for the fused RK3 path); the
+    // strips of active rows/columns are taken from there.  Euler runs in place
+    // and 1D y rows follow the reference's in-place order, so both keep A's.
+    const double* donor = nullptr;
+    if (h->htm->step > h->upload_step && h->ctx.ph.integrator != 1)
+        donor = (h->path == 1 && h->ctx.ph.integrator == 3) ? h->C : h->B;
+    if (donor) {
+        const size_t rowb = sizeof(double) * g.lenx, prow = sizeof(double) * g.pitch;
+        for (int n = 0; n < 5; ++n) {
+            for (int kk = 0; kk < g.nzs; ++kk) {
+                const int k = g.kofs + kk;
+                if (k < g.kb || k >= g.ke) continue;
+                double* dst = cons + ((size_t)(n * g.lenz + k) * g.leny) * g.lenx;
+                const double* src = donor + (size_t)kSlotOf[n] * g.vstride + (size_t)kk * g.kstride;
+                if (g.nx > 1) {
+                    for (int side = 0; side < 2; ++side) {
+                        const int i0 = side == 0 ? 0 : g.ie;
+                        GK_CUDA(h, cudaMemcpy2DAsync(dst + (size_t)g.jb * g.lenx + i0, rowb,
+                                                     src + (size_t)g.jb * g.pitch + i0, prow,
+                                                     sizeof(double) * g.ng, g.ny,
+                                                     cudaMemcpyDeviceToHost, h->stream));
+                    }
+                }
+                if (g.ny > 1) {
+                    for (int side = 0; side < 2; ++side) {
+                        const int j0 = side == 0 ? 0 : g.je;
+                        GK_CUDA(h, cudaMemcpy2DAsync(dst + (size_t)j0 * g.lenx + g.ib, rowb,
+                                                     src + (size_t)j0 * g.pitch + g.ib, prow,
+                                                     sizeof(double) * g.nx, g.ng,
+                                                     cudaMemcpyDeviceToHost, h->stream));
+                    }
+                }
+            }
+            if (g.nz > 1) {
+                for (int side = 0; side < 2; ++side) {
+                    if (!((h->ctx.ph.fill_z >> side) & 1)) continue;
+                    for (int gi = 0; gi < g.ng; ++gi) {
+                        const int k = side == 0 ? gi : g.ke + gi;
+                        double* dst = cons + ((size_t)(n * g.lenz + k) * g.leny) * g.lenx;
+                        const double* src = donor + (size_t)kSlotOf[n] * g.vstride +
+                                            (size_t)(k - g.kofs) * g.kstride;
+                        GK_CUDA(h, cudaMemcpy2DAsync(dst + (size_t)g.jb * g.lenx + g.ib, rowb,
+                                                     src + (size_t)g.jb * g.pitch + g.ib, prow,
+                                                     sizeof(double) * g.nx, g.ny,
+                                                     cudaMemcpyDeviceToHost, h->stream));
+                    }
+                }
+            }
         }
     }
     if (g.nzs == 1 && zero_other_planes) {
