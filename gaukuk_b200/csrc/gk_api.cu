@@ -735,3 +735,21 @@ const char* gk_strerror(int status) {
 const char* gk_last_error(const gk_handle* h) { return h ? h->err.c_str() : ""; }
 
 }  // extern "C"
+
+// Context of a descriptor pair without a handle, for entry points that take
+// caller-owned buffers (gk_noalloc.cu).  Returns a GK_* status; *err gets
+// the reason on failure.
+int gk_internal_build_ctx(const gk_grid_desc* gd, const gk_phys_desc* pd, gk::Ctx* ctx,
+                          std::string* err) {
+    gk_handle tmp;
+    tmp.gd = *gd;
+    tmp.pd = *pd;
+    const int rc = build_ctx(&tmp);
+    if (rc != GK_OK) {
+        if (err) *err = tmp.err;
+        return rc;
+    }
+    tmp.ctx.h2d_rows = stage_rows(tmp.ctx.g);
+    *ctx = tmp.ctx;
+    return GK_OK;
+}

@@ -164,6 +164,31 @@ int gk_profile_steps(gk_handle* h, int nsteps, char* names, int names_cap,
  * device. */
 int gk_fastmath_check(int n, unsigned long long seed, double* worst3);
 
+/* One RK2 time step of a 2D problem (vz = 0, gz = 0) on a caller-owned
+ * device state, for callers that cannot allocate device memory while they
+ * run: their memory comes from their own pool or arena, or their budget is
+ * fixed at start-up.  No counterpart in the reference; the arithmetic is
+ * that of gk_run_steps with one step.  Nothing is allocated: the
+ * intermediate stage state and the device clock live in one fixed 64 MiB
+ * array inside the library, held by every GPU that loads it until the
+ * process exits, so grids whose stage state exceeds it (more than about
+ * 1440 x 1440 cells) are rejected with GK_ERR_INVALID.
+ *
+ * state: the device layout of the library -- five planes DEN, MTX, MTY, ENG,
+ * MTZ, each leny rows of `pitch` doubles (lenx rounded up to a multiple of
+ * 16), ghost columns and rows included; MTZ must be zero.  It is updated in
+ * place; its ghost cells are overwritten by the boundary fill.
+ * dt = min(CFL*drmin/cmax(state), dtmax) as in Sim::Advance (sim.cpp:77-81);
+ * *dt_used (host, may be NULL) receives it.  stream: a cudaStream_t or NULL;
+ * the call returns after that stream synchronises.
+ *
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture.  The array is shared by every call and keeps the
+ * last call's contents (the clock is reset on entry): calls whose work
+ * overlaps on one GPU race on it. */
+int gk_rk2_step_noalloc(const gk_grid_desc* grid, const gk_phys_desc* phys, double* state,
+                        double dtmax, double* dt_used, void* stream);
+
 /* Text for a status code, and the last failure message on a handle. */
 const char* gk_strerror(int status);
 const char* gk_last_error(const gk_handle* h);

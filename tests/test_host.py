@@ -50,7 +50,7 @@ def test_noise_is_counter_based():
 def _header_symbols():
     with open(os.path.join(ROOT, "include", "gaukuk_cuda.h")) as f:
         text = f.read()
-    return sorted(set(re.findall(r"\b(gk_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(gk_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_cabi_library_exports_every_declared_symbol():
