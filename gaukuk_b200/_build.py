@@ -71,7 +71,7 @@ def build_cuda(verbose: bool = False, force: bool = False) -> str:
         if force or _newer(obj, [src] + headers):
             _run([NVCC] + NVCC_FLAGS + flags + ["-c", src, "-o", obj], verbose)
     if force or _newer(CUDA_LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", CUDA_LIB] + objs + ["-lcuda"], verbose)
+        _run([NVCC] + ARCH + ["-shared", "-o", CUDA_LIB] + objs, verbose)
     return CUDA_LIB
 
 

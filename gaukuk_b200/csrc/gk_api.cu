@@ -433,6 +433,7 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
     h->path = (g.ndim == 2 && !h->ctx.has_vz && h->ctx.ph.integrator != 1 &&
                h->ctx.ph.grav[2] == 0) ? 1 : 0;
     h->ctx.h2d_rows = stage_rows(g);
+    h->ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
     if (h->path == 0) {
         int rc = alloc_generic(h);
         if (rc != GK_OK) return rc;
@@ -750,6 +751,7 @@ int gk_internal_build_ctx(const gk_grid_desc* gd, const gk_phys_desc* pd, gk::Ct
         return rc;
     }
     tmp.ctx.h2d_rows = stage_rows(tmp.ctx.g);
+    tmp.ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
     *ctx = tmp.ctx;
     return GK_OK;
 }

@@ -63,7 +63,7 @@ struct DevTime {
     double* log;                      // dt of each step
 };
 
-enum { STATUS_NONFINITE = 1 };
+enum { STATUS_NONFINITE = 1, STATUS_TMA_TIMEOUT = 2 };
 
 struct Ctx {
     Geom g;
@@ -71,6 +71,7 @@ struct Ctx {
     DevTime* tm;
     int has_vz;      // 2D: MTZ not identically zero -> generic path
     int h2d_rows;    // fused 2D kernel: rows per CTA segment
+    int use_tma;     // fused 2D kernel: rows staged in shared memory by TMA
 };
 
 // Kernel classes, for per-kernel profiling.

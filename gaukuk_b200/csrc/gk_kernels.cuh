@@ -15,9 +15,13 @@
 // Sim::Advance on the device clock (DevTime).
 #pragma once
 
-#include <cfloat>
-#include <cstdio>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <math_constants.h>
+
+#include <cfloat>
+#include <cstdint>
+#include <cstdio>
 
 #include "gk_internal.h"
 
@@ -645,6 +649,290 @@ __global__ void __launch_bounds__(kStageThreads, 3)
 }
 
 
+
+// ------------------------------------------------------------ fused 2D stage, TMA rows
+// The same stage with its input rows staged in shared memory by the tensor
+// memory accelerator instead of registers.  One cp.async.bulk.tensor load
+// brings a 3D box of 128 columns x 1 row x 4 variable planes (4 KB) into a
+// ring slot; an mbarrier per slot counts its bytes.  Raw rows run four
+// ahead of the row being converted (ring of 6: rows f-2 .. f+3 live); the
+// RK base state u0 runs three ahead (ring of 4).  A slot is refilled only
+// after the barrier that follows its last read, behind a proxy fence.  The
+// box origin is column 124*blockIdx.x, a multiple of 16 bytes; columns past
+// the last one read as zero (TMA out-of-bounds fill) and feed only halo lanes.
+// Waits are bounded: a wait that gives up sets STATUS_TMA_TIMEOUT and the
+// kernel carries on, so it cannot hang.
+constexpr int kRing = 6;
+constexpr int kRing0 = 4;
+constexpr unsigned kRowBytes = 4u * kStageThreads * sizeof(double);
+constexpr int kRowDoubles = 4 * kStageThreads;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tma_row(double* dst, const CUtensorMap* map, int x, int y,
+                                        uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(kRowBytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"((unsigned long long)map), "r"(x), "r"(y), "r"(0), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned phase, int* status) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(phase)
+            : "memory");
+        if (ok) return;
+    }
+    atomicOr(status, gk::STATUS_TMA_TIMEOUT);
+}
+
+template <int KIND, bool PLM>
+__global__ void __launch_bounds__(kStageThreads, 4)
+    k_stage2d_tma(const __grid_constant__ CUtensorMap mapc, const __grid_constant__ CUtensorMap map0,
+                  double* out, Geom g, Phys ph, double c1, double c2, double c3, DevTime* tm,
+                  int rows) {
+    constexpr bool THREE = KIND >= 1;
+    constexpr bool LAST = KIND == 2;
+    if (!tm->active) return;
+    extern __shared__ __align__(128) double dyn[];
+    double* ring = dyn;                          // [kRing][4][128]
+    double* ring0 = dyn + kRing * kRowDoubles;   // [kRing0][4][128]
+    __shared__ __align__(8) uint64_t bar[kRing];
+    __shared__ __align__(8) uint64_t bar0[kRing0];
+    __shared__ double sP[4][kStageThreads];
+    __shared__ double sXL[4][kStageThreads];
+    __shared__ double sF[4][kStageThreads];
+    unsigned long long cbest = 0ull;
+
+    const double dt = tm->dt;
+    const double dtdx = dt * g.dxRec, dtdy = dt * g.dyRec;
+    const int t = threadIdx.x;
+    const int tl = t > 0 ? t - 1 : 0;
+    const int tr = t < kStageThreads - 1 ? t + 1 : t;
+    const int x0 = g.ib - 2 + blockIdx.x * kStageCols;  // box origin column
+    const int xi = x0 + t;
+    const bool do_cell = t >= 2 && t <= kStageThreads - 3 && xi < g.ie;
+    const int y0 = g.jb + blockIdx.y * rows;
+    const int y1 = min(y0 + rows, g.je);
+    const int rlo = y0 - 2;
+    const long long vs = g.vstride;
+    const long long P = g.pitch;
+    const long long cbase = sidx(g, g.kb, 0, xi < g.lenx ? xi : g.lenx - 1);
+    int* status = &tm->status;
+
+    auto slot = [&](int r) { return (r - rlo) % kRing; };
+    auto slot0 = [&](int r) { return (r - y0) % kRing0; };
+    auto issue = [&](int r) { tma_row(ring + slot(r) * kRowDoubles, &mapc, x0, r, &bar[slot(r)]); };
+    auto issue0 = [&](int r) {
+        tma_row(ring0 + slot0(r) * kRowDoubles, &map0, x0, r, &bar0[slot0(r)]);
+    };
+    auto wait = [&](int r) { mbar_wait(&bar[slot(r)], (unsigned)(((r - rlo) / kRing) & 1), status); };
+    auto wait0 = [&](int r) {
+        mbar_wait(&bar0[slot0(r)], (unsigned)(((r - y0) / kRing0) & 1), status);
+    };
+    auto rowq = [&](int r) {
+        const double* p = ring + slot(r) * kRowDoubles;
+        return Q4{p[t], p[kStageThreads + t], p[2 * kStageThreads + t], p[3 * kStageThreads + t]};
+    };
+    auto rowq0 = [&](int r) {
+        const double* p = ring0 + slot0(r) * kRowDoubles;
+        return Q4{p[t], p[kStageThreads + t], p[2 * kStageThreads + t], p[3 * kStageThreads + t]};
+    };
+
+    if (t == 0) {
+        for (int i = 0; i < kRing; ++i) mbar_init(&bar[i], 1);
+        for (int i = 0; i < kRing0; ++i) mbar_init(&bar0[i], 1);
+        fence_proxy_async();
+    }
+    __syncthreads();
+    if (t == 0) {
+        for (int r = rlo; r <= min(y0 + 3, y1 + 1); ++r) issue(r);
+        if (THREE)
+            for (int r = y0; r <= min(y0 + 2, y1 - 1); ++r) issue0(r);
+    }
+
+    // prologue: primitives of rows y0-2, y0-1, y0
+    wait(y0 - 2);
+    const W4 Pm2 = c2p4(rowq(y0 - 2), ph);
+    wait(y0 - 1);
+    W4 Pm1 = c2p4(rowq(y0 - 1), ph);
+    wait(y0);
+    W4 P0 = c2p4(rowq(y0), ph);
+    W4 wlNext = PLM ? plus_half(Pm1, vl4(Pm2, Pm1, P0)) : Pm1;
+    Flux5 fyPrev;
+    {
+        // y face y0
+        wait(y0 + 1);
+        const W4 P1 = c2p4(rowq(y0 + 1), ph);
+        __syncthreads();  // rows y0-2 is read by all: its slot may be refilled
+        if (t == 0 && y0 + 4 <= y1 + 1) {
+            fence_proxy_async();
+            issue(y0 + 4);
+        }
+        W4 wr = P0, wlNew = P0;
+        if (PLM) {
+            const W4 s = vl4(Pm1, P0, P1);
+            wr = minus_half(P0, s);
+            wlNew = plus_half(P0, s);
+        }
+        hllc_y(wlNext, wr, ph, fyPrev);
+        wlNext = wlNew;
+        Pm1 = P0;
+        P0 = P1;
+    }
+
+    for (int f = y0 + 1; f <= y1; ++f) {
+        wait(f + 1);
+        const W4 P1 = c2p4(rowq(f + 1), ph);
+        sP[0][t] = Pm1.r; sP[1][t] = Pm1.vx; sP[2][t] = Pm1.vy; sP[3][t] = Pm1.p;
+        __syncthreads();
+        if (t == 0) {
+            // rows f-2 (raw) and f-2 (base state) were last read in iteration f-1
+            fence_proxy_async();
+            if (f + 4 <= y1 + 1) issue(f + 4);
+            if (THREE && f + 2 <= y1 - 1) issue0(f + 2);
+        }
+        W4 xr = Pm1, wr = P0, wlNew = P0;
+        if (PLM) {
+            const W4 a{sP[0][tl], sP[1][tl], sP[2][tl], sP[3][tl]};
+            const W4 c{sP[0][tr], sP[1][tr], sP[2][tr], sP[3][tr]};
+            const W4 sx = vl4(a, Pm1, c);
+            const W4 sy = vl4(Pm1, P0, P1);
+            const W4 xlft = plus_half(Pm1, sx);
+            xr = minus_half(Pm1, sx);
+            wr = minus_half(P0, sy);
+            wlNew = plus_half(P0, sy);
+            sXL[0][t] = xlft.r; sXL[1][t] = xlft.vx; sXL[2][t] = xlft.vy; sXL[3][t] = xlft.p;
+        } else {
+            sXL[0][t] = Pm1.r; sXL[1][t] = Pm1.vx; sXL[2][t] = Pm1.vy; sXL[3][t] = Pm1.p;
+        }
+        __syncthreads();
+        const W4 xl_state{sXL[0][tl], sXL[1][tl], sXL[2][tl], sXL[3][tl]};
+        Flux5 fx, fy;
+        hllc_x(xl_state, xr, ph, fx);
+        hllc_y(wlNext, wr, ph, fy);
+        sF[0][t] = fx.d; sF[1][t] = fx.n; sF[2][t] = fx.t1; sF[3][t] = fx.e;
+        __syncthreads();
+        if (do_cell) {
+            const Q4 Qm1 = rowq(f - 1);
+            double dF0 = (sF[0][tr] - fx.d) * dtdx + (fy.d - fyPrev.d) * dtdy;
+            double dF1 = (sF[1][tr] - fx.n) * dtdx + (fy.t1 - fyPrev.t1) * dtdy;
+            double dF2 = (sF[2][tr] - fx.t1) * dtdx + (fy.n - fyPrev.n) * dtdy;
+            double dF3 = (sF[3][tr] - fx.e) * dtdx + (fy.e - fyPrev.e) * dtdy;
+            double r[4];
+            if (THREE) {
+                wait0(f - 1);
+                const Q4 U0 = rowq0(f - 1);
+                r[0] = c1 * U0.d + c2 * Qm1.d - c3 * dF0;
+                r[1] = c1 * U0.mx + c2 * Qm1.mx - c3 * dF1;
+                r[2] = c1 * U0.my + c2 * Qm1.my - c3 * dF2;
+                r[3] = c1 * U0.e + c2 * Qm1.e - c3 * dF3;
+            } else {
+                r[0] = c1 * Qm1.d - c2 * dF0;
+                r[1] = c1 * Qm1.mx - c2 * dF1;
+                r[2] = c1 * Qm1.my - c2 * dF2;
+                r[3] = c1 * Qm1.e - c2 * dF3;
+            }
+            floors4(r, ph);
+            if (LAST) {
+                if (ph.has_grav) {
+                    const double hdt = 0.5 * dt;
+                    if (ph.grav[0] != 0) {
+                        r[3] += r[1] * ph.grav[0] * hdt;
+                        r[1] += r[0] * ph.grav[0] * hdt;
+                    }
+                    if (ph.grav[1] != 0) {
+                        r[3] += r[2] * ph.grav[1] * hdt;
+                        r[2] += r[0] * ph.grav[1] * hdt;
+                    }
+                }
+                const double local = cell_cmax(r[0], r[1], r[2], 0.0, r[3], ph, false);
+                const unsigned long long b = (unsigned long long)__double_as_longlong(local);
+                cbest = b > cbest ? b : cbest;
+            }
+            const long long oc = cbase + (f - 1) * P;
+            out[oc] = r[0];
+            out[vs + oc] = r[1];
+            out[2 * vs + oc] = r[2];
+            out[3 * vs + oc] = r[3];
+        } else if (THREE) {
+            wait0(f - 1);  // every lane keeps the base-state ring in step
+        }
+        fyPrev = fy;
+        wlNext = wlNew;
+        Pm1 = P0;
+        P0 = P1;
+    }
+    if (LAST) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long x = __shfl_xor_sync(0xffffffffu, cbest, o);
+            cbest = x > cbest ? x : cbest;
+        }
+        __shared__ unsigned long long wmax[kStageThreads / 32];
+        __shared__ bool last;
+        if ((t & 31) == 0) wmax[t >> 5] = cbest;
+        __syncthreads();
+        if (t == 0) {
+            unsigned long long m = wmax[0];
+            for (int w = 1; w < kStageThreads / 32; ++w) m = wmax[w] > m ? wmax[w] : m;
+            atomicMax(&tm->cmax_acc, m);
+            __threadfence();
+            const unsigned int prev = atomicAdd(&tm->done_ctas, 1u);
+            last = (prev == gridDim.x * gridDim.y - 1);
+        }
+        __syncthreads();
+        if (last && t == 0) {
+            __threadfence();
+            step_epilogue(tm, g, ph, 1);
+        }
+    }
+}
+
+// Tensor map of the four evolved planes of a state buffer: dims (pitch,
+// leny, 4) doubles, box (128, 1, 4), no swizzle, zero fill out of bounds.
+static bool encode_rows_map(CUtensorMap* map, const double* base, const Geom& g) {
+    cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)g.leny, 4};
+    cuuint64_t strides[2] = {(cuuint64_t)g.pitch * sizeof(double),
+                             (cuuint64_t)g.vstride * sizeof(double)};
+    cuuint32_t box[3] = {(cuuint32_t)kStageThreads, 1, 4};
+    cuuint32_t estr[3] = {1, 1, 1};
+    // resolved through the runtime so the library carries no link-time
+    // dependency on the driver library
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return false;
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                                        const_cast<double*>(base), dims, strides, box, estr,
+                                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 // ------------------------------------------------------------ launchers
 static inline dim3 cell_grid(const Geom& g, int threads) {
     return dim3((g.nx + threads - 1) / threads, g.ny, g.nz);
@@ -699,10 +987,45 @@ void launch_cfl(const Ctx& c, const double* u, int epilogue, cudaStream_t s) {
         k_cfl<false><<<blocks, 256, 0, s>>>(u, g, c.ph, c.tm, epilogue);
 }
 
+template <int KIND, bool PLM>
+static void launch_stage2d_tma(const Ctx& c, const CUtensorMap& mc, const CUtensorMap& m0,
+                               double* out, double c1, double c2, double c3, cudaStream_t s) {
+    const Geom& g = c.g;
+    const int rows = c.h2d_rows;
+    dim3 grid((g.nx + kStageCols - 1) / kStageCols, (g.ny + rows - 1) / rows);
+    const size_t dyn = (size_t)(kRing + (KIND >= 1 ? kRing0 : 0)) * kRowBytes;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_stage2d_tma<KIND, PLM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dyn);
+        attr_set = true;
+    }
+    k_stage2d_tma<KIND, PLM><<<grid, kStageThreads, dyn, s>>>(mc, m0, out, g, c.ph, c1, c2, c3,
+                                                              c.tm, rows);
+}
+
 void launch_stage2d(const Ctx& c, const double* uc, const double* u0, double* out, int kind,
                     double c1, double c2, double c3, cudaStream_t s) {
     const Geom& g = c.g;
     const int rows = c.h2d_rows;
+    if (c.use_tma) {
+        CUtensorMap mc, m0;
+        if (encode_rows_map(&mc, uc, g) && encode_rows_map(&m0, u0 ? u0 : uc, g)) {
+#define GK_TMA(K, PL) launch_stage2d_tma<K, PL>(c, mc, m0, out, c1, c2, c3, s)
+            if (c.ph.plm) {
+                if (kind == 0) GK_TMA(0, true);
+                else if (kind == 1) GK_TMA(1, true);
+                else GK_TMA(2, true);
+            } else {
+                if (kind == 0) GK_TMA(0, false);
+                else if (kind == 1) GK_TMA(1, false);
+                else GK_TMA(2, false);
+            }
+#undef GK_TMA
+            return;
+        }
+        std::fprintf(stderr, "gaukuk: tensor map encoding failed; using register-staged rows\n");
+    }
     dim3 grid((g.nx + kStageCols - 1) / kStageCols, (g.ny + rows - 1) / rows);
 #define GK_STAGE(K, PL) k_stage2d<K, PL><<<grid, kStageThreads, 0, s>>>(uc, u0, out, g, c.ph, c1, c2, c3, c.tm, rows)
     if (c.ph.plm) {
