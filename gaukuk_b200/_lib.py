@@ -59,6 +59,16 @@ SIGNATURES = {
     "gk_fastmath_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_ulonglong, _dp]),
     "gk_rk2_step_noalloc": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(PhysDesc),
                                            _vp, ctypes.c_double, _dp, _vp]),
+    "gk_set_tiling": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "gk_ens_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_void_p)]),
+    "gk_ens_destroy": (None, [_vp]),
+    "gk_ens_set_tiling": (ctypes.c_int, [_vp, ctypes.c_int, _ip]),
+    "gk_ens_advance": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "gk_ens_run_steps": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "gk_ens_enqueue_steps": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "gk_ens_info": (ctypes.c_int, [_vp, _ip, _ip, ctypes.POINTER(ctypes.c_void_p)]),
+    "gk_ens_last_error": (ctypes.c_char_p, [_vp]),
     "gk_strerror": (ctypes.c_char_p, [ctypes.c_int]),
     "gk_last_error": (ctypes.c_char_p, [_vp]),
 }

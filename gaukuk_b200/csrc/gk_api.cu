@@ -17,12 +17,42 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "gaukuk_cuda.h"
 #include "gk_internal.h"
 
 namespace gk_fast {
 int fastmath_check(int n, unsigned long long seed, double* host_worst3);
 }
+
+namespace gk {
+
+bool encode_rows_map(CUtensorMap* map, const double* base, const Geom& g, int nt) {
+    // resolved through the runtime so the library has no link-time dependency
+    // on the driver library
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return false;
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)g.leny, 4};
+    cuuint64_t strides[2] = {(cuuint64_t)g.pitch * sizeof(double),
+                             (cuuint64_t)g.vstride * sizeof(double)};
+    cuuint32_t box[3] = {(cuuint32_t)nt, 1, 4};
+    cuuint32_t estr[3] = {1, 1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace gk
 
 namespace {
 
@@ -36,16 +66,21 @@ struct KernelSet {
     decltype(&gk_parity::launch_stage2d) stage2d;
     decltype(&gk_parity::launch_begin) begin;
     decltype(&gk_parity::launch_mtz_check) mtz_check;
+    decltype(&gk_parity::launch_ens_stage) ens_stage;
+    decltype(&gk_parity::launch_ens_bc) ens_bc;
+    decltype(&gk_parity::launch_ens_begin) ens_begin;
 };
 
 const KernelSet kParity = {gk_parity::launch_bc,     gk_parity::launch_c2p,
                            gk_parity::launch_flux,   gk_parity::launch_update,
                            gk_parity::launch_kick,   gk_parity::launch_cfl,
                            gk_parity::launch_stage2d, gk_parity::launch_begin,
-                           gk_parity::launch_mtz_check};
+                           gk_parity::launch_mtz_check, gk_parity::launch_ens_stage,
+                           gk_parity::launch_ens_bc,  gk_parity::launch_ens_begin};
 const KernelSet kFast = {gk_fast::launch_bc,     gk_fast::launch_c2p,     gk_fast::launch_flux,
                          gk_fast::launch_update, gk_fast::launch_kick,    gk_fast::launch_cfl,
-                         gk_fast::launch_stage2d, gk_fast::launch_begin,  gk_fast::launch_mtz_check};
+                         gk_fast::launch_stage2d, gk_fast::launch_begin,  gk_fast::launch_mtz_check,
+                         gk_fast::launch_ens_stage, gk_fast::launch_ens_bc, gk_fast::launch_ens_begin};
 
 constexpr int kLogCap = 1 << 20;
 
@@ -78,6 +113,8 @@ struct gk_handle {
     int path = 0;  // 0 generic, 1 fused 2D
     bool uploaded = false;
     int upload_step = 0;  // clock step at the last upload
+    bool tiling_set = false;  // gk_set_tiling overrides the default tiling
+    int tiling_rows = 0;
     cudaGraphExec_t gexec = nullptr;
     int graph_steps = 0;
     int graph_path = -1;
@@ -226,6 +263,13 @@ int alloc_generic(gk_handle* h) {
 int env_int(const char* name, int dflt) {
     const char* v = std::getenv(name);
     return v && *v ? std::atoi(v) : dflt;
+}
+
+// Threads per CTA of the TMA stage kernel: 128 unless GK_STAGE_THREADS says
+// 64 or 256 (tuning).
+int stage_threads_default() {
+    const int v = env_int("GK_STAGE_THREADS", 128);
+    return (v == 64 || v == 256) ? v : 128;
 }
 
 // Rows per CTA segment of the fused kernel.  Short segments (16 rows) give
@@ -434,6 +478,8 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
                h->ctx.ph.grav[2] == 0) ? 1 : 0;
     h->ctx.h2d_rows = stage_rows(g);
     h->ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
+    if (!h->tiling_set) h->ctx.stage_threads = stage_threads_default();
+    else h->ctx.h2d_rows = h->tiling_rows;
     if (h->path == 0) {
         int rc = alloc_generic(h);
         if (rc != GK_OK) return rc;
@@ -752,6 +798,247 @@ int gk_internal_build_ctx(const gk_grid_desc* gd, const gk_phys_desc* pd, gk::Ct
     }
     tmp.ctx.h2d_rows = stage_rows(tmp.ctx.g);
     tmp.ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
+    tmp.ctx.stage_threads = stage_threads_default();
     *ctx = tmp.ctx;
     return GK_OK;
 }
+
+// ------------------------------------------------------------ tiling
+extern "C" int gk_set_tiling(gk_handle* h, int threads, int rows) {
+    if (!h) return GK_ERR_INVALID;
+    if (threads != 64 && threads != 128 && threads != 256)
+        return fail(h, GK_ERR_INVALID, "threads per CTA must be 64, 128 or 256");
+    if (rows < 1) return fail(h, GK_ERR_INVALID, "rows per segment must be positive");
+    h->ctx.stage_threads = threads;
+    h->ctx.h2d_rows = rows;
+    h->tiling_set = true;
+    h->tiling_rows = rows;
+    if (h->gexec) {  // the graph holds the old launch shapes
+        cudaGraphExecDestroy(h->gexec);
+        h->gexec = nullptr;
+    }
+    return GK_OK;
+}
+
+// ------------------------------------------------------------ ensembles
+// A batch of independent 2D problems advanced together: every stage of every
+// instance is one persistent launch over a tile table (k_ens_stage), every
+// ghost fill one launch over all instances, and a CUDA graph holds whole
+// steps.  Each instance keeps its own handle, buffers and clock, so its dt
+// and t follow its own CFL condition exactly as if it ran alone.
+struct gk_ensemble {
+    std::vector<gk_handle*> h;
+    int n = 0, threads = 128, plm = 1, device = 0;
+    const KernelSet* ks = nullptr;
+    cudaStream_t stream = nullptr;
+    gk::EnsInst* dinst = nullptr;
+    int2* dtiles = nullptr;
+    unsigned* dcount = nullptr;  // work counters of the two stages
+    int* dany = nullptr;
+    int ntiles = 0, max_bc = 0;
+    std::vector<int> rows;
+    cudaGraphExec_t gexec = nullptr;
+    int graph_steps = 8;
+    std::string err;
+};
+
+namespace {
+
+int efail(gk_ensemble* e, int code, const std::string& msg) {
+    if (e) e->err = msg;
+    return code;
+}
+
+#define GK_ECUDA(e, call)                                                                       \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return efail((e), GK_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+__global__ void k_ens_any_active(const gk::EnsInst* __restrict__ inst, int n, int* any) {
+    int a = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a |= inst[i].tm->active;
+    a = __syncthreads_or(a);
+    if (threadIdx.x == 0) *any = a;
+}
+
+int ens_build(gk_ensemble* e) {
+    std::vector<gk::EnsInst> inst(e->n);
+    std::vector<int2> tiles;
+    e->max_bc = 0;
+    for (int i = 0; i < e->n; ++i) {
+        const gk::Ctx& c = e->h[i]->ctx;
+        const gk::Geom& g = c.g;
+        gk::EnsInst& I = inst[i];
+        std::memset(&I, 0, sizeof(I));
+        if (!gk::encode_rows_map(&I.mapA, e->h[i]->A, g, e->threads) ||
+            !gk::encode_rows_map(&I.mapB, e->h[i]->B, g, e->threads))
+            return efail(e, GK_ERR_CUDA, "tensor map encoding failed");
+        I.A = e->h[i]->A;
+        I.B = e->h[i]->B;
+        I.tm = e->h[i]->tm;
+        I.rows = std::max(1, e->rows[i]);
+        I.tiles_x = (g.nx + e->threads - 5) / (e->threads - 4);
+        I.tiles = I.tiles_x * ((g.ny + I.rows - 1) / I.rows);
+        I.g = g;
+        I.ph = c.ph;
+        for (int t = 0; t < I.tiles; ++t) tiles.push_back(make_int2(i, t));
+        e->max_bc = std::max(e->max_bc, g.ng * std::max(g.nx, g.ny));
+    }
+    cudaFree(e->dinst);
+    cudaFree(e->dtiles);
+    e->dinst = nullptr;
+    e->dtiles = nullptr;
+    e->ntiles = (int)tiles.size();
+    GK_ECUDA(e, cudaMalloc(&e->dinst, sizeof(gk::EnsInst) * e->n));
+    GK_ECUDA(e, cudaMalloc(&e->dtiles, sizeof(int2) * tiles.size()));
+    GK_ECUDA(e, cudaMemcpy(e->dinst, inst.data(), sizeof(gk::EnsInst) * e->n,
+                           cudaMemcpyHostToDevice));
+    GK_ECUDA(e, cudaMemcpy(e->dtiles, tiles.data(), sizeof(int2) * tiles.size(),
+                           cudaMemcpyHostToDevice));
+    if (e->gexec) {
+        cudaGraphExecDestroy(e->gexec);
+        e->gexec = nullptr;
+    }
+    return GK_OK;
+}
+
+// One RK2 step of every instance (rk2.cpp:11-23 per instance).
+void ens_enqueue_step(gk_ensemble* e) {
+    const KernelSet& k = *e->ks;
+    cudaStream_t s = e->stream;
+    cudaMemsetAsync(e->dcount, 0, 2 * sizeof(unsigned), s);
+    k.ens_bc(e->dinst, e->n, 0, e->max_bc, s);
+    k.ens_stage(e->threads, 0, e->plm, e->dinst, e->dtiles, e->ntiles, e->dcount, 1.0, 1.0, 0.0, s);
+    k.ens_bc(e->dinst, e->n, 1, e->max_bc, s);
+    k.ens_stage(e->threads, 2, e->plm, e->dinst, e->dtiles, e->ntiles, e->dcount + 1, 0.5, 0.5,
+                0.5, s);
+}
+
+int ens_graph(gk_ensemble* e) {
+    if (e->gexec) return GK_OK;
+    cudaGraph_t graph;
+    GK_ECUDA(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < e->graph_steps; ++i) ens_enqueue_step(e);
+    GK_ECUDA(e, cudaStreamEndCapture(e->stream, &graph));
+    cudaError_t err = cudaGraphInstantiate(&e->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess)
+        return efail(e, GK_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(err));
+    return GK_OK;
+}
+
+int ens_run(gk_ensemble* e, double dtoutput, int nsteps, bool wait) {
+    GK_ECUDA(e, cudaSetDevice(e->device));
+    for (gk_handle* h : e->h) GK_ECUDA(e, cudaStreamSynchronize(h->stream));
+    int rc = ens_graph(e);
+    if (rc != GK_OK) return rc;
+    e->ks->ens_begin(e->dinst, e->n, dtoutput, nsteps, e->stream);
+    GK_ECUDA(e, cudaGetLastError());
+    if (nsteps > 0) {
+        const int launches = (nsteps + e->graph_steps - 1) / e->graph_steps;
+        for (int i = 0; i < launches; ++i) GK_ECUDA(e, cudaGraphLaunch(e->gexec, e->stream));
+        if (wait) GK_ECUDA(e, cudaStreamSynchronize(e->stream));
+        return GK_OK;
+    }
+    int batch = 1, any = 1;
+    while (any) {
+        for (int i = 0; i < batch; ++i) GK_ECUDA(e, cudaGraphLaunch(e->gexec, e->stream));
+        k_ens_any_active<<<1, 128, 0, e->stream>>>(e->dinst, e->n, e->dany);
+        GK_ECUDA(e, cudaMemcpyAsync(&any, e->dany, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+        GK_ECUDA(e, cudaStreamSynchronize(e->stream));
+        batch = std::min(batch * 2, 64);
+    }
+    return GK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gk_ens_create(gk_handle* const* handles, int n, gk_ensemble** out) {
+    if (!handles || n <= 0 || !out) return GK_ERR_INVALID;
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        gk_handle* h = handles[i];
+        if (!h || !h->uploaded) return GK_ERR_STATE;
+        if (h->path != 1 || h->ctx.ph.integrator != 2) return GK_ERR_UNSUPPORTED;
+        if (h->ks != handles[0]->ks || h->device != handles[0]->device ||
+            h->ctx.ph.plm != handles[0]->ctx.ph.plm)
+            return GK_ERR_INVALID;
+    }
+    gk_ensemble* e = new gk_ensemble();
+    e->h.assign(handles, handles + n);
+    e->n = n;
+    e->ks = handles[0]->ks;
+    e->plm = handles[0]->ctx.ph.plm;
+    e->device = handles[0]->device;
+    e->rows.assign(n, 16);
+    cudaError_t ce = cudaSetDevice(e->device);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaMalloc(&e->dcount, 2 * sizeof(unsigned));
+    if (ce == cudaSuccess) ce = cudaMalloc(&e->dany, sizeof(int));
+    int rc = ce == cudaSuccess ? ens_build(e) : GK_ERR_CUDA;
+    if (rc != GK_OK) {
+        std::fprintf(stderr, "gk_ens_create: %s\n",
+                     ce != cudaSuccess ? cudaGetErrorString(ce) : e->err.c_str());
+        gk_ens_destroy(e);
+        return rc;
+    }
+    *out = e;
+    return GK_OK;
+}
+
+void gk_ens_destroy(gk_ensemble* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    cudaFree(e->dinst);
+    cudaFree(e->dtiles);
+    cudaFree(e->dcount);
+    cudaFree(e->dany);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+int gk_ens_set_tiling(gk_ensemble* e, int threads, const int* rows) {
+    if (!e) return GK_ERR_INVALID;
+    if (threads != 64 && threads != 128 && threads != 256)
+        return efail(e, GK_ERR_INVALID, "threads per CTA must be 64, 128 or 256");
+    e->threads = threads;
+    if (rows)
+        for (int i = 0; i < e->n; ++i) e->rows[i] = std::max(1, rows[i]);
+    cudaSetDevice(e->device);
+    return ens_build(e);
+}
+
+int gk_ens_advance(gk_ensemble* e, double dtoutput) {
+    if (!e) return GK_ERR_INVALID;
+    return ens_run(e, dtoutput, 0, true);
+}
+
+int gk_ens_run_steps(gk_ensemble* e, int nsteps) {
+    if (!e) return GK_ERR_INVALID;
+    if (nsteps <= 0) return GK_OK;
+    return ens_run(e, 0.0, nsteps, true);
+}
+
+int gk_ens_enqueue_steps(gk_ensemble* e, int nsteps) {
+    if (!e) return GK_ERR_INVALID;
+    if (nsteps <= 0) return GK_OK;
+    return ens_run(e, 0.0, nsteps, false);
+}
+
+int gk_ens_info(gk_ensemble* e, int* ntiles, int* threads, void** stream) {
+    if (!e) return GK_ERR_INVALID;
+    if (ntiles) *ntiles = e->ntiles;
+    if (threads) *threads = e->threads;
+    if (stream) *stream = (void*)e->stream;
+    return GK_OK;
+}
+
+const char* gk_ens_last_error(const gk_ensemble* e) { return e ? e->err.c_str() : ""; }
+
+}  // extern "C"

@@ -9,6 +9,7 @@
 // fills and face indices read exactly like the reference loops.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -70,9 +71,28 @@ struct Ctx {
     Phys ph;
     DevTime* tm;
     int has_vz;      // 2D: MTZ not identically zero -> generic path
-    int h2d_rows;    // fused 2D kernel: rows per CTA segment
-    int use_tma;     // fused 2D kernel: rows staged in shared memory by TMA
+    int h2d_rows;       // fused 2D kernel: rows per CTA segment
+    int use_tma;        // fused 2D kernel: rows staged in shared memory by TMA
+    int stage_threads;  // fused 2D kernel (TMA): threads per CTA, 64 / 128 / 256
 };
+
+// One instance of an ensemble, as the persistent stage kernel reads it from
+// global memory: tensor maps of its two state buffers, the buffers, its
+// clock, its tiling and geometry.
+struct alignas(64) EnsInst {
+    CUtensorMap mapA;
+    CUtensorMap mapB;
+    double* A;
+    double* B;
+    DevTime* tm;
+    int rows, tiles_x, tiles;
+    Geom g;
+    Phys ph;
+};
+
+// Tensor map of the four evolved planes of a state buffer: dims (pitch, leny,
+// 4) doubles, box (nt, 1, 4), no swizzle, zero fill out of bounds (gk_api.cu).
+bool encode_rows_map(CUtensorMap* map, const double* base, const Geom& g, int nt);
 
 // Kernel classes, for per-kernel profiling.
 enum KClass { K_BC = 0, K_C2P, K_FLUX, K_UPDATE, K_KICK, K_CFL, K_STAGE, K_BEGIN, K_NCLASS };
@@ -98,6 +118,13 @@ static const char* const kClassNames[K_NCLASS] = {
                         int kind, double c1, double c2, double c3, cudaStream_t s);            \
     void launch_begin(const gk::Ctx& c, double dtoutput, int steps, cudaStream_t s);           \
     void launch_mtz_check(const gk::Ctx& c, const double* u, int* flag, cudaStream_t s);       \
+    void launch_ens_stage(int threads, int kind, int plm, const gk::EnsInst* inst,             \
+                          const int2* tiles, int ntiles, unsigned* counter, double c1,          \
+                          double c2, double c3, cudaStream_t s);                                \
+    void launch_ens_bc(const gk::EnsInst* inst, int n, int which, int max_count,               \
+                       cudaStream_t s);                                                        \
+    void launch_ens_begin(const gk::EnsInst* inst, int n, double dtoutput, int steps,          \
+                          cudaStream_t s);                                                     \
     }
 
 GK_DECLARE_KERNEL_SET(gk_parity)

@@ -19,6 +19,7 @@
 #include <cudaTypedefs.h>
 #include <math_constants.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 #include <cstdio>
@@ -53,19 +54,13 @@ __device__ __forceinline__ long long fidx(const Geom& g, int k, int j, int i) {
 // rows/columns only; corners untouched.  With n >= nghost in every filled
 // direction each ghost depends on one active cell, so all sides fill in one
 // launch.  blockIdx.y = 2*dir + side.
-__global__ void k_bc(double* __restrict__ u, Geom g, Phys ph, const DevTime* __restrict__ tm) {
-    if (!tm->active) return;
-    const int dir = blockIdx.y >> 1, side = blockIdx.y & 1;
+// One ghost cell (id enumerates ghost layer fastest, then the transverse
+// active cells) of side `side` in direction `dir`, every variable.
+__device__ __forceinline__ void bc_fill_one(double* __restrict__ u, const Geom& g, const Phys& ph,
+                                            int dir, int side, long long id) {
     const int n3[3] = {g.nx, g.ny, g.nz};
-    if (n3[dir] <= 1) return;
-    if (dir == 2 && !((ph.fill_z >> side) & 1)) return;
-    const int type = ph.bc[blockIdx.y];
-    // transverse extents (active), ghost layers along dir
+    const int type = ph.bc[2 * dir + side];
     const int ta = dir == 0 ? g.ny : g.nx;
-    const int tb = dir == 2 ? g.ny : g.nz;
-    const long long count = (long long)g.ng * ta * tb;
-    long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= count) return;
     const int gi = (int)(id % g.ng);
     const long long r = id / g.ng;
     const int a = (int)(r % ta), b = (int)(r / ta);
@@ -102,6 +97,20 @@ __global__ void k_bc(double* __restrict__ u, Geom g, Phys ph, const DevTime* __r
     }
 #pragma unroll
     for (int v = 0; v < 5; ++v) u[v * g.vstride + dst] = q[v];
+}
+
+__global__ void k_bc(double* __restrict__ u, Geom g, Phys ph, const DevTime* __restrict__ tm) {
+    if (!tm->active) return;
+    const int dir = blockIdx.y >> 1, side = blockIdx.y & 1;
+    const int n3[3] = {g.nx, g.ny, g.nz};
+    if (n3[dir] <= 1) return;
+    if (dir == 2 && !((ph.fill_z >> side) & 1)) return;
+    const int ta = dir == 0 ? g.ny : g.nx;
+    const int tb = dir == 2 ? g.ny : g.nz;
+    const long long count = (long long)g.ng * ta * tb;
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= count) return;
+    bc_fill_one(u, g, ph, dir, side, id);
 }
 
 // ------------------------------------------------------------ ConsToPrim
@@ -373,7 +382,8 @@ __global__ void __launch_bounds__(256) k_cfl(const double* __restrict__ u, Geom 
 
 // Start of a Sim::Advance call (sim.cpp:70-72, 77-81) or of a fixed-count
 // run (steps > 0: no output time, step budget).
-__global__ void k_begin(DevTime* tm, Geom g, Phys ph, double dtoutput, int steps) {
+__device__ __forceinline__ void begin_one(DevTime* tm, const Geom& g, const Phys& ph,
+                                          double dtoutput, int steps) {
     if (steps > 0) {
         tm->tNext = CUDART_INF;
         tm->dtUntilOutput = CUDART_INF;
@@ -389,6 +399,10 @@ __global__ void k_begin(DevTime* tm, Geom g, Phys ph, double dtoutput, int steps
         tm->dt = smin(dt, tm->dtUntilOutput);
     }
     tm->active = act;
+}
+
+__global__ void k_begin(DevTime* tm, Geom g, Phys ph, double dtoutput, int steps) {
+    begin_one(tm, g, ph, dtoutput, steps);
 }
 
 __global__ void k_mtz_check(const double* __restrict__ u, Geom g, int* flag) {
@@ -653,19 +667,22 @@ __global__ void __launch_bounds__(kStageThreads, 3)
 // ------------------------------------------------------------ fused 2D stage, TMA rows
 // The same stage with its input rows staged in shared memory by the tensor
 // memory accelerator instead of registers.  One cp.async.bulk.tensor load
-// brings a 3D box of 128 columns x 1 row x 4 variable planes (4 KB) into a
-// ring slot; an mbarrier per slot counts its bytes.  Raw rows run four
-// ahead of the row being converted (ring of 6: rows f-2 .. f+3 live); the
-// RK base state u0 runs three ahead (ring of 4).  A slot is refilled only
-// after the barrier that follows its last read, behind a proxy fence.  The
-// box origin is column 124*blockIdx.x, a multiple of 16 bytes; columns past
-// the last one read as zero (TMA out-of-bounds fill) and feed only halo lanes.
-// Waits are bounded: a wait that gives up sets STATUS_TMA_TIMEOUT and the
-// kernel carries on, so it cannot hang.
+// brings a 3D box of NT columns x 1 row x 4 variable planes into a ring
+// slot; an mbarrier per slot counts its bytes.  Raw rows run four ahead of
+// the row being converted (ring of 6: rows f-2 .. f+3 live); the RK base
+// state u0 runs three ahead (ring of 4).  A slot is refilled only after the
+// barrier that follows its last read, behind a proxy fence.  The box origin
+// is column (NT-4)*strip, a multiple of 16 bytes for NT = 64, 128, 256;
+// columns past the last one read as zero (TMA out-of-bounds fill) and feed
+// only halo lanes.  Waits are bounded: a wait that gives up sets
+// STATUS_TMA_TIMEOUT and the kernel carries on, so it cannot hang.
+//
+// stage_tile_tma does one tile (strip bx, segment by).  The single-problem
+// kernel runs one tile per CTA; the ensemble kernel (k_ens_stage) is
+// persistent: each CTA takes tiles of any instance from a tile table through
+// an atomic counter, reusing its ring and barriers.
 constexpr int kRing = 6;
 constexpr int kRing0 = 4;
-constexpr unsigned kRowBytes = 4u * kStageThreads * sizeof(double);
-constexpr int kRowDoubles = 4 * kStageThreads;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -678,9 +695,9 @@ __device__ __forceinline__ void fence_proxy_async() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 __device__ __forceinline__ void tma_row(double* dst, const CUtensorMap* map, int x, int y,
-                                        uint64_t* bar) {
+                                        unsigned bytes, uint64_t* bar) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(kRowBytes)
+                 "r"(bytes)
                  : "memory");
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
@@ -702,33 +719,55 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned phase, int* st
     atomicOr(status, gk::STATUS_TMA_TIMEOUT);
 }
 
-template <int KIND, bool PLM>
-__global__ void __launch_bounds__(kStageThreads, 4)
-    k_stage2d_tma(const __grid_constant__ CUtensorMap mapc, const __grid_constant__ CUtensorMap map0,
-                  double* out, Geom g, Phys ph, double c1, double c2, double c3, DevTime* tm,
-                  int rows) {
+template <int NT>
+struct StageShared {
+    double sP[4][NT];
+    double sXL[4][NT];
+    double sF[4][NT];
+    uint64_t bar[kRing];
+    uint64_t bar0[kRing0];
+    unsigned long long wmax[NT / 32];
+    int cur;
+    int last;
+};
+
+template <int NT>
+__device__ __forceinline__ void stage_init_barriers(StageShared<NT>& sm) {
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kRing; ++i) mbar_init(&sm.bar[i], 1);
+        for (int i = 0; i < kRing0; ++i) mbar_init(&sm.bar0[i], 1);
+        fence_proxy_async();
+    }
+    __syncthreads();
+}
+
+// seq / seq0: rows of raw state / base state this CTA has loaded so far;
+// they fix each row's ring slot and mbarrier phase across tiles.
+// tiles_total: tiles of this problem; the LAST stage's last tile runs the
+// step epilogue.
+template <int NT, int KIND, bool PLM>
+__device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CUtensorMap* map0,
+                                               double* out, const Geom& g, const Phys& ph,
+                                               double c1, double c2, double c3, DevTime* tm,
+                                               int rows, int bx, int by, unsigned tiles_total,
+                                               double* ring, double* ring0, StageShared<NT>& sm,
+                                               unsigned& seq, unsigned& seq0) {
     constexpr bool THREE = KIND >= 1;
     constexpr bool LAST = KIND == 2;
-    if (!tm->active) return;
-    extern __shared__ __align__(128) double dyn[];
-    double* ring = dyn;                          // [kRing][4][128]
-    double* ring0 = dyn + kRing * kRowDoubles;   // [kRing0][4][128]
-    __shared__ __align__(8) uint64_t bar[kRing];
-    __shared__ __align__(8) uint64_t bar0[kRing0];
-    __shared__ double sP[4][kStageThreads];
-    __shared__ double sXL[4][kStageThreads];
-    __shared__ double sF[4][kStageThreads];
+    constexpr int COLS = NT - 4;
+    constexpr int RD = 4 * NT;
+    constexpr unsigned RB = RD * sizeof(double);
     unsigned long long cbest = 0ull;
 
     const double dt = tm->dt;
     const double dtdx = dt * g.dxRec, dtdy = dt * g.dyRec;
     const int t = threadIdx.x;
     const int tl = t > 0 ? t - 1 : 0;
-    const int tr = t < kStageThreads - 1 ? t + 1 : t;
-    const int x0 = g.ib - 2 + blockIdx.x * kStageCols;  // box origin column
+    const int tr = t < NT - 1 ? t + 1 : t;
+    const int x0 = g.ib - 2 + bx * COLS;  // box origin column
     const int xi = x0 + t;
-    const bool do_cell = t >= 2 && t <= kStageThreads - 3 && xi < g.ie;
-    const int y0 = g.jb + blockIdx.y * rows;
+    const bool do_cell = t >= 2 && t <= NT - 3 && xi < g.ie;
+    const int y0 = g.jb + by * rows;
     const int y1 = min(y0 + rows, g.je);
     const int rlo = y0 - 2;
     const long long vs = g.vstride;
@@ -736,32 +775,32 @@ __global__ void __launch_bounds__(kStageThreads, 4)
     const long long cbase = sidx(g, g.kb, 0, xi < g.lenx ? xi : g.lenx - 1);
     int* status = &tm->status;
 
-    auto slot = [&](int r) { return (r - rlo) % kRing; };
-    auto slot0 = [&](int r) { return (r - y0) % kRing0; };
-    auto issue = [&](int r) { tma_row(ring + slot(r) * kRowDoubles, &mapc, x0, r, &bar[slot(r)]); };
-    auto issue0 = [&](int r) {
-        tma_row(ring0 + slot0(r) * kRowDoubles, &map0, x0, r, &bar0[slot0(r)]);
+    auto rs = [&](int r) { return seq + (unsigned)(r - rlo); };
+    auto rs0 = [&](int r) { return seq0 + (unsigned)(r - y0); };
+    auto issue = [&](int r) {
+        const unsigned q = rs(r) % kRing;
+        tma_row(ring + q * RD, mapc, x0, r, RB, &sm.bar[q]);
     };
-    auto wait = [&](int r) { mbar_wait(&bar[slot(r)], (unsigned)(((r - rlo) / kRing) & 1), status); };
+    auto issue0 = [&](int r) {
+        const unsigned q = rs0(r) % kRing0;
+        tma_row(ring0 + q * RD, map0, x0, r, RB, &sm.bar0[q]);
+    };
+    auto wait = [&](int r) { mbar_wait(&sm.bar[rs(r) % kRing], (rs(r) / kRing) & 1u, status); };
     auto wait0 = [&](int r) {
-        mbar_wait(&bar0[slot0(r)], (unsigned)(((r - y0) / kRing0) & 1), status);
+        mbar_wait(&sm.bar0[rs0(r) % kRing0], (rs0(r) / kRing0) & 1u, status);
     };
     auto rowq = [&](int r) {
-        const double* p = ring + slot(r) * kRowDoubles;
-        return Q4{p[t], p[kStageThreads + t], p[2 * kStageThreads + t], p[3 * kStageThreads + t]};
+        const double* p = ring + (rs(r) % kRing) * RD;
+        return Q4{p[t], p[NT + t], p[2 * NT + t], p[3 * NT + t]};
     };
     auto rowq0 = [&](int r) {
-        const double* p = ring0 + slot0(r) * kRowDoubles;
-        return Q4{p[t], p[kStageThreads + t], p[2 * kStageThreads + t], p[3 * kStageThreads + t]};
+        const double* p = ring0 + (rs0(r) % kRing0) * RD;
+        return Q4{p[t], p[NT + t], p[2 * NT + t], p[3 * NT + t]};
     };
 
+    __syncthreads();  // the previous tile is done with every ring slot
     if (t == 0) {
-        for (int i = 0; i < kRing; ++i) mbar_init(&bar[i], 1);
-        for (int i = 0; i < kRing0; ++i) mbar_init(&bar0[i], 1);
         fence_proxy_async();
-    }
-    __syncthreads();
-    if (t == 0) {
         for (int r = rlo; r <= min(y0 + 3, y1 + 1); ++r) issue(r);
         if (THREE)
             for (int r = y0; r <= min(y0 + 2, y1 - 1); ++r) issue0(r);
@@ -780,7 +819,7 @@ __global__ void __launch_bounds__(kStageThreads, 4)
         // y face y0
         wait(y0 + 1);
         const W4 P1 = c2p4(rowq(y0 + 1), ph);
-        __syncthreads();  // rows y0-2 is read by all: its slot may be refilled
+        __syncthreads();  // row y0-2 is read by all: its slot may be refilled
         if (t == 0 && y0 + 4 <= y1 + 1) {
             fence_proxy_async();
             issue(y0 + 4);
@@ -800,44 +839,44 @@ __global__ void __launch_bounds__(kStageThreads, 4)
     for (int f = y0 + 1; f <= y1; ++f) {
         wait(f + 1);
         const W4 P1 = c2p4(rowq(f + 1), ph);
-        sP[0][t] = Pm1.r; sP[1][t] = Pm1.vx; sP[2][t] = Pm1.vy; sP[3][t] = Pm1.p;
+        sm.sP[0][t] = Pm1.r; sm.sP[1][t] = Pm1.vx; sm.sP[2][t] = Pm1.vy; sm.sP[3][t] = Pm1.p;
         __syncthreads();
         if (t == 0) {
-            // rows f-2 (raw) and f-2 (base state) were last read in iteration f-1
+            // raw row f-2 and base-state row f-2 were last read in iteration f-1
             fence_proxy_async();
             if (f + 4 <= y1 + 1) issue(f + 4);
             if (THREE && f + 2 <= y1 - 1) issue0(f + 2);
         }
         W4 xr = Pm1, wr = P0, wlNew = P0;
         if (PLM) {
-            const W4 a{sP[0][tl], sP[1][tl], sP[2][tl], sP[3][tl]};
-            const W4 c{sP[0][tr], sP[1][tr], sP[2][tr], sP[3][tr]};
+            const W4 a{sm.sP[0][tl], sm.sP[1][tl], sm.sP[2][tl], sm.sP[3][tl]};
+            const W4 c{sm.sP[0][tr], sm.sP[1][tr], sm.sP[2][tr], sm.sP[3][tr]};
             const W4 sx = vl4(a, Pm1, c);
             const W4 sy = vl4(Pm1, P0, P1);
             const W4 xlft = plus_half(Pm1, sx);
             xr = minus_half(Pm1, sx);
             wr = minus_half(P0, sy);
             wlNew = plus_half(P0, sy);
-            sXL[0][t] = xlft.r; sXL[1][t] = xlft.vx; sXL[2][t] = xlft.vy; sXL[3][t] = xlft.p;
+            sm.sXL[0][t] = xlft.r; sm.sXL[1][t] = xlft.vx; sm.sXL[2][t] = xlft.vy; sm.sXL[3][t] = xlft.p;
         } else {
-            sXL[0][t] = Pm1.r; sXL[1][t] = Pm1.vx; sXL[2][t] = Pm1.vy; sXL[3][t] = Pm1.p;
+            sm.sXL[0][t] = Pm1.r; sm.sXL[1][t] = Pm1.vx; sm.sXL[2][t] = Pm1.vy; sm.sXL[3][t] = Pm1.p;
         }
         __syncthreads();
-        const W4 xl_state{sXL[0][tl], sXL[1][tl], sXL[2][tl], sXL[3][tl]};
+        const W4 xl_state{sm.sXL[0][tl], sm.sXL[1][tl], sm.sXL[2][tl], sm.sXL[3][tl]};
         Flux5 fx, fy;
         hllc_x(xl_state, xr, ph, fx);
         hllc_y(wlNext, wr, ph, fy);
-        sF[0][t] = fx.d; sF[1][t] = fx.n; sF[2][t] = fx.t1; sF[3][t] = fx.e;
+        sm.sF[0][t] = fx.d; sm.sF[1][t] = fx.n; sm.sF[2][t] = fx.t1; sm.sF[3][t] = fx.e;
         __syncthreads();
+        if (THREE) wait0(f - 1);
         if (do_cell) {
             const Q4 Qm1 = rowq(f - 1);
-            double dF0 = (sF[0][tr] - fx.d) * dtdx + (fy.d - fyPrev.d) * dtdy;
-            double dF1 = (sF[1][tr] - fx.n) * dtdx + (fy.t1 - fyPrev.t1) * dtdy;
-            double dF2 = (sF[2][tr] - fx.t1) * dtdx + (fy.n - fyPrev.n) * dtdy;
-            double dF3 = (sF[3][tr] - fx.e) * dtdx + (fy.e - fyPrev.e) * dtdy;
+            double dF0 = (sm.sF[0][tr] - fx.d) * dtdx + (fy.d - fyPrev.d) * dtdy;
+            double dF1 = (sm.sF[1][tr] - fx.n) * dtdx + (fy.t1 - fyPrev.t1) * dtdy;
+            double dF2 = (sm.sF[2][tr] - fx.t1) * dtdx + (fy.n - fyPrev.n) * dtdy;
+            double dF3 = (sm.sF[3][tr] - fx.e) * dtdx + (fy.e - fyPrev.e) * dtdy;
             double r[4];
             if (THREE) {
-                wait0(f - 1);
                 const Q4 U0 = rowq0(f - 1);
                 r[0] = c1 * U0.d + c2 * Qm1.d - c3 * dF0;
                 r[1] = c1 * U0.mx + c2 * Qm1.mx - c3 * dF1;
@@ -871,8 +910,6 @@ __global__ void __launch_bounds__(kStageThreads, 4)
             out[vs + oc] = r[1];
             out[2 * vs + oc] = r[2];
             out[3 * vs + oc] = r[3];
-        } else if (THREE) {
-            wait0(f - 1);  // every lane keeps the base-state ring in step
         }
         fyPrev = fy;
         wlNext = wlNew;
@@ -885,52 +922,98 @@ __global__ void __launch_bounds__(kStageThreads, 4)
             const unsigned long long x = __shfl_xor_sync(0xffffffffu, cbest, o);
             cbest = x > cbest ? x : cbest;
         }
-        __shared__ unsigned long long wmax[kStageThreads / 32];
-        __shared__ bool last;
-        if ((t & 31) == 0) wmax[t >> 5] = cbest;
+        if ((t & 31) == 0) sm.wmax[t >> 5] = cbest;
         __syncthreads();
         if (t == 0) {
-            unsigned long long m = wmax[0];
-            for (int w = 1; w < kStageThreads / 32; ++w) m = wmax[w] > m ? wmax[w] : m;
+            unsigned long long m = sm.wmax[0];
+            for (int w = 1; w < NT / 32; ++w) m = sm.wmax[w] > m ? sm.wmax[w] : m;
             atomicMax(&tm->cmax_acc, m);
             __threadfence();
             const unsigned int prev = atomicAdd(&tm->done_ctas, 1u);
-            last = (prev == gridDim.x * gridDim.y - 1);
+            sm.last = (prev == tiles_total - 1);
         }
         __syncthreads();
-        if (last && t == 0) {
+        if (sm.last && t == 0) {
             __threadfence();
             step_epilogue(tm, g, ph, 1);
         }
     }
+    seq += (unsigned)(y1 + 2 - rlo);
+    if (THREE) seq0 += (unsigned)(y1 - y0);
 }
 
-// Tensor map of the four evolved planes of a state buffer: dims (pitch,
-// leny, 4) doubles, box (128, 1, 4), no swizzle, zero fill out of bounds.
-static bool encode_rows_map(CUtensorMap* map, const double* base, const Geom& g) {
-    cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)g.leny, 4};
-    cuuint64_t strides[2] = {(cuuint64_t)g.pitch * sizeof(double),
-                             (cuuint64_t)g.vstride * sizeof(double)};
-    cuuint32_t box[3] = {(cuuint32_t)kStageThreads, 1, 4};
-    cuuint32_t estr[3] = {1, 1, 1};
-    // resolved through the runtime so the library carries no link-time
-    // dependency on the driver library
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
-        void* fn = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
-                cudaSuccess ||
-            q != cudaDriverEntryPointSuccess || !fn)
-            return false;
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+template <int NT, bool THREE>
+constexpr size_t stage_dyn_bytes() {
+    return (size_t)(kRing + (THREE ? kRing0 : 0)) * 4 * NT * sizeof(double);
+}
+
+template <int NT, int KIND, bool PLM>
+__global__ void __launch_bounds__(NT, 512 / NT)
+    k_stage2d_tma(const __grid_constant__ CUtensorMap mapc, const __grid_constant__ CUtensorMap map0,
+                  double* out, Geom g, Phys ph, double c1, double c2, double c3, DevTime* tm,
+                  int rows) {
+    if (!tm->active) return;
+    extern __shared__ __align__(128) double dyn[];
+    __shared__ StageShared<NT> sm;
+    stage_init_barriers(sm);
+    unsigned seq = 0, seq0 = 0;
+    stage_tile_tma<NT, KIND, PLM>(&mapc, &map0, out, g, ph, c1, c2, c3, tm, rows, blockIdx.x,
+                                  blockIdx.y, gridDim.x * gridDim.y, dyn, dyn + kRing * 4 * NT, sm,
+                                  seq, seq0);
+}
+
+// Persistent stage over an ensemble: tiles[i] = (instance, tile of that
+// instance), claimed through *counter (zeroed before the launch).  Stage
+// KIND 0 reads A and writes B; KIND 2 reads B and A and writes A.
+template <int NT, int KIND, bool PLM>
+__global__ void __launch_bounds__(NT, 512 / NT)
+    k_ens_stage(const gk::EnsInst* __restrict__ inst, const int2* __restrict__ tiles, int ntiles,
+                unsigned* counter, double c1, double c2, double c3) {
+    extern __shared__ __align__(128) double dyn[];
+    __shared__ StageShared<NT> sm;
+    stage_init_barriers(sm);
+    unsigned seq = 0, seq0 = 0;
+    for (;;) {
+        if (threadIdx.x == 0) sm.cur = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int id = sm.cur;
+        __syncthreads();
+        if (id >= ntiles) break;
+        const int2 tl = tiles[id];
+        const gk::EnsInst* I = inst + tl.x;
+        DevTime* tm = I->tm;
+        if (!tm->active) continue;
+        const Geom g = I->g;
+        const Phys ph = I->ph;
+        const int bx = tl.y % I->tiles_x, by = tl.y / I->tiles_x;
+        if (KIND == 0)
+            stage_tile_tma<NT, KIND, PLM>(&I->mapA, &I->mapA, I->B, g, ph, c1, c2, c3, tm, I->rows,
+                                          bx, by, (unsigned)I->tiles, dyn, dyn + kRing * 4 * NT,
+                                          sm, seq, seq0);
+        else
+            stage_tile_tma<NT, KIND, PLM>(&I->mapB, &I->mapA, I->A, g, ph, c1, c2, c3, tm, I->rows,
+                                          bx, by, (unsigned)I->tiles, dyn, dyn + kRing * 4 * NT,
+                                          sm, seq, seq0);
     }
-    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
-                                        const_cast<double*>(base), dims, strides, box, estr,
-                                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS;
+}
+
+// Ghost fill of every instance: blockIdx.z = instance, blockIdx.y = side
+// (x left, x right, y left, y right); which = 0 fills A, 1 fills B.
+__global__ void k_ens_bc(const gk::EnsInst* __restrict__ inst, int which) {
+    const gk::EnsInst* I = inst + blockIdx.z;
+    if (!I->tm->active) return;
+    const int dir = blockIdx.y >> 1, side = blockIdx.y & 1;
+    const Geom& g = I->g;
+    const long long count = (long long)g.ng * (dir == 0 ? g.ny : g.nx);
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= count) return;
+    bc_fill_one(which ? I->B : I->A, g, I->ph, dir, side, id);
+}
+
+__global__ void k_ens_begin(const gk::EnsInst* __restrict__ inst, int n, double dtoutput,
+                            int steps) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) begin_one(inst[i].tm, inst[i].g, inst[i].ph, dtoutput, steps);
 }
 
 // ------------------------------------------------------------ launchers
@@ -987,21 +1070,35 @@ void launch_cfl(const Ctx& c, const double* u, int epilogue, cudaStream_t s) {
         k_cfl<false><<<blocks, 256, 0, s>>>(u, g, c.ph, c.tm, epilogue);
 }
 
-template <int KIND, bool PLM>
+template <int NT, int KIND, bool PLM>
 static void launch_stage2d_tma(const Ctx& c, const CUtensorMap& mc, const CUtensorMap& m0,
                                double* out, double c1, double c2, double c3, cudaStream_t s) {
     const Geom& g = c.g;
     const int rows = c.h2d_rows;
-    dim3 grid((g.nx + kStageCols - 1) / kStageCols, (g.ny + rows - 1) / rows);
-    const size_t dyn = (size_t)(kRing + (KIND >= 1 ? kRing0 : 0)) * kRowBytes;
+    dim3 grid((g.nx + NT - 5) / (NT - 4), (g.ny + rows - 1) / rows);
+    const size_t dyn = stage_dyn_bytes<NT, (KIND >= 1)>();
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_stage2d_tma<KIND, PLM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dyn);
+        cudaFuncSetAttribute(k_stage2d_tma<NT, KIND, PLM>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
         attr_set = true;
     }
-    k_stage2d_tma<KIND, PLM><<<grid, kStageThreads, dyn, s>>>(mc, m0, out, g, c.ph, c1, c2, c3,
-                                                              c.tm, rows);
+    k_stage2d_tma<NT, KIND, PLM><<<grid, NT, dyn, s>>>(mc, m0, out, g, c.ph, c1, c2, c3, c.tm, rows);
+}
+
+template <int NT>
+static void launch_stage2d_tma_nt(const Ctx& c, const CUtensorMap& mc, const CUtensorMap& m0,
+                                  double* out, int kind, double c1, double c2, double c3,
+                                  cudaStream_t s) {
+    if (c.ph.plm) {
+        if (kind == 0) launch_stage2d_tma<NT, 0, true>(c, mc, m0, out, c1, c2, c3, s);
+        else if (kind == 1) launch_stage2d_tma<NT, 1, true>(c, mc, m0, out, c1, c2, c3, s);
+        else launch_stage2d_tma<NT, 2, true>(c, mc, m0, out, c1, c2, c3, s);
+    } else {
+        if (kind == 0) launch_stage2d_tma<NT, 0, false>(c, mc, m0, out, c1, c2, c3, s);
+        else if (kind == 1) launch_stage2d_tma<NT, 1, false>(c, mc, m0, out, c1, c2, c3, s);
+        else launch_stage2d_tma<NT, 2, false>(c, mc, m0, out, c1, c2, c3, s);
+    }
 }
 
 void launch_stage2d(const Ctx& c, const double* uc, const double* u0, double* out, int kind,
@@ -1009,19 +1106,12 @@ void launch_stage2d(const Ctx& c, const double* uc, const double* u0, double* ou
     const Geom& g = c.g;
     const int rows = c.h2d_rows;
     if (c.use_tma) {
+        const int nt = c.stage_threads;
         CUtensorMap mc, m0;
-        if (encode_rows_map(&mc, uc, g) && encode_rows_map(&m0, u0 ? u0 : uc, g)) {
-#define GK_TMA(K, PL) launch_stage2d_tma<K, PL>(c, mc, m0, out, c1, c2, c3, s)
-            if (c.ph.plm) {
-                if (kind == 0) GK_TMA(0, true);
-                else if (kind == 1) GK_TMA(1, true);
-                else GK_TMA(2, true);
-            } else {
-                if (kind == 0) GK_TMA(0, false);
-                else if (kind == 1) GK_TMA(1, false);
-                else GK_TMA(2, false);
-            }
-#undef GK_TMA
+        if (gk::encode_rows_map(&mc, uc, g, nt) && gk::encode_rows_map(&m0, u0 ? u0 : uc, g, nt)) {
+            if (nt == 64) launch_stage2d_tma_nt<64>(c, mc, m0, out, kind, c1, c2, c3, s);
+            else if (nt == 256) launch_stage2d_tma_nt<256>(c, mc, m0, out, kind, c1, c2, c3, s);
+            else launch_stage2d_tma_nt<128>(c, mc, m0, out, kind, c1, c2, c3, s);
             return;
         }
         std::fprintf(stderr, "gaukuk: tensor map encoding failed; using register-staged rows\n");
@@ -1038,6 +1128,51 @@ void launch_stage2d(const Ctx& c, const double* uc, const double* u0, double* ou
         else GK_STAGE(2, false);
     }
 #undef GK_STAGE
+}
+
+template <int NT, int KIND, bool PLM>
+static void launch_ens_stage_k(const gk::EnsInst* inst, const int2* tiles, int ntiles,
+                               unsigned* counter, double c1, double c2, double c3, int ctas,
+                               cudaStream_t s) {
+    const size_t dyn = stage_dyn_bytes<NT, (KIND >= 1)>();
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_ens_stage<NT, KIND, PLM>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        attr_set = true;
+    }
+    k_ens_stage<NT, KIND, PLM><<<ctas, NT, dyn, s>>>(inst, tiles, ntiles, counter, c1, c2, c3);
+}
+
+template <int NT>
+static void launch_ens_stage_nt(int kind, int plm, const gk::EnsInst* inst, const int2* tiles,
+                                int ntiles, unsigned* counter, double c1, double c2, double c3,
+                                cudaStream_t s) {
+    const int ctas = std::min(ntiles, 148 * (512 / NT));
+    if (plm) {
+        if (kind == 0) launch_ens_stage_k<NT, 0, true>(inst, tiles, ntiles, counter, c1, c2, c3, ctas, s);
+        else launch_ens_stage_k<NT, 2, true>(inst, tiles, ntiles, counter, c1, c2, c3, ctas, s);
+    } else {
+        if (kind == 0) launch_ens_stage_k<NT, 0, false>(inst, tiles, ntiles, counter, c1, c2, c3, ctas, s);
+        else launch_ens_stage_k<NT, 2, false>(inst, tiles, ntiles, counter, c1, c2, c3, ctas, s);
+    }
+}
+
+void launch_ens_stage(int threads, int kind, int plm, const gk::EnsInst* inst, const int2* tiles,
+                      int ntiles, unsigned* counter, double c1, double c2, double c3,
+                      cudaStream_t s) {
+    if (threads == 64) launch_ens_stage_nt<64>(kind, plm, inst, tiles, ntiles, counter, c1, c2, c3, s);
+    else if (threads == 256) launch_ens_stage_nt<256>(kind, plm, inst, tiles, ntiles, counter, c1, c2, c3, s);
+    else launch_ens_stage_nt<128>(kind, plm, inst, tiles, ntiles, counter, c1, c2, c3, s);
+}
+
+void launch_ens_bc(const gk::EnsInst* inst, int n, int which, int max_count, cudaStream_t s) {
+    dim3 grid((max_count + 127) / 128, 4, n);
+    k_ens_bc<<<grid, 128, 0, s>>>(inst, which);
+}
+
+void launch_ens_begin(const gk::EnsInst* inst, int n, double dtoutput, int steps, cudaStream_t s) {
+    k_ens_begin<<<(n + 63) / 64, 64, 0, s>>>(inst, n, dtoutput, steps);
 }
 
 void launch_begin(const Ctx& c, double dtoutput, int steps, cudaStream_t s) {

@@ -153,3 +153,21 @@ def random_smooth(p: Params, seed: int = 0, with_vz: bool = False):
     if p.ny == 1:
         vy = np.zeros_like(rho) if not with_vz else vy
     return prim_to_cons(p, rho, vx, vy, vz, pre)
+
+
+def kh_ensemble(n: int = 64, seed: int = 0, sizes=(128, 256, 512), tmax: float = 1.0, **kw):
+    """Ensemble of independent KH problems.  Per instance, drawn from a seeded
+    generator: grid size from `sizes`, density ratio U[1.5, 4] (rho_out = 1,
+    rho_in = ratio), shear-layer half-width U[0.2, 0.3], perturbation
+    amplitude U[0.005, 0.02]; periodic, PLM, HLLC, RK2.  Returns a list of
+    (params, cons, draw) with the draws recorded."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        size = int(sizes[rng.integers(0, len(sizes))])
+        draw = {"size": size, "ratio": float(rng.uniform(1.5, 4.0)),
+                "half_width": float(rng.uniform(0.2, 0.3)), "amp": float(rng.uniform(0.005, 0.02))}
+        p, c = kh(size, seed=seed * 1000 + i, rho_in=draw["ratio"], rho_out=1.0,
+                  half_width=draw["half_width"], amp=draw["amp"], tmax=tmax, **kw)
+        out.append((p, c, draw))
+    return out

@@ -154,6 +154,11 @@ class Sim:
         _lib.check(self._L.gk_path(self.h, ctypes.byref(p)), self.h)
         return {0: "generic", 1: "fused2d"}[p.value]
 
+    def set_tiling(self, threads: int, rows: int) -> None:
+        """Tile shape of the fused 2D stage kernel (threads per CTA 64/128/256,
+        rows per segment); see gaukuk_b200.autotune."""
+        _lib.check(self._L.gk_set_tiling(self.h, int(threads), int(rows)), self.h)
+
     def graph_info(self) -> Tuple[int, int]:
         """(whole steps per graph launch, kernel launches per step)."""
         a, b = ctypes.c_int(), ctypes.c_int()

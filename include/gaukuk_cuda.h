@@ -157,6 +157,36 @@ int gk_graph_info(gk_handle* h, int* steps_per_graph, int* launches_per_step);
 int gk_profile_steps(gk_handle* h, int nsteps, char* names, int names_cap,
                      double* total_ms, int* launches, int cap, int* n);
 
+/* Tile shape of the fused 2D stage kernel: threads per CTA (64, 128 or 256;
+ * each CTA updates threads-4 columns) and rows per CTA segment.  Takes effect
+ * from the next run; the project's autotuner (gaukuk_b200/autotune.py) picks
+ * it by measurement. */
+int gk_set_tiling(gk_handle* h, int threads, int rows);
+
+/* Ensembles: independent 2D problems (fused path: vz = 0, RK2, same mode
+ * and device) advanced together.  Every RK stage of every instance is one
+ * persistent launch over a tile table and every ghost fill one launch, held
+ * in a CUDA graph of whole steps; each instance keeps its own handle, clock
+ * and dt, and its results equal those of running it alone.  The handles
+ * stay valid for upload, download and time queries; they must outlive the
+ * ensemble.  No counterpart in the reference, which runs one problem per
+ * process. */
+typedef struct gk_ensemble gk_ensemble;
+int gk_ens_create(gk_handle* const* handles, int n, gk_ensemble** out);
+void gk_ens_destroy(gk_ensemble* e);
+/* threads per CTA (64, 128, 256) for all instances; rows: one entry per
+ * instance, or NULL to keep the current ones (default 16). */
+int gk_ens_set_tiling(gk_ensemble* e, int threads, const int* rows);
+/* Sim::Advance(dtoutput) on every instance, each from its own time. */
+int gk_ens_advance(gk_ensemble* e, double dtoutput);
+/* nsteps steps of every instance (no output time); the enqueue form returns
+ * at once, for timing with events on the ensemble's stream. */
+int gk_ens_run_steps(gk_ensemble* e, int nsteps);
+int gk_ens_enqueue_steps(gk_ensemble* e, int nsteps);
+/* Number of tiles, threads per CTA and the ensemble's CUDA stream. */
+int gk_ens_info(gk_ensemble* e, int* ntiles, int* threads, void** stream);
+const char* gk_ens_last_error(const gk_ensemble* e);
+
 /* Diagnostic of the FAST mode arithmetic: the largest error, in ulp of the
  * IEEE result, of its refined reciprocal, square root and reciprocal square
  * root against CUDA's IEEE division and sqrt, over n arguments spread over

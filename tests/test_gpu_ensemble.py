@@ -1,0 +1,78 @@
+"""Ensembles (persistent launch over a tile table, captured graph): every
+instance must equal the same problem run alone, bit for bit in parity mode,
+dt sequence included, whatever the tile shape."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from gaukuk_b200 import problems
+from helpers import active
+
+pytestmark = pytest.mark.gpu
+
+
+def _instances():
+    out = []
+    for i, (nx, ny) in enumerate([(64, 64), (48, 40), (130, 70), (96, 72), (20, 300), (257, 33)]):
+        p, c = problems.kh(nx, ny=ny, seed=i, rho_in=1.5 + 0.4 * i, half_width=0.2 + 0.015 * i)
+        out.append((dataclasses.replace(p, tmax=0.06, dtoutput=0.03), c))
+    return out
+
+
+def _solo(p, c, mode):
+    from gaukuk_b200.sim import Sim
+    s = Sim(p, c, mode=mode)
+    s.run(p.tmax, p.dtoutput)
+    return active(p, s.download()), s.dt_log()
+
+
+@pytest.mark.parametrize("mode", ["parity", "fast"])
+def test_ensemble_equals_solo_runs(mode):
+    from gaukuk_b200.ensemble import Ensemble
+    from gaukuk_b200.sim import Sim
+    inst = _instances()
+    sims = [Sim(p, c, mode=mode) for p, c in inst]
+    ens = Ensemble(sims)
+    ens.run(0.06, 0.03)
+    for (p, c), s in zip(inst, sims):
+        ref, ref_dts = _solo(p, c, mode)
+        assert s.dt_log() == ref_dts
+        assert np.array_equal(active(p, s.download()), ref)
+
+
+@pytest.mark.parametrize("threads,rows", [(64, [3, 5, 7, 4, 9, 2]), (256, [16] * 6), (128, [32] * 6)])
+def test_ensemble_tiling_does_not_change_results(threads, rows):
+    from gaukuk_b200.ensemble import Ensemble
+    from gaukuk_b200.sim import Sim
+    inst = _instances()
+    sims = [Sim(p, c, mode="parity") for p, c in inst]
+    ens = Ensemble(sims, threads=threads, rows=rows)
+    ens.run_steps(5)
+    for (p, c), s in zip(inst, sims):
+        solo = Sim(p, c, mode="parity")
+        solo.run_steps(5)
+        assert s.dt_log() == solo.dt_log()
+        assert np.array_equal(active(p, s.download()), active(p, solo.download()))
+
+
+@pytest.mark.parametrize("threads,rows", [(64, 5), (256, 3), (128, 64)])
+def test_single_problem_tiling_does_not_change_results(threads, rows):
+    from gaukuk_b200.sim import Sim
+    p, c = problems.kh(150, ny=90, seed=2)
+    a = Sim(p, c, mode="parity")
+    b = Sim(p, c, mode="parity")
+    b.set_tiling(threads, rows)
+    a.run_steps(6)
+    b.run_steps(6)
+    assert a.dt_log() == b.dt_log()
+    assert np.array_equal(active(p, a.download()), active(p, b.download()))
+
+
+def test_autotuner_applies_a_candidate():
+    from gaukuk_b200 import autotune
+    from gaukuk_b200.sim import Sim
+    p, c = problems.kh(256, seed=1)
+    s = Sim(p, c, mode="fast")
+    th, rows, ms = autotune.tune_single(s, steps=2, use_cache=False)
+    assert th in autotune.THREADS and rows in autotune.ROWS and ms > 0
