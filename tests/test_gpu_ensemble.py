@@ -1,13 +1,15 @@
 """Ensembles (persistent launch over a tile table, captured graph): every
 instance must equal the same problem run alone, bit for bit in parity mode,
-dt sequence included, whatever the tile shape."""
+dt sequence included, whatever the tile shape.  In fast mode the compiler
+may contract the ensemble kernel's arithmetic differently from the
+single-problem kernel's, so there the contract is the fast-mode tolerance."""
 import dataclasses
 
 import numpy as np
 import pytest
 
 from gaukuk_b200 import problems
-from helpers import active
+from helpers import active, rel_linf
 
 pytestmark = pytest.mark.gpu
 
@@ -37,8 +39,15 @@ def test_ensemble_equals_solo_runs(mode):
     ens.run(0.06, 0.03)
     for (p, c), s in zip(inst, sims):
         ref, ref_dts = _solo(p, c, mode)
-        assert s.dt_log() == ref_dts
-        assert np.array_equal(active(p, s.download()), ref)
+        dts = s.dt_log()
+        if mode == "parity":
+            assert dts == ref_dts
+            assert np.array_equal(active(p, s.download()), ref)
+        else:
+            assert len(dts) == len(ref_dts)
+            np.testing.assert_allclose(dts, ref_dts, rtol=1e-12)
+            errs = rel_linf(active(p, s.download()), ref)
+            assert max(errs[v] for v in (0, 1, 2, 4)) <= 1e-12, errs
 
 
 @pytest.mark.parametrize("threads,rows", [(64, [3, 5, 7, 4, 9, 2]), (256, [16] * 6), (128, [32] * 6)])
