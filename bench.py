@@ -433,6 +433,67 @@ def main_ensemble(args, rank, world, local_rank):
     return 0
 
 
+def main_learned(args, rank, world, local_rank):
+    """Pattern 4: data from 4x finer plain runs, training on the GPU with the
+    project's BF16 kernels, evaluation on held-out seeds against plain coarse,
+    plain 2x coarse and the 4x fine judge (L1 density error, GPU time)."""
+    import numpy as np
+    import torch
+
+    from gaukuk_b200 import learned
+
+    torch.cuda.set_device(local_rank)
+    log = (lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else None
+    train_seeds = list(range(1000, 1000 + args.train_seeds))
+    eval_seeds = list(range(5000, 5000 + args.eval_seeds))
+    t0 = time.perf_counter()
+    X, Y = learned.generate(train_seeds, coarse=args.coarse, t_end=args.t_end,
+                            snapshots=args.snapshots, frac=args.frac, log=log)
+    t_data = time.perf_counter() - t0
+    blob = learned.init_model(X, Y, seed=0)
+    tr = learned.Trainer(blob, X, Y, device=local_rank)
+    losses = [tr.train(1, batch=args.batch, lr=args.lr)]
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    chunk = max(1, args.train_steps // 10)
+    done = 0
+    while done < args.train_steps:
+        k = min(chunk, args.train_steps - done)
+        losses.append(tr.train(k, batch=args.batch, lr=args.lr, seed=done + 1))
+        done += k
+        if log:
+            log(f"step {done}: loss {losses[-1]:.4g}")
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t1
+    model = tr.model()
+    tr.close()
+    if args.model_out:
+        os.makedirs(os.path.dirname(os.path.abspath(args.model_out)), exist_ok=True)
+        np.save(args.model_out, model)
+    ev = learned.evaluate(model, eval_seeds, coarse=args.coarse, t_end=args.t_end,
+                          times=(0.5 * args.t_end, args.t_end), log=log)
+    sm = ev["summary"]
+    c, c2 = "plain_%d" % args.coarse, "plain_%d" % (2 * args.coarse)
+    lr_ = "learned_%d" % args.coarse
+    if rank == 0:
+        print(json.dumps({
+            "metric": "L1 density error vs 4x fine plain FP64 run, at equal resolution",
+            "workload": f"KH (ensemble parameter ranges), coarse {args.coarse}^2, t = "
+                        f"{0.5 * args.t_end} and {args.t_end}; {len(train_seeds)} training "
+                        f"seeds (fine {4 * args.coarse}^2 restricted), {len(eval_seeds)} held-out",
+            "train": {"samples": int(len(X)), "steps": args.train_steps, "batch": args.batch,
+                      "lr": args.lr, "loss_first": losses[0], "loss_last": losses[-1],
+                      "data_seconds": t_data, "train_seconds": t_train},
+            "summary": sm,
+            "time_ratio_learned_over_plain2x": sm[lr_]["mean_seconds"] / sm[c2]["mean_seconds"],
+            "l1_ratio_learned_over_plain": [a / b for a, b in zip(sm[lr_]["mean_l1_at_%d" % args.coarse],
+                                                                  sm[c]["mean_l1_at_%d" % args.coarse])],
+            "l1_ratio_learned_over_plain2x": [a / b for a, b in zip(sm[lr_]["mean_l1_at_%d" % args.coarse],
+                                                                    sm[c2]["mean_l1_at_%d" % args.coarse])],
+            "model": args.model_out}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=None)
@@ -443,7 +504,17 @@ def main():
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="kh4096", choices=["kh4096", "ensemble"])
+    ap.add_argument("--workload", default="kh4096", choices=["kh4096", "ensemble", "learned"])
+    ap.add_argument("--train-seeds", type=int, default=16)
+    ap.add_argument("--eval-seeds", type=int, default=8)
+    ap.add_argument("--coarse", type=int, default=256)
+    ap.add_argument("--t-end", type=float, default=2.0)
+    ap.add_argument("--snapshots", type=int, default=12)
+    ap.add_argument("--frac", type=float, default=0.25)
+    ap.add_argument("--train-steps", type=int, default=20000)
+    ap.add_argument("--batch", type=int, default=65536)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--model-out", default="")
     ap.add_argument("--ens-n", type=int, default=64)
     ap.add_argument("--ens-tmax", type=float, default=1.0)
     ap.add_argument("--ncu-case", action="store_true",
@@ -461,6 +532,8 @@ def main():
         return main_reference(args, rank, world)
     if args.workload == "ensemble":
         return main_ensemble(args, rank, world, local_rank)
+    if args.workload == "learned":
+        return main_learned(args, rank, world, local_rank)
     return main_ours(args, rank, world, local_rank)
 
 

@@ -69,6 +69,19 @@ SIGNATURES = {
     "gk_ens_enqueue_steps": (ctypes.c_int, [_vp, ctypes.c_int]),
     "gk_ens_info": (ctypes.c_int, [_vp, _ip, _ip, ctypes.POINTER(ctypes.c_void_p)]),
     "gk_ens_last_error": (ctypes.c_char_p, [_vp]),
+    "gk_mlp_nparams": (ctypes.c_int, []),
+    "gk_mlp_nmodel": (ctypes.c_int, []),
+    "gk_mlp_create": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
+    "gk_mlp_destroy": (None, [_vp]),
+    "gk_mlp_get": (ctypes.c_int, [_vp, _vp]),
+    "gk_mlp_grad": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_longlong, ctypes.c_int, _vp, _vp]),
+    "gk_mlp_train": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_float, ctypes.c_ulonglong, _vp]),
+    "gk_mlp_forward": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _vp]),
+    "gk_set_flux_model": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_float, ctypes.c_float]),
+    "gk_flux_model_fired": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint)]),
+    "gk_face_fluxes": (ctypes.c_int, [_vp, _vp, _vp]),
+    "gk_tap_substeps": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _vp]),
     "gk_strerror": (ctypes.c_char_p, [ctypes.c_int]),
     "gk_last_error": (ctypes.c_char_p, [_vp]),
 }

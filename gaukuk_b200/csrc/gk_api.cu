@@ -114,6 +114,9 @@ struct gk_handle {
     bool uploaded = false;
     int upload_step = 0;  // clock step at the last upload
     bool tiling_set = false;  // gk_set_tiling overrides the default tiling
+    float* model = nullptr;   // learned flux correction (device), or null
+    float shock_jump = 0.5f, pos_frac = 0.1f;
+    unsigned* fired = nullptr;  // faces where the detector kept plain HLLC
     int tiling_rows = 0;
     cudaGraphExec_t gexec = nullptr;
     int graph_steps = 0;
@@ -435,6 +438,8 @@ void gk_destroy(gk_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     for (double* p : {h->A, h->B, h->C, h->W, h->F1, h->F2, h->F3, h->dlog}) cudaFree(p);
+    cudaFree(h->model);
+    cudaFree(h->fired);
     cudaFree(h->tm);
     cudaFree(h->dflag);
     if (h->htm) cudaFreeHost(h->htm);
@@ -475,7 +480,7 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
     }
     // (gz != 0 would make MTZ non-zero in the kick, so it also needs the generic path)
     h->path = (g.ndim == 2 && !h->ctx.has_vz && h->ctx.ph.integrator != 1 &&
-               h->ctx.ph.grav[2] == 0) ? 1 : 0;
+               h->ctx.ph.grav[2] == 0 && !h->model) ? 1 : 0;
     h->ctx.h2d_rows = stage_rows(g);
     h->ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
     if (!h->tiling_set) h->ctx.stage_threads = stage_threads_default();
@@ -1042,3 +1047,167 @@ int gk_ens_info(gk_ensemble* e, int* ntiles, int* threads, void** stream) {
 const char* gk_ens_last_error(const gk_ensemble* e) { return e ? e->err.c_str() : ""; }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ flux taps
+// Device side of the learned flux correction's data: face fluxes of the
+// current state, and restricted fine-grid fluxes over fixed sub-steps.
+namespace {
+
+__global__ void k_arm_clock(gk::DevTime* tm, double dt) {
+    tm->dt = dt;
+    tm->active = 1;
+}
+
+__global__ void k_clock_advance(gk::DevTime* tm, double dt, int n) {
+    for (int i = 0; i < n; ++i) tm->t += dt;
+    tm->step += n;
+    tm->active = 0;
+}
+
+// acc[v][jc][ic] += w * sum of the `ratio` fine faces making up the left
+// (x) or lower (y) face of coarse cell (jc, ic).
+__global__ void k_restrict_faces(const double* __restrict__ F, double* __restrict__ acc,
+                                 gk::Geom g, int ratio, int nxc, int nyc, int dir, double w) {
+    const int ic = blockIdx.x * blockDim.x + threadIdx.x;
+    const int jc = blockIdx.y;
+    const int v = blockIdx.z;
+    if (ic >= nxc) return;
+    double s = 0.0;
+    for (int k = 0; k < ratio; ++k) {
+        const int i = dir == 0 ? g.ib + ratio * ic : g.ib + ratio * ic + k;
+        const int j = dir == 0 ? g.jb + ratio * jc + k : g.jb + ratio * jc;
+        s += F[v * g.fvstride + (long long)j * g.fpitch + i];
+    }
+    acc[((long long)v * nyc + jc) * nxc + ic] += w * s;
+}
+
+// Face flux arrays keep DEN, MTX, MTY, ENG in slots 0..3 (gk::Slot).
+int copy_faces(gk_handle* h, const double* F, int dir, double* out) {
+    const gk::Geom& g = h->ctx.g;
+    const int nfx = dir == 0 ? g.nx + 1 : g.nx, nfy = dir == 0 ? g.ny : g.ny + 1;
+    for (int v = 0; v < 4; ++v) {
+        const double* src = F + v * g.fvstride + (long long)g.jb * g.fpitch + g.ib;
+        GK_CUDA(h, cudaMemcpy2DAsync(out + (size_t)v * nfx * nfy, sizeof(double) * nfx, src,
+                                     sizeof(double) * g.fpitch, sizeof(double) * nfx, nfy,
+                                     cudaMemcpyDeviceToHost, h->stream));
+    }
+    return GK_OK;
+}
+
+}  // namespace
+
+extern "C" int gk_face_fluxes(gk_handle* h, double* fx, double* fy) {
+    int rc = check_ready(h);
+    if (rc != GK_OK) return rc;
+    if (h->ctx.g.ndim != 2) return fail(h, GK_ERR_UNSUPPORTED, "face fluxes are provided for 2D runs");
+    rc = alloc_generic(h);
+    if (rc != GK_OK) return rc;
+    const KernelSet& k = *h->ks;
+    k_arm_clock<<<1, 1, 0, h->stream>>>(h->tm, 0.0);
+    k.bc(h->ctx, h->A, h->stream);
+    k.c2p(h->ctx, h->A, h->W, h->stream);
+    k.flux(h->ctx, 0, h->W, h->F1, h->stream);
+    k.flux(h->ctx, 1, h->W, h->F2, h->stream);
+    GK_CUDA(h, cudaGetLastError());
+    if (fx && (rc = copy_faces(h, h->F1, 0, fx)) != GK_OK) return rc;
+    if (fy && (rc = copy_faces(h, h->F2, 1, fy)) != GK_OK) return rc;
+    k_clock_advance<<<1, 1, 0, h->stream>>>(h->tm, 0.0, 0);
+    GK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return GK_OK;
+}
+
+extern "C" int gk_tap_substeps(gk_handle* h, int nsub, double dt_sub, int ratio, double* fx_acc,
+                               double* fy_acc) {
+    int rc = check_ready(h);
+    if (rc != GK_OK) return rc;
+    const gk::Geom& g = h->ctx.g;
+    if (g.ndim != 2 || h->ctx.ph.integrator != 2 || h->ctx.ph.has_grav)
+        return fail(h, GK_ERR_UNSUPPORTED, "flux taps need a 2D RK2 run without sources");
+    if (ratio < 1 || nsub < 1 || g.nx % ratio || g.ny % ratio || !(dt_sub > 0))
+        return fail(h, GK_ERR_INVALID, "ratio must divide the grid; nsub, dt_sub positive");
+    rc = alloc_generic(h);
+    if (rc != GK_OK) return rc;
+    const int nxc = g.nx / ratio, nyc = g.ny / ratio;
+    const size_t nacc = (size_t)4 * nxc * nyc;
+    double* acc = nullptr;
+    GK_CUDA(h, cudaMallocAsync(&acc, 2 * nacc * sizeof(double), h->stream));
+    GK_CUDA(h, cudaMemsetAsync(acc, 0, 2 * nacc * sizeof(double), h->stream));
+    const KernelSet& k = *h->ks;
+    const gk::Ctx& c = h->ctx;
+    cudaStream_t s = h->stream;
+    // RK2 stage weight 1/2, time average 1/nsub, face average 1/ratio
+    const double w = 0.5 / nsub / ratio;
+    const dim3 grid((nxc + 127) / 128, nyc, 4);
+    k_arm_clock<<<1, 1, 0, s>>>(h->tm, dt_sub);
+    for (int n = 0; n < nsub; ++n) {
+        for (int stage = 0; stage < 2; ++stage) {
+            double* u = stage == 0 ? h->A : h->B;
+            k.bc(c, u, s);
+            k.c2p(c, u, h->W, s);
+            k.flux(c, 0, h->W, h->F1, s);
+            k.flux(c, 1, h->W, h->F2, s);
+            k_restrict_faces<<<grid, 128, 0, s>>>(h->F1, acc, g, ratio, nxc, nyc, 0, w);
+            k_restrict_faces<<<grid, 128, 0, s>>>(h->F2, acc + nacc, g, ratio, nxc, nyc, 1, w);
+            if (stage == 0)
+                k.update(c, nullptr, h->A, h->B, h->F1, h->F2, h->F3, 0, 1.0, 1.0, 0.0, s);
+            else
+                k.update(c, h->A, h->B, h->A, h->F1, h->F2, h->F3, 1, 0.5, 0.5, 0.5, s);
+        }
+    }
+    k_clock_advance<<<1, 1, 0, s>>>(h->tm, dt_sub, nsub);
+    k.cfl(c, h->A, 0, s);  // cmax of the new state for the next step's dt
+    GK_CUDA(h, cudaGetLastError());
+    if (fx_acc) GK_CUDA(h, cudaMemcpyAsync(fx_acc, acc, nacc * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (fy_acc)
+        GK_CUDA(h, cudaMemcpyAsync(fy_acc, acc + nacc, nacc * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GK_CUDA(h, cudaFreeAsync(acc, s));
+    GK_CUDA(h, cudaStreamSynchronize(s));
+    return pull_time(h);
+}
+
+// ------------------------------------------------------------ learned correction on a handle
+extern "C" int gk_set_flux_model(gk_handle* h, const float* model_host, int nmodel,
+                                 float shock_jump, float pos_frac) {
+    if (!h) return GK_ERR_INVALID;
+    GK_CUDA(h, cudaSetDevice(h->device));
+    if (!model_host) {
+        cudaFree(h->model);
+        h->model = nullptr;
+    } else {
+        if (h->ctx.g.ndim != 2) return fail(h, GK_ERR_UNSUPPORTED, "the flux model is for 2D runs");
+        if (nmodel != gk_mlp_nmodel()) return fail(h, GK_ERR_INVALID, "model size mismatch");
+        if (!h->model) GK_CUDA(h, cudaMalloc(&h->model, sizeof(float) * nmodel));
+        if (!h->fired) {
+            GK_CUDA(h, cudaMalloc(&h->fired, sizeof(unsigned)));
+            GK_CUDA(h, cudaMemset(h->fired, 0, sizeof(unsigned)));
+        }
+        GK_CUDA(h, cudaMemcpy(h->model, model_host, sizeof(float) * nmodel, cudaMemcpyHostToDevice));
+        h->shock_jump = shock_jump;
+        h->pos_frac = pos_frac;
+        int rc = alloc_generic(h);
+        if (rc != GK_OK) return rc;
+    }
+    // the path and the graph follow the model
+    if (h->uploaded) {
+        const gk::Geom& g = h->ctx.g;
+        h->path = (g.ndim == 2 && !h->ctx.has_vz && h->ctx.ph.integrator != 1 &&
+                   h->ctx.ph.grav[2] == 0 && !h->model) ? 1 : 0;
+        if (h->path == 0) {
+            int rc = alloc_generic(h);
+            if (rc != GK_OK) return rc;
+        }
+    }
+    if (h->gexec) {
+        cudaGraphExecDestroy(h->gexec);
+        h->gexec = nullptr;
+    }
+    return GK_OK;
+}
+
+extern "C" int gk_flux_model_fired(gk_handle* h, unsigned* fired) {
+    if (!h || !fired) return GK_ERR_INVALID;
+    *fired = 0;
+    if (!h->fired) return GK_OK;
+    GK_CUDA(h, cudaMemcpy(fired, h->fired, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    return GK_OK;
+}

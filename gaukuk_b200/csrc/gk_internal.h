@@ -94,6 +94,12 @@ struct alignas(64) EnsInst {
 // 4) doubles, box (nt, 1, 4), no swizzle, zero fill out of bounds (gk_api.cu).
 bool encode_rows_map(CUtensorMap* map, const double* base, const Geom& g, int nt);
 
+// The learned flux correction of one direction of a generic-path stage
+// (gk_mlp.cu).
+void launch_flux_correct(const float* model, const double* W, double* F, const Geom& g,
+                         const Phys& ph, const DevTime* tm, int dir, float shock_jump,
+                         float pos_frac, unsigned* fired, cudaStream_t s);
+
 // Kernel classes, for per-kernel profiling.
 enum KClass { K_BC = 0, K_C2P, K_FLUX, K_UPDATE, K_KICK, K_CFL, K_STAGE, K_BEGIN, K_NCLASS };
 static const char* const kClassNames[K_NCLASS] = {

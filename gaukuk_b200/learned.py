@@ -1,0 +1,341 @@
+"""Learned flux correction for coarse grids (pattern 4).
+
+A small MLP (16 -> 64 -> 64 -> 4, GELU) predicts, for every face of a coarse
+grid, the difference between the flux a 4x finer run pushes through that face
+(averaged over the fine faces, the RK stages and the fine steps) and the HLLC
+flux of the coarse state.  The coarse solver adds the prediction to its FP64
+HLLC flux at every stage (gk_set_flux_model), so the update stays conservative;
+a shock / positivity detector keeps plain HLLC where it fires.
+
+Everything that touches the grid runs in libgk_cuda.so: the fine runs, the
+flux taps (gk_tap_substeps), the coarse HLLC fluxes (gk_face_fluxes), training
+(gk_mlp_train: BF16 tensor-core forward, hand-written backward, Adam) and the
+corrected coarse runs.  NumPy only assembles stencils and statistics.
+
+Features per face (``face_features``): the 4 cells across the face, each as
+(rho/rho_ref - 1, vn/c_ref, vt/c_ref, p/p_ref - 1), rho_ref and p_ref the
+stencil means, c_ref = sqrt(gamma p_ref / rho_ref); targets are scaled by
+rho_ref*c_ref (mass), rho_ref*c_ref^2 (momenta), rho_ref*c_ref^3 (energy).
+The kernel k_flux_correct forms the same quantities on the device.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import time
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib, problems
+from .config import Params
+
+NI, NH, NO = 16, 64, 4
+NPARAM = NH * NI + NH + NH * NH + NH + NO * NH + NO
+NMODEL = NPARAM + 2 * NI + 2 * NO
+
+
+# ------------------------------------------------------------------ grid helpers
+def restrict(p: Params, cons: np.ndarray, ratio: int) -> Tuple[Params, np.ndarray]:
+    """Conservative restriction of a 2D state (block means of the active cells)."""
+    g = p.ng
+    q = dataclasses.replace(p, nx=p.nx // ratio, ny=p.ny // ratio)
+    a = cons[:, g, g:g + p.ny, g:g + p.nx]
+    a = a.reshape(5, q.ny, ratio, q.nx, ratio).mean(axis=(2, 4))
+    out = np.zeros(q.shape)
+    out[:, q.ng, q.ng:q.ng + q.ny, q.ng:q.ng + q.nx] = a
+    return q, out
+
+
+def active2d(p: Params, cons: np.ndarray) -> np.ndarray:
+    g = p.ng
+    return cons[:, g, g:g + p.ny, g:g + p.nx]
+
+
+def primitives(p: Params, a: np.ndarray):
+    """ConsToPrim (adiabatic.cpp:41-57) on active cells: rho, vx, vy, p."""
+    d = np.maximum(a[0], p.dfloor)
+    inv = 1.0 / d
+    vx, vy = a[1] * inv, a[2] * inv
+    ek = 0.5 * inv * (a[1] * a[1] + a[2] * a[2] + a[3] * a[3])
+    pre = np.maximum((p.gamma - 1.0) * (a[4] - ek), p.pfloor)
+    return d, vx, vy, pre
+
+
+def face_features(p: Params, a: np.ndarray, direction: int):
+    """Features (n, 16) and scales (n, 3) of the left (x) or lower (y) face of
+    every active cell of a periodic 2D state."""
+    rho, vx, vy, pre = primitives(p, a)
+    ax = 1 if direction == 0 else 0
+    vn, vt = (vx, vy) if direction == 0 else (vy, vx)
+    st = [np.roll(f, s, axis=ax) for s in (2, 1, 0, -1)
+          for f in (rho, vn, vt, pre)]  # cells -2, -1, 0, +1 relative to the face
+    r = [st[4 * c + 0] for c in range(4)]
+    pr = [st[4 * c + 3] for c in range(4)]
+    rr = 0.25 * (r[0] + r[1] + r[2] + r[3])
+    pp = 0.25 * (pr[0] + pr[1] + pr[2] + pr[3])
+    cr = np.sqrt(p.gamma * pp / rr)
+    feats = []
+    for c in range(4):
+        feats += [st[4 * c + 0] / rr - 1.0, st[4 * c + 1] / cr, st[4 * c + 2] / cr,
+                  st[4 * c + 3] / pp - 1.0]
+    X = np.stack([f.ravel() for f in feats], axis=1)
+    S = np.stack([(rr * cr).ravel(), (rr * cr * cr).ravel(), (rr * cr ** 3).ravel()], axis=1)
+    return X, S
+
+
+def rotate_to_face(delta: np.ndarray, direction: int) -> np.ndarray:
+    """(DEN, MTX, MTY, ENG) planes -> (mass, normal, tangential, energy) columns."""
+    d, mx, my, e = delta
+    n, t = (mx, my) if direction == 0 else (my, mx)
+    return np.stack([d.ravel(), n.ravel(), t.ravel(), e.ravel()], axis=1)
+
+
+# ------------------------------------------------------------------ device views
+def _ptr(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def face_fluxes(sim) -> Tuple[np.ndarray, np.ndarray]:
+    """HLLC face fluxes of a Sim's current state: x [4][ny][nx+1], y [4][ny+1][nx]."""
+    p = sim.params
+    fx = np.empty((4, p.ny, p.nx + 1))
+    fy = np.empty((4, p.ny + 1, p.nx))
+    _lib.check(sim._L.gk_face_fluxes(sim.h, fx.ctypes.data_as(ctypes.c_void_p),
+                                     fy.ctypes.data_as(ctypes.c_void_p)), sim.h)
+    return fx, fy
+
+
+def tap(sim, nsub: int, dt_sub: float, ratio: int) -> Tuple[np.ndarray, np.ndarray]:
+    """Advance nsub fixed steps; restricted face fluxes [4][ny/r][nx/r] x and y."""
+    p = sim.params
+    nxc, nyc = p.nx // ratio, p.ny // ratio
+    fx = np.empty((4, nyc, nxc))
+    fy = np.empty((4, nyc, nxc))
+    _lib.check(sim._L.gk_tap_substeps(sim.h, int(nsub), float(dt_sub), int(ratio),
+                                      fx.ctypes.data_as(ctypes.c_void_p),
+                                      fy.ctypes.data_as(ctypes.c_void_p)), sim.h)
+    return fx, fy
+
+
+# ------------------------------------------------------------------ data
+def kh_instance(seed: int, n: int, tmax: float) -> Tuple[Params, np.ndarray, Dict]:
+    """One KH problem with the ensemble's parameter ranges, at resolution n."""
+    rng = np.random.default_rng(seed)
+    draw = {"ratio": float(rng.uniform(1.5, 4.0)), "half_width": float(rng.uniform(0.2, 0.3)),
+            "amp": float(rng.uniform(0.005, 0.02))}
+    p, c = problems.kh(n, seed=seed, rho_in=draw["ratio"], rho_out=1.0,
+                       half_width=draw["half_width"], amp=draw["amp"], tmax=tmax)
+    return p, c, draw
+
+
+def generate(seeds: Sequence[int], coarse: int = 256, ratio: int = 4, t_end: float = 2.0,
+             snapshots: int = 16, frac: float = 0.25, mode: str = "fast",
+             sample_seed: int = 0, log=print) -> Tuple[np.ndarray, np.ndarray]:
+    """Training pairs from fine runs (coarse*ratio)^2 restricted to coarse^2.
+
+    At `snapshots` times spread over (0, t_end] the fine state is restricted,
+    the coarse HLLC fluxes of the restricted state are computed, and the fine
+    run is advanced by one coarse CFL step in `ratio` fixed sub-steps while
+    the fluxes through the coarse faces are accumulated; the target is their
+    difference.  A fraction `frac` of the faces of each snapshot is kept."""
+    from .sim import Sim
+    rng = np.random.default_rng(sample_seed)
+    Xs, Ys = [], []
+    for k, seed in enumerate(seeds):
+        t0 = time.time()
+        pf, cf, _ = kh_instance(seed, coarse * ratio, t_end)
+        fine = Sim(pf, cf, mode=mode)
+        pc, cc = restrict(pf, cf, ratio)
+        crs = Sim(pc, cc, mode=mode)
+        drmin_c = min((pc.xmax - pc.xmin) / pc.nx, (pc.ymax - pc.ymin) / pc.ny)
+        for s in range(1, snapshots + 1):
+            ts = t_end * s / (snapshots + 1)
+            t = fine.get_time()
+            if ts > t + 1e-12:
+                fine.advance(ts - t)
+            _, cc = restrict(pf, fine.download(), ratio)
+            crs.set_time(0.0, 0)
+            crs.upload(cc)
+            fx_c, fy_c = face_fluxes(crs)
+            dt_c = pc.cfl * drmin_c / crs.cmax()
+            fx_f, fy_f = tap(fine, ratio, dt_c / ratio, ratio)
+            a = active2d(pc, cc)
+            for direction, Ff, Fc in ((0, fx_f, fx_c[:, :, :pc.nx]), (1, fy_f, fy_c[:, :pc.ny, :])):
+                X, S = face_features(pc, a, direction)
+                D = rotate_to_face(Ff - Fc, direction)
+                Y = np.stack([D[:, 0] / S[:, 0], D[:, 1] / S[:, 1], D[:, 2] / S[:, 1],
+                              D[:, 3] / S[:, 2]], axis=1)
+                keep = rng.random(len(X)) < frac
+                Xs.append(X[keep].astype(np.float32))
+                Ys.append(Y[keep].astype(np.float32))
+        fine.close()
+        crs.close()
+        if log:
+            log(f"instance {k + 1}/{len(seeds)} (seed {seed}): {time.time() - t0:.1f} s")
+    return np.concatenate(Xs), np.concatenate(Ys)
+
+
+# ------------------------------------------------------------------ model
+def init_model(X: np.ndarray, Y: np.ndarray, seed: int = 0) -> np.ndarray:
+    """He-initialised weights, zero biases, small last layer, and the data's
+    standardisation appended (gk_mlp model blob)."""
+    rng = np.random.default_rng(seed)
+    w1 = rng.normal(0, np.sqrt(2.0 / NI), (NH, NI))
+    w2 = rng.normal(0, np.sqrt(2.0 / NH), (NH, NH))
+    w3 = rng.normal(0, 0.1 * np.sqrt(1.0 / NH), (NO, NH))
+    xm, xs = X.mean(0), X.std(0) + 1e-6
+    ym, ys = Y.mean(0), Y.std(0) + 1e-12
+    blob = np.concatenate([w1.ravel(), np.zeros(NH), w2.ravel(), np.zeros(NH), w3.ravel(),
+                           np.zeros(NO), xm, xs, ym, ys]).astype(np.float32)
+    assert blob.size == NMODEL
+    return blob
+
+
+def standardise(blob: np.ndarray, X: np.ndarray, Y: Optional[np.ndarray] = None):
+    xm, xs = blob[NPARAM:NPARAM + NI], blob[NPARAM + NI:NPARAM + 2 * NI]
+    Xn = (X - xm) / xs
+    if Y is None:
+        return Xn
+    ym, ys = blob[NPARAM + 2 * NI:NPARAM + 2 * NI + NO], blob[NPARAM + 2 * NI + NO:]
+    return Xn, (Y - ym) / ys
+
+
+class Trainer:
+    """Device-side training state (gk_mlp): the model, Adam moments and the
+    standardised data set in HBM (BF16 inputs, FP32 targets)."""
+
+    def __init__(self, blob: np.ndarray, X: np.ndarray, Y: np.ndarray, device: int = 0):
+        import torch
+        self._L = _lib.load()
+        b = np.ascontiguousarray(blob, dtype=np.float32)
+        m = ctypes.c_void_p()
+        _lib.check(self._L.gk_mlp_create(b.ctypes.data_as(ctypes.c_void_p), ctypes.byref(m)))
+        self.m = m
+        Xn, Yn = standardise(b, X, Y)
+        dev = torch.device("cuda", device)
+        self.X = torch.from_numpy(np.ascontiguousarray(Xn, dtype=np.float32)).to(dev).to(torch.bfloat16)
+        self.Y = torch.from_numpy(np.ascontiguousarray(Yn, dtype=np.float32)).to(dev)
+        self.n = len(X)
+
+    def close(self):
+        if getattr(self, "m", None):
+            self._L.gk_mlp_destroy(self.m)
+            self.m = None
+
+    def train(self, steps: int, batch: int = 65536, lr: float = 1e-3, seed: int = 0) -> float:
+        loss = ctypes.c_float()
+        _lib.check(self._L.gk_mlp_train(self.m, _ptr(self.X), _ptr(self.Y), self.n, int(batch),
+                                        int(steps), float(lr), int(seed), ctypes.byref(loss)))
+        return loss.value
+
+    def gradient(self, batch: int):
+        g = np.empty(NPARAM, dtype=np.float32)
+        loss = ctypes.c_float()
+        _lib.check(self._L.gk_mlp_grad(self.m, _ptr(self.X), _ptr(self.Y), self.n, int(batch),
+                                       g.ctypes.data_as(ctypes.c_void_p), ctypes.byref(loss)))
+        return g, loss.value
+
+    def forward(self, n: Optional[int] = None) -> np.ndarray:
+        import torch
+        n = self.n if n is None else n
+        out = torch.empty((n, NO), dtype=torch.float32, device=self.Y.device)
+        _lib.check(self._L.gk_mlp_forward(self.m, _ptr(self.X), int(n), _ptr(out)))
+        return out.cpu().numpy()
+
+    def model(self) -> np.ndarray:
+        b = np.empty(NMODEL, dtype=np.float32)
+        _lib.check(self._L.gk_mlp_get(self.m, b.ctypes.data_as(ctypes.c_void_p)))
+        return b
+
+
+def install(sim, blob: Optional[np.ndarray], shock_jump: float = 0.5, pos_frac: float = 0.1):
+    """Installs (or, with None, removes) the correction on a 2D Sim."""
+    if blob is None:
+        _lib.check(sim._L.gk_set_flux_model(sim.h, None, 0, 0.0, 0.0), sim.h)
+        return
+    b = np.ascontiguousarray(blob, dtype=np.float32)
+    _lib.check(sim._L.gk_set_flux_model(sim.h, b.ctypes.data_as(ctypes.c_void_p), b.size,
+                                        float(shock_jump), float(pos_frac)), sim.h)
+
+
+def detector_count(sim) -> int:
+    c = ctypes.c_uint()
+    _lib.check(sim._L.gk_flux_model_fired(sim.h, ctypes.byref(c)), sim.h)
+    return c.value
+
+
+# ------------------------------------------------------------------ evaluation
+def _timed_run(sim, times: Sequence[float]) -> Tuple[List[np.ndarray], float]:
+    """Runs to each time in `times`; returns the density at each and the GPU
+    wall time spent inside the advance calls."""
+    import torch
+    out, spent = [], 0.0
+    for tt in times:
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        sim.advance(tt - sim.get_time())
+        torch.cuda.synchronize()
+        spent += time.perf_counter() - a
+        out.append(active2d(sim.params, sim.download())[0].copy())
+    return out, spent
+
+
+def _restrict_rho(rho: np.ndarray, r: int) -> np.ndarray:
+    ny, nx = rho.shape
+    return rho.reshape(ny // r, r, nx // r, r).mean(axis=(1, 3))
+
+
+def evaluate(blob: np.ndarray, seeds: Sequence[int], coarse: int = 256, t_end: float = 2.0,
+             times: Sequence[float] = (0.5, 1.0, 2.0), mode: str = "fast",
+             shock_jump: float = 0.5, pos_frac: float = 0.1, log=print) -> Dict:
+    """L1 density error against the 4x fine plain run (the judge) for plain
+    coarse, plain 2x coarse and learned coarse, each started from the
+    restriction of the same fine initial state, and their GPU times."""
+    from .sim import Sim
+    rows = []
+    for seed in seeds:
+        pf, cf, draw = kh_instance(seed, 4 * coarse, t_end)
+        judge, _ = _timed_run(Sim(pf, cf, mode=mode), times)
+        res = {"seed": seed, **draw}
+        for name, ratio, learned in (("plain_%d" % coarse, 4, False),
+                                     ("plain_%d" % (2 * coarse), 2, False),
+                                     ("learned_%d" % coarse, 4, True)):
+            pc, cc = restrict(pf, cf, ratio)
+            s = Sim(pc, cc, mode=mode)
+            if learned:
+                install(s, blob, shock_jump, pos_frac)
+            s.run_steps(1)  # build the graph outside the timing
+            s.set_time(0.0, 0)
+            s.upload(cc)
+            rho, secs = _timed_run(s, times)
+            m0 = active2d(pc, cc)[0].sum()
+            res[name] = {
+                "seconds": secs,
+                "l1": [float(np.mean(np.abs(r - _restrict_rho(j, ratio)))) for r, j in zip(rho, judge)],
+                "l1_at_%d" % coarse: [float(np.mean(np.abs(_restrict_rho(r, 4 // ratio) - _restrict_rho(j, 4))))
+                                      for r, j in zip(rho, judge)],
+                "mass_drift": float(abs(rho[-1].sum() - m0) / m0),
+            }
+            if learned:
+                res[name]["detector_faces"] = detector_count(s)
+            s.close()
+        rows.append(res)
+        if log:
+            log(json_line(res))
+    return {"runs": rows, "summary": summarise(rows, coarse)}
+
+
+def json_line(d) -> str:
+    import json
+    return json.dumps(d)
+
+
+def summarise(rows: List[Dict], coarse: int) -> Dict:
+    keys = ["plain_%d" % coarse, "plain_%d" % (2 * coarse), "learned_%d" % coarse]
+    out = {}
+    for k in keys:
+        l1 = np.array([r[k]["l1_at_%d" % coarse] for r in rows])
+        out[k] = {"mean_l1_at_%d" % coarse: l1.mean(axis=0).tolist(),
+                  "mean_seconds": float(np.mean([r[k]["seconds"] for r in rows]))}
+    return out

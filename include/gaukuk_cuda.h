@@ -187,6 +187,53 @@ int gk_ens_enqueue_steps(gk_ensemble* e, int nsteps);
 int gk_ens_info(gk_ensemble* e, int* ntiles, int* threads, void** stream);
 const char* gk_ens_last_error(const gk_ensemble* e);
 
+/* ---- Learned flux correction (no counterpart in the reference) ----
+ * A 16 -> 64 -> 64 -> 4 MLP with GELU predicts a correction to each face's
+ * HLLC flux on a coarse grid from the 4-cell stencil of primitives across
+ * the face; it is trained to the restricted fluxes of a finer run.  Model
+ * blob (gk_mlp_nmodel() floats): W1[64][16] b1[64] W2[64][64] b2[64]
+ * W3[4][64] b3[4] (gk_mlp_nparams() parameters), then the input means[16],
+ * input deviations[16], output means[4], output deviations[4].  Training and
+ * inference run in BF16 on the tensor cores with FP32 accumulation
+ * (gaukuk_b200/csrc/gk_mlp.cu); the correction is added to the FP64 flux. */
+typedef struct gk_mlp gk_mlp;
+int gk_mlp_nparams(void);
+int gk_mlp_nmodel(void);
+int gk_mlp_create(const float* model_host, gk_mlp** out);
+void gk_mlp_destroy(gk_mlp* m);
+int gk_mlp_get(gk_mlp* m, float* model_host);
+/* Summed gradient of the first `batch` samples (no update).  X: n x 16 BF16
+ * and T: n x 4 FP32 (standardised), on the device. */
+int gk_mlp_grad(gk_mlp* m, const void* X, const float* T, long long n, int batch,
+                float* grad_host, float* loss_host);
+/* `steps` Adam steps (b1 0.9, b2 0.999, eps 1e-8) on batches drawn with
+ * replacement; *loss_host: mean squared error of the last batch. */
+int gk_mlp_train(gk_mlp* m, const void* X, const float* T, long long n, int batch, int steps,
+                 float lr, unsigned long long seed, float* loss_host);
+/* Standardised outputs of n samples (device X, device Y n x 4). */
+int gk_mlp_forward(gk_mlp* m, const void* X, long long n, float* Y);
+
+/* Installs (model_host != NULL) or removes the correction on a 2D handle:
+ * every stage then adds the network's correction to each face flux, except
+ * where the detector fires -- a pressure ratio above 1 + shock_jump over the
+ * stencil, or a correction moving more than pos_frac of an adjacent cell's
+ * mass or internal energy in one step -- which keeps plain HLLC there. */
+int gk_set_flux_model(gk_handle* h, const float* model_host, int nmodel, float shock_jump,
+                      float pos_frac);
+/* Faces where the detector has fired since the model was installed. */
+int gk_flux_model_fired(gk_handle* h, unsigned* fired);
+
+/* Training data: the HLLC face fluxes of the current state (2D; DEN, MTX,
+ * MTY, ENG planes; x faces [4][ny][nx+1], y faces [4][ny+1][nx], host). */
+int gk_face_fluxes(gk_handle* h, double* fx, double* fy);
+/* Advances a 2D RK2 run by nsub steps of fixed dt_sub and returns the
+ * fluxes through the faces of the grid coarsened by `ratio`, averaged over
+ * the fine faces of each coarse face, the two RK stages and the steps:
+ * fx_acc, fy_acc [4][ny/ratio][nx/ratio] (left / lower face of each coarse
+ * cell), host. */
+int gk_tap_substeps(gk_handle* h, int nsub, double dt_sub, int ratio, double* fx_acc,
+                    double* fy_acc);
+
 /* Diagnostic of the FAST mode arithmetic: the largest error, in ulp of the
  * IEEE result, of its refined reciprocal, square root and reciprocal square
  * root against CUDA's IEEE division and sqrt, over n arguments spread over

@@ -1,0 +1,130 @@
+"""The learned flux correction on the GPU: training kernels against the CPU
+oracle, the flux tap's conservation identity, and the corrected solver's
+fall-back and conservation properties."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from gaukuk_b200 import learned, problems
+from helpers import active
+
+pytestmark = pytest.mark.gpu
+mlp_oracle = pytest.importorskip("mlp_oracle")
+
+
+def _data(n=2048, seed=0):
+    rng = np.random.default_rng(seed)
+    X = rng.normal(size=(n, 16))
+    a = rng.normal(size=(16, 4))
+    Y = np.tanh(X @ a * 0.3) + 0.05 * rng.normal(size=(n, 4))
+    return X.astype(np.float32), Y.astype(np.float32)
+
+
+def test_gradient_matches_cpu_oracle():
+    X, Y = _data(1024)
+    blob = learned.init_model(X, Y, seed=3)
+    tr = learned.Trainer(blob, X, Y)
+    g, loss = tr.gradient(1024)
+    Xn, Yn = learned.standardise(blob, X, Y)
+    l_ref, g_ref, _ = mlp_oracle.forward_backward(blob[:learned.NPARAM], Xn, Yn, rounding=True)
+    assert abs(loss - l_ref) <= 1e-3 * l_ref
+    err = np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
+    assert err < 1e-2, err
+    # and per block (W1, b1, W2, b2, W3, b3)
+    cuts = np.cumsum([0, 1024, 64, 4096, 64, 256, 4])
+    for a, b in zip(cuts[:-1], cuts[1:]):
+        e = np.linalg.norm(g[a:b] - g_ref[a:b]) / (np.linalg.norm(g_ref[a:b]) + 1e-30)
+        assert e < 3e-2, (a, b, e)
+    tr.close()
+
+
+def test_forward_matches_cpu_oracle():
+    X, Y = _data(512, seed=1)
+    blob = learned.init_model(X, Y, seed=4)
+    tr = learned.Trainer(blob, X, Y)
+    y = tr.forward()
+    Xn, Yn = learned.standardise(blob, X, Y)
+    _, _, y_ref = mlp_oracle.forward_backward(blob[:learned.NPARAM], Xn, Yn, rounding=True)
+    assert np.max(np.abs(y - y_ref)) < 1e-3 * (1 + np.max(np.abs(y_ref)))
+    tr.close()
+
+
+def test_training_reduces_loss():
+    X, Y = _data(8192, seed=2)
+    blob = learned.init_model(X, Y, seed=5)
+    tr = learned.Trainer(blob, X, Y)
+    l0 = tr.train(1, batch=1024, lr=1e-3)
+    l1 = tr.train(600, batch=1024, lr=3e-3)
+    assert l1 < 0.2 * l0, (l0, l1)
+    tr.close()
+
+
+def test_flux_tap_is_the_restricted_update():
+    """The fine run's update restricted to the coarse grid equals the coarse
+    flux divergence of the tapped fluxes (RK2 is u - dt/2 (dF(u) + dF(u*)))."""
+    from gaukuk_b200.sim import Sim
+    p, c = problems.kh(128, seed=4)
+    s = Sim(p, c, mode="parity")
+    s.run_steps(3)
+    r = 4
+    q, u0 = learned.restrict(p, s.download(), r)
+    nsub, dt = 4, 2e-4
+    fx, fy = learned.tap(s, nsub, dt, r)
+    _, u1 = learned.restrict(p, s.download(), r)
+    a0, a1 = learned.active2d(q, u0), learned.active2d(q, u1)
+    T = nsub * dt
+    dx, dy = 1.0 / q.nx, 1.0 / q.ny
+    for v, pl in ((0, 0), (1, 1), (2, 2), (4, 3)):
+        div = (np.roll(fx[pl], -1, axis=1) - fx[pl]) / dx + (np.roll(fy[pl], -1, axis=0) - fy[pl]) / dy
+        pred = a0[v] - T * div
+        err = np.max(np.abs(pred - a1[v])) / np.max(np.abs(a1[v]))
+        assert err < 1e-12, (v, err)
+    assert len(s.dt_log()) == 3 and abs(s.get_time() - (sum(s.dt_log()) + T)) < 1e-12
+
+
+def test_zero_model_is_plain_hllc_bitwise():
+    from gaukuk_b200.sim import Sim
+    p, c = problems.kh(96, ny=80, seed=1)
+    blob = np.zeros(learned.NMODEL, dtype=np.float32)
+    blob[learned.NPARAM + 16:learned.NPARAM + 32] = 1.0  # input deviations
+    blob[learned.NPARAM + 36:] = 1.0                    # output deviations
+    a, b = Sim(p, c, mode="parity"), Sim(p, c, mode="parity")
+    learned.install(b, blob)
+    assert b.path == "generic"
+    a.run_steps(12)
+    b.run_steps(12)
+    assert a.dt_log() == b.dt_log()
+    assert np.array_equal(active(p, a.download()), active(p, b.download()))
+
+
+def test_detector_fallback_is_plain_hllc():
+    """With pos_frac = 0 every correction trips the positivity detector, so
+    the corrected solver must reproduce plain HLLC exactly."""
+    from gaukuk_b200.sim import Sim
+    p, c = problems.kh(64, seed=2)
+    X, Y = _data(256)
+    blob = learned.init_model(X, Y, seed=6)
+    a, b = Sim(p, c, mode="parity"), Sim(p, c, mode="parity")
+    learned.install(b, blob, shock_jump=0.5, pos_frac=0.0)
+    a.run_steps(6)
+    b.run_steps(6)
+    assert np.array_equal(active(p, a.download()), active(p, b.download()))
+    assert learned.detector_count(b) == 6 * 2 * 2 * 64 * 65
+
+
+def test_corrected_run_conserves_mass_and_changes_the_solution():
+    from gaukuk_b200.sim import Sim
+    p, c = problems.kh(128, seed=3)
+    X, Y = _data(256)
+    blob = learned.init_model(X, Y, seed=7)
+    blob[learned.NPARAM + 36:] *= 1e-4  # small corrections
+    a, b = Sim(p, c, mode="fast"), Sim(p, c, mode="fast")
+    learned.install(b, blob, shock_jump=0.5, pos_frac=0.5)
+    a.run_steps(20)
+    b.run_steps(20)
+    ma, mb = active(p, a.download()), active(p, b.download())
+    m0 = active(p, c)[0].sum()
+    assert abs(mb[0].sum() - m0) / m0 < 1e-13
+    assert abs(mb[4].sum() - active(p, c)[4].sum()) / active(p, c)[4].sum() < 1e-13
+    assert not np.array_equal(ma, mb)
