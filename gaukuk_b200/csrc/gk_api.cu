@@ -335,6 +335,13 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
         GK_L(gk::K_FLUX, k.flux(c, 0, h->W, h->F1, s));
         if (c.g.ndim >= 2) GK_L(gk::K_FLUX, k.flux(c, 1, h->W, h->F2, s));
         if (c.g.ndim == 3) GK_L(gk::K_FLUX, k.flux(c, 2, h->W, h->F3, s));
+        if (h->model) {
+            // learned correction of the face fluxes (gk_mlp.cu)
+            GK_L(gk::K_FLUX, gk::launch_flux_correct(h->model, h->W, h->F1, c.g, c.ph, c.tm, 0,
+                                                     h->shock_jump, h->pos_frac, h->fired, s));
+            GK_L(gk::K_FLUX, gk::launch_flux_correct(h->model, h->W, h->F2, c.g, c.ph, c.tm, 1,
+                                                     h->shock_jump, h->pos_frac, h->fired, s));
+        }
     };
     GK_L(gk::K_BC, k.bc(c, A, s));
     fluxes(A);
