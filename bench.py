@@ -447,9 +447,14 @@ def main_learned(args, rank, world, local_rank):
     train_seeds = list(range(1000, 1000 + args.train_seeds))
     eval_seeds = list(range(5000, 5000 + args.eval_seeds))
     t0 = time.perf_counter()
+    tv_min = learned.TV_GATE if args.tv_min is None else args.tv_min
+    diss_frac = learned.DISS_FRAC if args.diss_frac is None else args.diss_frac
     X, Y = learned.generate(train_seeds, coarse=args.coarse, t_end=args.t_end,
-                            snapshots=args.snapshots, frac=args.frac, log=log)
+                            snapshots=args.snapshots, frac=args.frac, tv_min=tv_min,
+                            noise=args.noise, log=log)
     t_data = time.perf_counter() - t0
+    hold = np.random.default_rng(7).random(len(X)) < 0.1
+    Xv, Yv, X, Y = X[hold], Y[hold], X[~hold], Y[~hold]
     blob = learned.init_model(X, Y, seed=0)
     tr = learned.Trainer(blob, X, Y, device=local_rank)
     losses = [tr.train(1, batch=args.batch, lr=args.lr)]
@@ -467,23 +472,30 @@ def main_learned(args, rank, world, local_rank):
     t_train = time.perf_counter() - t1
     model = tr.model()
     tr.close()
+    fit = {"r2_train": learned.r2(model, X, Y), "r2_held_out": learned.r2(model, Xv, Yv)}
+    if log:
+        log(f"fit: {fit}")
     if args.model_out:
         os.makedirs(os.path.dirname(os.path.abspath(args.model_out)), exist_ok=True)
         np.save(args.model_out, model)
     ev = learned.evaluate(model, eval_seeds, coarse=args.coarse, t_end=args.t_end,
-                          times=(0.5 * args.t_end, args.t_end), log=log)
+                          times=(0.25 * args.t_end, 0.5 * args.t_end, args.t_end),
+                          tv_min=tv_min, diss_frac=diss_frac, log=log)
     sm = ev["summary"]
     c, c2 = "plain_%d" % args.coarse, "plain_%d" % (2 * args.coarse)
     lr_ = "learned_%d" % args.coarse
     if rank == 0:
         print(json.dumps({
             "metric": "L1 density error vs 4x fine plain FP64 run, at equal resolution",
-            "workload": f"KH (ensemble parameter ranges), coarse {args.coarse}^2, t = "
+            "workload": f"KH (ensemble parameter ranges, tanh shear layers of thickness "
+                        f"{learned.KH_SMOOTH}), coarse {args.coarse}^2, t = {0.25 * args.t_end}, "
                         f"{0.5 * args.t_end} and {args.t_end}; {len(train_seeds)} training "
                         f"seeds (fine {4 * args.coarse}^2 restricted), {len(eval_seeds)} held-out",
             "train": {"samples": int(len(X)), "steps": args.train_steps, "batch": args.batch,
                       "lr": args.lr, "loss_first": losses[0], "loss_last": losses[-1],
-                      "data_seconds": t_data, "train_seconds": t_train},
+                      "data_seconds": t_data, "train_seconds": t_train, "noise": args.noise,
+                      **fit},
+            "gate": {"tv_min": tv_min, "diss_frac": diss_frac, "shock_jump": 0.5, "pos_frac": 0.02},
             "summary": sm,
             "time_ratio_learned_over_plain2x": sm[lr_]["mean_seconds"] / sm[c2]["mean_seconds"],
             "l1_ratio_learned_over_plain": [a / b for a, b in zip(sm[lr_]["mean_l1_at_%d" % args.coarse],
@@ -515,6 +527,9 @@ def main():
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--model-out", default="")
+    ap.add_argument("--noise", type=float, default=0.03, help="training-state block noise")
+    ap.add_argument("--tv-min", type=float, default=None, help="smoothness gate (default: library's)")
+    ap.add_argument("--diss-frac", type=float, default=None, help="dissipation clip (default: library's)")
     ap.add_argument("--ens-n", type=int, default=64)
     ap.add_argument("--ens-tmax", type=float, default=1.0)
     ap.add_argument("--ncu-case", action="store_true",

@@ -115,7 +115,7 @@ struct gk_handle {
     int upload_step = 0;  // clock step at the last upload
     bool tiling_set = false;  // gk_set_tiling overrides the default tiling
     float* model = nullptr;   // learned flux correction (device), or null
-    float shock_jump = 0.5f, pos_frac = 0.1f;
+    gk::FluxGate gate;
     unsigned* fired = nullptr;  // faces where the detector kept plain HLLC
     int tiling_rows = 0;
     cudaGraphExec_t gexec = nullptr;
@@ -338,9 +338,9 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
         if (h->model) {
             // learned correction of the face fluxes (gk_mlp.cu)
             GK_L(gk::K_FLUX, gk::launch_flux_correct(h->model, h->W, h->F1, c.g, c.ph, c.tm, 0,
-                                                     h->shock_jump, h->pos_frac, h->fired, s));
+                                                     h->gate, h->fired, s));
             GK_L(gk::K_FLUX, gk::launch_flux_correct(h->model, h->W, h->F2, c.g, c.ph, c.tm, 1,
-                                                     h->shock_jump, h->pos_frac, h->fired, s));
+                                                     h->gate, h->fired, s));
         }
     };
     GK_L(gk::K_BC, k.bc(c, A, s));
@@ -1115,6 +1115,12 @@ extern "C" int gk_face_fluxes(gk_handle* h, double* fx, double* fy) {
     k.c2p(h->ctx, h->A, h->W, h->stream);
     k.flux(h->ctx, 0, h->W, h->F1, h->stream);
     k.flux(h->ctx, 1, h->W, h->F2, h->stream);
+    if (h->model) {  // dt is 0 here, so only the shock detector can veto a face
+        gk::launch_flux_correct(h->model, h->W, h->F1, h->ctx.g, h->ctx.ph, h->ctx.tm, 0, h->gate,
+                                nullptr, h->stream);
+        gk::launch_flux_correct(h->model, h->W, h->F2, h->ctx.g, h->ctx.ph, h->ctx.tm, 1, h->gate,
+                                nullptr, h->stream);
+    }
     GK_CUDA(h, cudaGetLastError());
     if (fx && (rc = copy_faces(h, h->F1, 0, fx)) != GK_OK) return rc;
     if (fy && (rc = copy_faces(h, h->F2, 1, fy)) != GK_OK) return rc;
@@ -1153,6 +1159,10 @@ extern "C" int gk_tap_substeps(gk_handle* h, int nsub, double dt_sub, int ratio,
             k.c2p(c, u, h->W, s);
             k.flux(c, 0, h->W, h->F1, s);
             k.flux(c, 1, h->W, h->F2, s);
+            if (h->model) {  // an installed correction is part of the tapped flux
+                gk::launch_flux_correct(h->model, h->W, h->F1, c.g, c.ph, c.tm, 0, h->gate, h->fired, s);
+                gk::launch_flux_correct(h->model, h->W, h->F2, c.g, c.ph, c.tm, 1, h->gate, h->fired, s);
+            }
             k_restrict_faces<<<grid, 128, 0, s>>>(h->F1, acc, g, ratio, nxc, nyc, 0, w);
             k_restrict_faces<<<grid, 128, 0, s>>>(h->F2, acc + nacc, g, ratio, nxc, nyc, 1, w);
             if (stage == 0)
@@ -1174,7 +1184,8 @@ extern "C" int gk_tap_substeps(gk_handle* h, int nsub, double dt_sub, int ratio,
 
 // ------------------------------------------------------------ learned correction on a handle
 extern "C" int gk_set_flux_model(gk_handle* h, const float* model_host, int nmodel,
-                                 float shock_jump, float pos_frac) {
+                                 float shock_jump, float pos_frac, float tv_min,
+                                 float diss_frac) {
     if (!h) return GK_ERR_INVALID;
     GK_CUDA(h, cudaSetDevice(h->device));
     if (!model_host) {
@@ -1189,8 +1200,10 @@ extern "C" int gk_set_flux_model(gk_handle* h, const float* model_host, int nmod
             GK_CUDA(h, cudaMemset(h->fired, 0, sizeof(unsigned)));
         }
         GK_CUDA(h, cudaMemcpy(h->model, model_host, sizeof(float) * nmodel, cudaMemcpyHostToDevice));
-        h->shock_jump = shock_jump;
-        h->pos_frac = pos_frac;
+        h->gate.shock_jump = shock_jump;
+        h->gate.pos_frac = pos_frac;
+        h->gate.tv_min = tv_min;
+        h->gate.diss_frac = diss_frac;
         int rc = alloc_generic(h);
         if (rc != GK_OK) return rc;
     }

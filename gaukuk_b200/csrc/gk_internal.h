@@ -94,11 +94,28 @@ struct alignas(64) EnsInst {
 // 4) doubles, box (nt, 1, 4), no swizzle, zero fill out of bounds (gk_api.cu).
 bool encode_rows_map(CUtensorMap* map, const double* base, const Geom& g, int nt);
 
+// Where and how far the learned flux correction applies.  A face keeps its
+// plain HLLC flux when max(p)/min(p) over its stencil exceeds 1 + shock_jump,
+// or when the correction would move more than pos_frac of an adjacent cell's
+// mass or internal energy through it in one step (both counted as detector
+// firings), or when the total variation of its stencil's features is below
+// tv_min (smooth flow, where the plain method is accurate; not counted).
+// Each component of a correction is clipped to diss_frac times the face's
+// HLL dissipation (1/2) max(|vn| + c) |U_R - U_L| of the PLM face states, so
+// the corrected flux keeps part of the scheme's own dissipation
+// (diss_frac < 0: no clip).
+struct FluxGate {
+    float shock_jump = 0.5f;
+    float pos_frac = 0.02f;
+    float tv_min = 0.0f;
+    float diss_frac = -1.0f;
+};
+
 // The learned flux correction of one direction of a generic-path stage
 // (gk_mlp.cu).
 void launch_flux_correct(const float* model, const double* W, double* F, const Geom& g,
-                         const Phys& ph, const DevTime* tm, int dir, float shock_jump,
-                         float pos_frac, unsigned* fired, cudaStream_t s);
+                         const Phys& ph, const DevTime* tm, int dir, const FluxGate& gate,
+                         unsigned* fired, cudaStream_t s);
 
 // Kernel classes, for per-kernel profiling.
 enum KClass { K_BC = 0, K_C2P, K_FLUX, K_UPDATE, K_KICK, K_CFL, K_STAGE, K_BEGIN, K_NCLASS };

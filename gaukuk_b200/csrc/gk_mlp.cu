@@ -408,26 +408,64 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ p
 }
 
 // ------------------------------------------------------------ inference
+// van Leer slope of the PLM reconstruction, (2ab)/(a+b) for ab > 0 else 0.
+__device__ __forceinline__ double vl_slope(double a, double b) {
+    const double m = a * b;
+    return m <= 0.0 ? 0.0 : (2.0 * m) / (a + b);
+}
+
+// PLM face states of the stencil (cells -2, -1 | 0, +1) as conserved
+// variables (mass, normal momentum, tangential momentum, energy) and the fast
+// signal speeds |vn| + c on each side.
+__device__ __forceinline__ void face_states(const double (&r)[4], const double (&vn)[4],
+                                            const double (&vt)[4], const double (&p)[4], double gamma,
+                                            double gm1Rec, double (&ul)[4], double (&ur)[4],
+                                            double& sl, double& sr) {
+    const double* q[4] = {r, vn, vt, p};
+    double wl[4], wr[4];
+    for (int v = 0; v < 4; ++v) {
+        wl[v] = q[v][1] + 0.5 * vl_slope(q[v][1] - q[v][0], q[v][2] - q[v][1]);
+        wr[v] = q[v][2] - 0.5 * vl_slope(q[v][2] - q[v][1], q[v][3] - q[v][2]);
+    }
+    const double* w[2] = {wl, wr};
+    double* u[2] = {ul, ur};
+    double s[2];
+    for (int side = 0; side < 2; ++side) {
+        const double d = fmax(w[side][0], 1e-300), a = w[side][1], b = w[side][2];
+        const double pp = fmax(w[side][3], 0.0);
+        u[side][0] = d;
+        u[side][1] = d * a;
+        u[side][2] = d * b;
+        u[side][3] = pp * gm1Rec + 0.5 * d * (a * a + b * b);
+        s[side] = fabs(a) + sqrt(gamma * pp / d);
+    }
+    sl = s[0];
+    sr = s[1];
+}
+
 // Adds the learned correction to the face fluxes of one direction of a 2D
 // generic-path stage (F: FP64 face fluxes, W: FP64 primitives).  One warp
-// per 16 faces.  The plain HLLC flux is kept where the detector fires:
-// a pressure jump max(p)/min(p) > 1 + shock_jump over the stencil, or a
+// per 16 faces.  The plain HLLC flux is kept where the detector fires (a
+// pressure jump max(p)/min(p) > 1 + shock_jump over the stencil, or a
 // correction that would move more than pos_frac of an adjacent cell's mass
-// or internal energy through the face in one step.
+// or internal energy through the face in one step) and in smooth flow (the
+// stencil's total variation below tv_min); each component is clipped to
+// diss_frac times the face's HLL dissipation (gk::FluxGate).
 struct InferShared {
     MlpWeights w;
     TileAct act[4];
     float norm[2 * NI + 2 * NO];
-    // per face: rho_ref*c, rho_ref*c^2, rho_ref*c^3, no-shock flag, the smaller
-    // density and internal energy of the two cells next to the face
-    float scale[4][16][6];
+    // per face: rho_ref*c, rho_ref*c^2, rho_ref*c^3, gate (0 shock, 1 correct,
+    // 2 smooth), the smaller density and internal energy of the two cells
+    // next to the face, the clip bounds of the 4 outputs (negative: none)
+    float scale[4][16][10];
 };
 
 __global__ void __launch_bounds__(128) k_flux_correct(const float* __restrict__ model,
                                                       const double* __restrict__ W,
                                                       double* __restrict__ F, gk::Geom g,
                                                       gk::Phys ph, const gk::DevTime* __restrict__ tm,
-                                                      int dir, float shock_jump, float pos_frac,
+                                                      int dir, gk::FluxGate gate,
                                                       unsigned* __restrict__ fired) {
     if (!tm->active) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -449,7 +487,7 @@ __global__ void __launch_bounds__(128) k_flux_correct(const float* __restrict__ 
         if (lane < 16) {
             const long long f = tile * 16 + lane;
             float feat[NI];
-            float sc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            float sc[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             if (f < nfaces) {
                 const int fi = (int)(f % nfx), fj = (int)(f / nfx);
                 const int i = g.ib + fi, j = g.jb + fj;  // face between cells (i-1|i) or (j-1|j)
@@ -471,21 +509,32 @@ __global__ void __launch_bounds__(128) k_flux_correct(const float* __restrict__ 
                     feat[4 * c + 2] = (float)(vt[c] / cr);
                     feat[4 * c + 3] = (float)(p[c] / pr - 1.0);
                 }
+                float tv = 0.f;  // total variation of the stencil's features
+                for (int e = 4; e < NI; ++e) tv += fabsf(feat[e] - feat[e - 4]);
                 double pmax = p[0], pmin = p[0];
                 for (int c = 1; c < 4; ++c) { pmax = fmax(pmax, p[c]); pmin = fmin(pmin, p[c]); }
-                const bool shock = pmax > (1.0 + shock_jump) * pmin;
+                const bool shock = pmax > (1.0 + gate.shock_jump) * pmin;
                 sc[0] = (float)(rr * cr);
                 sc[1] = (float)(rr * cr * cr);
                 sc[2] = (float)(rr * cr * cr * cr);
-                sc[3] = shock ? 0.f : 1.f;
+                sc[3] = shock ? 0.f : (tv >= gate.tv_min ? 1.f : 2.f);
                 sc[4] = (float)fmin(r[1], r[2]);
                 sc[5] = (float)(fmin(p[1], p[2]) * ph.gm1Rec);
+                if (gate.diss_frac >= 0.f) {
+                    // (1/2) max(s) |U_R - U_L| of the van Leer PLM face states
+                    double ul[4], ur[4], sl, sr;
+                    face_states(r, vn, vt, p, ph.gamma, ph.gm1Rec, ul, ur, sl, sr);
+                    const double sm = 0.5 * fmax(sl, sr) * gate.diss_frac;
+                    for (int o = 0; o < 4; ++o) sc[6 + o] = (float)(sm * fabs(ur[o] - ul[o]));
+                } else {
+                    for (int o = 0; o < 4; ++o) sc[6 + o] = -1.f;
+                }
             } else {
                 for (int e = 0; e < NI; ++e) feat[e] = 0.f;
             }
             for (int e = 0; e < NI; ++e)
                 act.x[lane * NI + e] = __float2bfloat16_rn((feat[e] - sh.norm[e]) / sh.norm[NI + e]);
-            for (int e = 0; e < 6; ++e) sh.scale[warp][lane][e] = sc[e];
+            for (int e = 0; e < 10; ++e) sh.scale[warp][lane][e] = sc[e];
         }
         __syncwarp();
         float z1[8][4], z2[8][4], y[4];
@@ -495,27 +544,30 @@ __global__ void __launch_bounds__(128) k_flux_correct(const float* __restrict__ 
         for (int half = 0; half < 2; ++half) {
             const int fl = gq + 8 * half;
             const long long f = tile * 16 + fl;
-            const bool mine = tq < 2 && f < nfaces;
             const float* sc = sh.scale[warp][fl];
+            const bool mine = tq < 2 && f < nfaces && sc[3] != 2.f;
             double corr[2] = {0.0, 0.0};
             int bad = 0;
             if (mine) {
                 for (int o2 = 0; o2 < 2; ++o2) {
                     const int o = 2 * tq + o2;
-                    const float ys = y[2 * half + o2] * sh.norm[2 * NI + NO + o] + sh.norm[2 * NI + o];
+                    // clip to the training range (+-4 deviations) before de-standardising
+                    const float yc = fminf(fmaxf(y[2 * half + o2], -4.f), 4.f);
+                    const float ys = yc * sh.norm[2 * NI + NO + o] + sh.norm[2 * NI + o];
                     corr[o2] = (double)ys * (double)(o == 0 ? sc[0] : (o == 3 ? sc[2] : sc[1]));
+                    const double bound = sc[6 + o];
+                    if (bound >= 0.0) corr[o2] = fmin(fmax(corr[o2], -bound), bound);
                 }
                 // positivity: mass (output 0) and energy (output 3) moved in one step
-                if (tq == 0) bad = fabs(corr[0]) * dtdx > pos_frac * sc[4];
-                else bad = fabs(corr[1]) * dtdx > pos_frac * sc[5];
+                if (tq == 0) bad = fabs(corr[0]) * dtdx > gate.pos_frac * sc[4];
+                else bad = fabs(corr[1]) * dtdx > gate.pos_frac * sc[5];
                 bad |= sc[3] == 0.f;
             }
             bad |= __shfl_xor_sync(0xffffffffu, bad, 1);
-            if (!mine) continue;
-            if (bad) {
-                if (tq == 0 && fired) atomicAdd(fired, 1u);
-                continue;
-            }
+            // one atomic per warp and half-tile for the faces left to plain HLLC
+            const unsigned nbad = __ballot_sync(0xffffffffu, mine && bad && tq == 0);
+            if (lane == 0 && fired && nbad) atomicAdd(fired, (unsigned)__popc(nbad));
+            if (!mine || bad) continue;
             const int fi = (int)(f % nfx), fj = (int)(f / nfx);
             const long long fc = (long long)(g.kb - g.kofs) * g.fkstride + (long long)(g.jb + fj) * g.fpitch + g.ib + fi;
             for (int o2 = 0; o2 < 2; ++o2) {
@@ -668,8 +720,8 @@ int gk_mlp_forward(gk_mlp* M, const void* X, long long n, float* Y) {
 namespace gk {
 size_t flux_correct_smem() { return sizeof(InferShared); }
 void launch_flux_correct(const float* model, const double* W, double* F, const Geom& g,
-                         const Phys& ph, const DevTime* tm, int dir, float shock_jump,
-                         float pos_frac, unsigned* fired, cudaStream_t s) {
+                         const Phys& ph, const DevTime* tm, int dir, const FluxGate& gate,
+                         unsigned* fired, cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_flux_correct, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -679,7 +731,7 @@ void launch_flux_correct(const float* model, const double* W, double* F, const G
     const long long nf = dir == 0 ? (long long)(g.nx + 1) * g.ny : (long long)g.nx * (g.ny + 1);
     const long long tiles = (nf + 15) / 16;
     const int ctas = (int)((tiles + 3) / 4 < 148 * 8 ? (tiles + 3) / 4 : 148 * 8);
-    k_flux_correct<<<ctas, 128, sizeof(InferShared), s>>>(model, W, F, g, ph, tm, dir, shock_jump,
-                                                           pos_frac, fired);
+    k_flux_correct<<<ctas, 128, sizeof(InferShared), s>>>(model, W, F, g, ph, tm, dir, gate,
+                                                           fired);
 }
 }  // namespace gk

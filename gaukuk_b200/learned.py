@@ -17,6 +17,12 @@ Features per face (``face_features``): the 4 cells across the face, each as
 stencil means, c_ref = sqrt(gamma p_ref / rho_ref); targets are scaled by
 rho_ref*c_ref (mass), rho_ref*c_ref^2 (momenta), rho_ref*c_ref^3 (energy).
 The kernel k_flux_correct forms the same quantities on the device.
+
+Where the correction applies (``install``): not where the detector fires,
+not on faces whose stencil total variation G (``stencil_variation``) is below
+tv_min, and each component at most diss_frac times the face's HLL
+dissipation (``hll_dissipation``), so the corrected flux keeps part of the
+scheme's own dissipation.
 """
 from __future__ import annotations
 
@@ -33,6 +39,8 @@ from .config import Params
 NI, NH, NO = 16, 64, 4
 NPARAM = NH * NI + NH + NH * NH + NH + NO * NH + NO
 NMODEL = NPARAM + 2 * NI + 2 * NO
+TV_GATE = 0.0     # default tv_min: faces with smoother stencils keep plain HLLC
+DISS_FRAC = 0.25  # default diss_frac: corrections within this part of the HLL dissipation
 
 
 # ------------------------------------------------------------------ grid helpers
@@ -84,6 +92,40 @@ def face_features(p: Params, a: np.ndarray, direction: int):
     return X, S
 
 
+def stencil_variation(X: np.ndarray) -> np.ndarray:
+    """Total variation G of each face's stencil: the sum over the 3 pairs of
+    neighbouring cells and the 4 features of |difference|."""
+    X = np.asarray(X, dtype=np.float64)
+    return np.abs(X[:, 4:] - X[:, :-4]).sum(axis=1)
+
+
+def hll_dissipation(p: Params, a: np.ndarray, direction: int) -> np.ndarray:
+    """(1/2) max(|vn| + c) |U_R - U_L| per face (n, 4: mass, normal momentum,
+    tangential momentum, energy), U_L, U_R the van Leer PLM face states of
+    the stencil; k_flux_correct clips the correction to diss_frac times it."""
+    rho, vx, vy, pre = primitives(p, a)
+    ax = 1 if direction == 0 else 0
+    vn, vt = (vx, vy) if direction == 0 else (vy, vx)
+
+    def slope(x, y):
+        m = x * y
+        return np.where(m > 0, 2.0 * m / np.where(m > 0, x + y, 1.0), 0.0)
+
+    wl, wr = [], []
+    for q in (rho, vn, vt, pre):
+        c = [np.roll(q, s, axis=ax).ravel() for s in (2, 1, 0, -1)]
+        wl.append(c[1] + 0.5 * slope(c[1] - c[0], c[2] - c[1]))
+        wr.append(c[2] - 0.5 * slope(c[2] - c[1], c[3] - c[2]))
+
+    def cons(w):
+        d, u, v, pp = np.maximum(w[0], 1e-300), w[1], w[2], np.maximum(w[3], 0.0)
+        return (np.stack([d, d * u, d * v, pp / (p.gamma - 1.0) + 0.5 * d * (u * u + v * v)], axis=1),
+                np.abs(u) + np.sqrt(p.gamma * pp / d))
+
+    (ul, sl), (ur, sr) = cons(wl), cons(wr)
+    return 0.5 * np.maximum(sl, sr)[:, None] * np.abs(ur - ul)
+
+
 def rotate_to_face(delta: np.ndarray, direction: int) -> np.ndarray:
     """(DEN, MTX, MTY, ENG) planes -> (mass, normal, tangential, energy) columns."""
     d, mx, my, e = delta
@@ -119,29 +161,86 @@ def tap(sim, nsub: int, dt_sub: float, ratio: int) -> Tuple[np.ndarray, np.ndarr
 
 
 # ------------------------------------------------------------------ data
-def kh_instance(seed: int, n: int, tmax: float) -> Tuple[Params, np.ndarray, Dict]:
-    """One KH problem with the ensemble's parameter ranges, at resolution n."""
+# Shear-layer thickness of the KH instances.  With sharp layers the
+# pointwise solution does not converge under refinement (secondary
+# instabilities seeded at the grid scale: plain 256^2 is no closer to a
+# 1024^2 run than plain 128^2), so an L1 error against a finer run would not
+# measure accuracy; tanh layers of thickness 0.01 converge at second order up
+# to t = 1 between 128^2 and 1024^2.
+KH_SMOOTH = 0.01
+
+
+def kh_instance(seed: int, n: int, tmax: float,
+                smooth: float = KH_SMOOTH) -> Tuple[Params, np.ndarray, Dict]:
+    """One KH problem with the ensemble's parameter ranges (density ratio,
+    half-width, perturbation amplitude), no cell noise, tanh shear layers of
+    thickness `smooth`, at resolution n."""
     rng = np.random.default_rng(seed)
     draw = {"ratio": float(rng.uniform(1.5, 4.0)), "half_width": float(rng.uniform(0.2, 0.3)),
             "amp": float(rng.uniform(0.005, 0.02))}
     p, c = problems.kh(n, seed=seed, rho_in=draw["ratio"], rho_out=1.0,
-                       half_width=draw["half_width"], amp=draw["amp"], tmax=tmax)
+                       half_width=draw["half_width"], amp=draw["amp"], noise=0.0,
+                       smooth=smooth, tmax=tmax)
     return p, c, draw
+
+
+def perturb(p: Params, cons: np.ndarray, ratio: int, sigma: float, rng) -> np.ndarray:
+    """A 2D state with noise that is constant over each ratio x ratio block:
+    rho (1 + sigma u1), vx + sigma c u2, vy + sigma c u3, p (1 + sigma u4),
+    u uniform in [-1, 1] per block, c the local sound speed."""
+    rho, vx, vy, pre = primitives(p, active2d(p, cons))
+    nyc, nxc = p.ny // ratio, p.nx // ratio
+
+    def field():
+        return np.repeat(np.repeat(rng.uniform(-1.0, 1.0, (nyc, nxc)), ratio, axis=0), ratio, axis=1)
+
+    c = np.sqrt(p.gamma * pre / rho)
+    rho2, vx2 = rho * (1.0 + sigma * field()), vx + sigma * c * field()
+    vy2, pre2 = vy + sigma * c * field(), pre * (1.0 + sigma * field())
+    return problems.prim_to_cons(p, rho2[None], vx2[None], vy2[None], np.zeros((1,) + rho.shape),
+                                 pre2[None])
 
 
 def generate(seeds: Sequence[int], coarse: int = 256, ratio: int = 4, t_end: float = 2.0,
              snapshots: int = 16, frac: float = 0.25, mode: str = "fast",
-             sample_seed: int = 0, log=print) -> Tuple[np.ndarray, np.ndarray]:
+             sample_seed: int = 0, tv_min: float = TV_GATE, noise: float = 0.0,
+             noisy: int = 1, first: float = 1.0, log=print) -> Tuple[np.ndarray, np.ndarray]:
     """Training pairs from fine runs (coarse*ratio)^2 restricted to coarse^2.
 
-    At `snapshots` times spread over (0, t_end] the fine state is restricted,
-    the coarse HLLC fluxes of the restricted state are computed, and the fine
-    run is advanced by one coarse CFL step in `ratio` fixed sub-steps while
-    the fluxes through the coarse faces are accumulated; the target is their
-    difference.  A fraction `frac` of the faces of each snapshot is kept."""
+    At `snapshots` times t_end (s + first) / (snapshots + first), s = 0 ..
+    snapshots - 1, the fine state is restricted; one coarse RK2 step of the
+    restricted state is taken with the coarse solver, recording its
+    stage-averaged face fluxes (1/2)(F(U) + F(U*)), and the fine run is
+    advanced over the same interval in `ratio` fixed sub-steps while the
+    fluxes through the coarse faces are accumulated.  The target is their
+    difference: added to both coarse stages it makes the coarse step
+    reproduce the restricted fine step.  A fraction `frac` of the faces whose
+    stencil variation is at least `tv_min` (the faces the correction is
+    applied to) is kept.
+
+    With noise > 0 each snapshot also yields `noisy` sets of pairs from the
+    fine state perturbed by ``perturb`` (block noise of relative amplitude
+    `noise` on the coarse cells): the fine solver's response to grid-scale
+    perturbations, which restricted states alone never show and which a
+    correction must damp for a coarse run to stay stable."""
     from .sim import Sim
     rng = np.random.default_rng(sample_seed)
     Xs, Ys = [], []
+
+    def pairs(pc, cc, fine, crs, dt_c):
+        fx_c, fy_c = tap(crs, 1, dt_c, 1)
+        fx_f, fy_f = tap(fine, ratio, dt_c / ratio, ratio)
+        a = active2d(pc, cc)
+        for direction, Ff, Fc in ((0, fx_f, fx_c), (1, fy_f, fy_c)):
+            X, S = face_features(pc, a, direction)
+            G = stencil_variation(X)
+            D = rotate_to_face(Ff - Fc, direction)
+            Y = np.stack([D[:, 0] / S[:, 0], D[:, 1] / S[:, 1], D[:, 2] / S[:, 1],
+                          D[:, 3] / S[:, 2]], axis=1)
+            keep = (rng.random(len(X)) < frac) & (G >= tv_min)
+            Xs.append(X[keep].astype(np.float32))
+            Ys.append(Y[keep].astype(np.float32))
+
     for k, seed in enumerate(seeds):
         t0 = time.time()
         pf, cf, _ = kh_instance(seed, coarse * ratio, t_end)
@@ -149,26 +248,28 @@ def generate(seeds: Sequence[int], coarse: int = 256, ratio: int = 4, t_end: flo
         pc, cc = restrict(pf, cf, ratio)
         crs = Sim(pc, cc, mode=mode)
         drmin_c = min((pc.xmax - pc.xmin) / pc.nx, (pc.ymax - pc.ymin) / pc.ny)
-        for s in range(1, snapshots + 1):
-            ts = t_end * s / (snapshots + 1)
+        for s in range(snapshots):
+            ts = t_end * (s + first) / (snapshots + first)
             t = fine.get_time()
             if ts > t + 1e-12:
                 fine.advance(ts - t)
-            _, cc = restrict(pf, fine.download(), ratio)
+            f0 = fine.download()
+            if noise > 0:
+                t_f, step_f = fine.get_time(), fine.get_step()
+                for _ in range(noisy):
+                    fn = perturb(pf, f0, ratio, noise, rng)
+                    fine.upload(fn)
+                    fine.set_time(t_f, step_f)
+                    _, cc = restrict(pf, fn, ratio)
+                    crs.set_time(0.0, 0)
+                    crs.upload(cc)
+                    pairs(pc, cc, fine, crs, pc.cfl * drmin_c / crs.cmax())
+                fine.upload(f0)
+                fine.set_time(t_f, step_f)
+            _, cc = restrict(pf, f0, ratio)
             crs.set_time(0.0, 0)
             crs.upload(cc)
-            fx_c, fy_c = face_fluxes(crs)
-            dt_c = pc.cfl * drmin_c / crs.cmax()
-            fx_f, fy_f = tap(fine, ratio, dt_c / ratio, ratio)
-            a = active2d(pc, cc)
-            for direction, Ff, Fc in ((0, fx_f, fx_c[:, :, :pc.nx]), (1, fy_f, fy_c[:, :pc.ny, :])):
-                X, S = face_features(pc, a, direction)
-                D = rotate_to_face(Ff - Fc, direction)
-                Y = np.stack([D[:, 0] / S[:, 0], D[:, 1] / S[:, 1], D[:, 2] / S[:, 1],
-                              D[:, 3] / S[:, 2]], axis=1)
-                keep = rng.random(len(X)) < frac
-                Xs.append(X[keep].astype(np.float32))
-                Ys.append(Y[keep].astype(np.float32))
+            pairs(pc, cc, fine, crs, pc.cfl * drmin_c / crs.cmax())
         fine.close()
         crs.close()
         if log:
@@ -249,14 +350,30 @@ class Trainer:
         return b
 
 
-def install(sim, blob: Optional[np.ndarray], shock_jump: float = 0.5, pos_frac: float = 0.1):
+def r2(blob: np.ndarray, X: np.ndarray, Y: np.ndarray, device: int = 0) -> List[float]:
+    """Coefficient of determination of each output of the model on (X, Y),
+    in standardised units, with the device forward (gk_mlp_forward)."""
+    t = Trainer(blob, X, Y, device=device)
+    try:
+        pred = t.forward()
+    finally:
+        t.close()
+    _, Yn = standardise(np.asarray(blob, dtype=np.float32), X, Y)
+    res = ((pred - Yn) ** 2).sum(0)
+    tot = ((Yn - Yn.mean(0)) ** 2).sum(0) + 1e-30
+    return (1.0 - res / tot).tolist()
+
+
+def install(sim, blob: Optional[np.ndarray], shock_jump: float = 0.5, pos_frac: float = 0.02,
+            tv_min: float = TV_GATE, diss_frac: float = DISS_FRAC):
     """Installs (or, with None, removes) the correction on a 2D Sim."""
     if blob is None:
-        _lib.check(sim._L.gk_set_flux_model(sim.h, None, 0, 0.0, 0.0), sim.h)
+        _lib.check(sim._L.gk_set_flux_model(sim.h, None, 0, 0.0, 0.0, 0.0, 0.0), sim.h)
         return
     b = np.ascontiguousarray(blob, dtype=np.float32)
     _lib.check(sim._L.gk_set_flux_model(sim.h, b.ctypes.data_as(ctypes.c_void_p), b.size,
-                                        float(shock_jump), float(pos_frac)), sim.h)
+                                        float(shock_jump), float(pos_frac), float(tv_min),
+                                        float(diss_frac)), sim.h)
 
 
 def detector_count(sim) -> int:
@@ -288,7 +405,8 @@ def _restrict_rho(rho: np.ndarray, r: int) -> np.ndarray:
 
 def evaluate(blob: np.ndarray, seeds: Sequence[int], coarse: int = 256, t_end: float = 2.0,
              times: Sequence[float] = (0.5, 1.0, 2.0), mode: str = "fast",
-             shock_jump: float = 0.5, pos_frac: float = 0.1, log=print) -> Dict:
+             shock_jump: float = 0.5, pos_frac: float = 0.02, tv_min: float = TV_GATE,
+             diss_frac: float = DISS_FRAC, log=print) -> Dict:
     """L1 density error against the 4x fine plain run (the judge) for plain
     coarse, plain 2x coarse and learned coarse, each started from the
     restriction of the same fine initial state, and their GPU times."""
@@ -304,7 +422,7 @@ def evaluate(blob: np.ndarray, seeds: Sequence[int], coarse: int = 256, t_end: f
             pc, cc = restrict(pf, cf, ratio)
             s = Sim(pc, cc, mode=mode)
             if learned:
-                install(s, blob, shock_jump, pos_frac)
+                install(s, blob, shock_jump, pos_frac, tv_min, diss_frac)
             s.run_steps(1)  # build the graph outside the timing
             s.set_time(0.0, 0)
             s.upload(cc)
@@ -312,6 +430,7 @@ def evaluate(blob: np.ndarray, seeds: Sequence[int], coarse: int = 256, t_end: f
             m0 = active2d(pc, cc)[0].sum()
             res[name] = {
                 "seconds": secs,
+                "steps": s.get_step(),
                 "l1": [float(np.mean(np.abs(r - _restrict_rho(j, ratio)))) for r, j in zip(rho, judge)],
                 "l1_at_%d" % coarse: [float(np.mean(np.abs(_restrict_rho(r, 4 // ratio) - _restrict_rho(j, 4))))
                                       for r, j in zip(rho, judge)],

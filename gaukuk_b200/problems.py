@@ -91,18 +91,27 @@ def sod(n: int = 256, x0: float = 0.5, integrator: int = 2, cfl: float = 0.4,
 
 def kh(n: int = 256, ny: int = None, seed: int = 0, rho_in: float = 2.0, rho_out: float = 1.0,
        half_width: float = 0.25, amp: float = 0.01, noise: float = 1e-3, pressure: float = 2.5,
-       integrator: int = 2, cfl: float = 0.4, tmax: float = 2.0, rc_order: int = 2, **kw):
+       integrator: int = 2, cfl: float = 0.4, tmax: float = 2.0, rc_order: int = 2,
+       smooth: float = 0.0, **kw):
     """2D Kelvin-Helmholtz on [0,1]^2, periodic: rho_in and vx=-0.5 where
     |y-0.5| < half_width, else rho_out and vx=+0.5; p uniform;
-    vy = amp*sin(4*pi*x) + noise*U(-1,1) with U keyed on (seed, global cell id)."""
+    vy = amp*sin(4*pi*x) + noise*U(-1,1) with U keyed on (seed, global cell id).
+    With smooth > 0 the two shear layers are tanh profiles of that thickness,
+    s(y) = (tanh((y - y1)/smooth) - tanh((y - y2)/smooth))/2 with
+    y1,2 = 0.5 -+ half_width, rho = rho_out + (rho_in - rho_out) s, vx = 0.5 - s."""
     ny = n if ny is None else ny
     p = Params(nx=n, ny=ny, nz=1, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
                gamma=1.4, cfl=cfl, integrator=integrator, rc_order=rc_order,
                bc=(BC_PERIODIC,) * 6, tmax=tmax, dtoutput=tmax, **kw)
     x, y, _ = _active_grids(p)
-    inside = np.abs(y - 0.5) < half_width
-    rho = np.where(inside, rho_in, rho_out)
-    vx = np.where(inside, -0.5, 0.5)
+    if smooth > 0.0:
+        sh = 0.5 * (np.tanh((y - (0.5 - half_width)) / smooth) - np.tanh((y - (0.5 + half_width)) / smooth))
+        rho = rho_out + (rho_in - rho_out) * sh
+        vx = 0.5 - sh
+    else:
+        inside = np.abs(y - 0.5) < half_width
+        rho = np.where(inside, rho_in, rho_out)
+        vx = np.where(inside, -0.5, 0.5)
     ids = np.arange(p.nx * p.ny, dtype=np.uint64).reshape(1, p.ny, p.nx)
     vy = amp * np.sin(4.0 * PI * x) + noise * uniform_pm1(seed, ids)
     pre = np.full_like(rho, pressure)

@@ -217,20 +217,30 @@ int gk_mlp_forward(gk_mlp* m, const void* X, long long n, float* Y);
  * every stage then adds the network's correction to each face flux, except
  * where the detector fires -- a pressure ratio above 1 + shock_jump over the
  * stencil, or a correction moving more than pos_frac of an adjacent cell's
- * mass or internal energy in one step -- which keeps plain HLLC there. */
+ * mass or internal energy in one step -- which keeps plain HLLC there, and
+ * except in smooth flow: faces whose stencil total variation (the sum of
+ * |differences| of neighbouring cells' normalised features) is below tv_min
+ * keep plain HLLC too, without counting as a detector firing.  Each
+ * component of a correction is clipped to diss_frac times the face's HLL
+ * dissipation (1/2) max(|vn| + c) |U_R - U_L| of its PLM face states, so the
+ * corrected flux keeps part of the scheme's dissipation; diss_frac < 0
+ * disables the clip. */
 int gk_set_flux_model(gk_handle* h, const float* model_host, int nmodel, float shock_jump,
-                      float pos_frac);
+                      float pos_frac, float tv_min, float diss_frac);
 /* Faces where the detector has fired since the model was installed. */
 int gk_flux_model_fired(gk_handle* h, unsigned* fired);
 
 /* Training data: the HLLC face fluxes of the current state (2D; DEN, MTX,
- * MTY, ENG planes; x faces [4][ny][nx+1], y faces [4][ny+1][nx], host). */
+ * MTY, ENG planes; x faces [4][ny][nx+1], y faces [4][ny+1][nx], host).  An
+ * installed flux model corrects them (its shock detector, smoothness gate
+ * and dissipation clip apply; the positivity detector, which needs a step
+ * size, does not). */
 int gk_face_fluxes(gk_handle* h, double* fx, double* fy);
 /* Advances a 2D RK2 run by nsub steps of fixed dt_sub and returns the
  * fluxes through the faces of the grid coarsened by `ratio`, averaged over
  * the fine faces of each coarse face, the two RK stages and the steps:
  * fx_acc, fy_acc [4][ny/ratio][nx/ratio] (left / lower face of each coarse
- * cell), host. */
+ * cell), host.  An installed flux model corrects the tapped fluxes. */
 int gk_tap_substeps(gk_handle* h, int nsub, double dt_sub, int ratio, double* fx_acc,
                     double* fy_acc);
 

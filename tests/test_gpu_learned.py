@@ -83,6 +83,70 @@ def test_flux_tap_is_the_restricted_update():
     assert len(s.dt_log()) == 3 and abs(s.get_time() - (sum(s.dt_log()) + T)) < 1e-12
 
 
+def test_device_correction_matches_the_oracle():
+    """k_flux_correct's correction of each face flux equals the CPU oracle's
+    forward pass on the Python features, de-standardised, scaled by the flux
+    scales and clipped to diss_frac times the HLL dissipation; faces whose
+    stencil variation is below tv_min uncorrected."""
+    from gaukuk_b200.sim import Sim
+    p, c, _ = learned.kh_instance(11, 64, 1.0)
+    s = Sim(p, c, mode="fast")
+    s.run_steps(20)
+    a = learned.active2d(p, s.download())
+    fx0, fy0 = learned.face_fluxes(s)
+    n = learned.NPARAM
+    feats = {d: learned.face_features(p, a, d) for d in (0, 1)}
+    # a gate in the widest gap between the middle faces' variations, so both
+    # kinds of face occur and none lies near it (the device sums in FP32)
+    gs = np.sort(np.concatenate([learned.stencil_variation(feats[d][0]) for d in (0, 1)]))
+    lo, hi = len(gs) // 4, 3 * len(gs) // 4
+    k = lo + int(np.argmax(np.diff(gs[lo:hi])))
+    tv_min = float(0.5 * (gs[k] + gs[k + 1]))
+    assert gs[k + 1] - gs[k] > 1e-4 * tv_min
+    diss_frac = 0.5
+    X, Y = _data(256)
+    blob = learned.init_model(X, Y, seed=8)
+    blob[n + 32:n + 36] = 0.0
+
+    def raw(d):
+        Xf, S = feats[d]
+        _, _, yn = mlp_oracle.forward_backward(blob[:n], learned.standardise(blob, Xf),
+                                               np.zeros((len(Xf), 4)), rounding=True)
+        return np.clip(yn, -4, 4) * np.stack([S[:, 0], S[:, 1], S[:, 1], S[:, 2]], axis=1)
+
+    # output deviations that put about half of the gated corrections above the bound
+    ratio = np.concatenate([(diss_frac * learned.hll_dissipation(p, a, d) / np.maximum(np.abs(raw(d)), 1e-300))
+                            [learned.stencil_variation(feats[d][0]) >= tv_min] for d in (0, 1)])
+    blob[n + 36:n + 40] = np.median(ratio, axis=0)
+    learned.install(s, blob, shock_jump=10.0, pos_frac=1.0, tv_min=tv_min, diss_frac=diss_frac)
+    fx1, fy1 = learned.face_fluxes(s)
+    for d, dF in ((0, (fx1 - fx0)[:, :, :p.nx]), (1, (fy1 - fy0)[:, :p.ny, :])):
+        gated = learned.stencil_variation(feats[d][0]) >= tv_min
+        ref = raw(d) * blob[n + 36:n + 40] * gated[:, None]
+        bound = diss_frac * learned.hll_dissipation(p, a, d)
+        clipped = np.abs(ref) > bound
+        assert clipped[gated].any() and (~clipped[gated]).any()
+        ref = np.clip(ref, -bound, bound)
+        got = learned.rotate_to_face(dF, d)
+        assert np.all(got[~gated] == 0)
+        for o in range(4):
+            err = np.linalg.norm(got[:, o] - ref[:, o]) / np.linalg.norm(ref[:, o])
+            assert err < 2e-2, (d, o, err)
+    s.close()
+
+
+def test_zero_dissipation_bound_is_plain_hllc():
+    from gaukuk_b200.sim import Sim
+    p, c = problems.kh(64, seed=5)
+    X, Y = _data(256)
+    blob = learned.init_model(X, Y, seed=9)
+    a, b = Sim(p, c, mode="parity"), Sim(p, c, mode="parity")
+    learned.install(b, blob, shock_jump=10.0, pos_frac=1.0, tv_min=0.0, diss_frac=0.0)
+    a.run_steps(6)
+    b.run_steps(6)
+    assert np.array_equal(active(p, a.download()), active(p, b.download()))
+
+
 def test_zero_model_is_plain_hllc_bitwise():
     from gaukuk_b200.sim import Sim
     p, c = problems.kh(96, ny=80, seed=1)
@@ -99,14 +163,15 @@ def test_zero_model_is_plain_hllc_bitwise():
 
 
 def test_detector_fallback_is_plain_hllc():
-    """With pos_frac = 0 every correction trips the positivity detector, so
-    the corrected solver must reproduce plain HLLC exactly."""
+    """With pos_frac = 0, no smoothness gate and no clip every correction
+    trips the positivity detector, so the corrected solver must reproduce
+    plain HLLC exactly."""
     from gaukuk_b200.sim import Sim
     p, c = problems.kh(64, seed=2)
     X, Y = _data(256)
     blob = learned.init_model(X, Y, seed=6)
     a, b = Sim(p, c, mode="parity"), Sim(p, c, mode="parity")
-    learned.install(b, blob, shock_jump=0.5, pos_frac=0.0)
+    learned.install(b, blob, shock_jump=0.5, pos_frac=0.0, tv_min=0.0, diss_frac=-1.0)
     a.run_steps(6)
     b.run_steps(6)
     assert np.array_equal(active(p, a.download()), active(p, b.download()))
