@@ -497,11 +497,13 @@ def main_learned(args, rank, world, local_rank):
                       **fit},
             "gate": {"tv_min": tv_min, "diss_frac": diss_frac, "shock_jump": 0.5, "pos_frac": 0.02},
             "summary": sm,
-            "time_ratio_learned_over_plain2x": sm[lr_]["mean_seconds"] / sm[c2]["mean_seconds"],
+            "time_ratio_learned_over_plain2x": (sm[lr_]["mean_seconds"] / sm[c2]["mean_seconds"]
+                                                if sm[lr_]["mean_seconds"] else None),
             "l1_ratio_learned_over_plain": [a / b for a, b in zip(sm[lr_]["mean_l1_at_%d" % args.coarse],
                                                                   sm[c]["mean_l1_at_%d" % args.coarse])],
             "l1_ratio_learned_over_plain2x": [a / b for a, b in zip(sm[lr_]["mean_l1_at_%d" % args.coarse],
                                                                     sm[c2]["mean_l1_at_%d" % args.coarse])],
+            "learned_diverged": sm[lr_]["diverged"],
             "model": args.model_out}))
     return 0
 

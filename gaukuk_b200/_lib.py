@@ -74,6 +74,7 @@ SIGNATURES = {
     "gk_mlp_create": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
     "gk_mlp_destroy": (None, [_vp]),
     "gk_mlp_get": (ctypes.c_int, [_vp, _vp]),
+    "gk_mlp_set_pair_loss": (ctypes.c_int, [_vp, ctypes.c_float]),
     "gk_mlp_grad": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_longlong, ctypes.c_int, _vp, _vp]),
     "gk_mlp_train": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_float, ctypes.c_ulonglong, _vp]),

@@ -181,11 +181,25 @@ struct TrainShared {
     TileAct act[4];
 };
 
+// Sample in row r of tile `tile` of a batch: idx[tile*16 + r] when a batch
+// index list is given, else the samples in order; in pair mode the in-order
+// rows r and r + 8 hold the two members of a pair (2m, 2m + 1).
+__device__ __forceinline__ long long batch_sample(const long long* idx, int tile, int r, bool pairs) {
+    if (idx) return idx[tile * 16 + r];
+    return (long long)tile * 16 + (pairs ? 2 * (r & 7) + (r >> 3) : r);
+}
+
+// Loss per sample: the squared error summed over the 4 outputs; in pair mode
+// (pairs of samples that are neighbouring faces, rows g and g + 8 of a tile)
+// (1 - pw) (e0^2 + e1^2) + pw (e1 - e0)^2 per output, e the errors of the two
+// members: the error of their difference is what the cell between the two
+// faces sees.
 __global__ void __launch_bounds__(128) k_mlp_grad(const float* __restrict__ params,
                                                   const __nv_bfloat16* __restrict__ X,
                                                   const float* __restrict__ T, long long n,
                                                   const long long* __restrict__ idx, int batch,
-                                                  float* __restrict__ grad, float* __restrict__ loss) {
+                                                  float* __restrict__ grad, float* __restrict__ loss,
+                                                  int pairs, float pw) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TrainShared& sh = *reinterpret_cast<TrainShared*>(smem_raw);
     load_weights(sh.w, params);
@@ -202,7 +216,7 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const float* __restrict__ para
         // ---- per-tile forward and backward (one warp per tile)
         if (live) {
             for (int e = lane; e < 16 * NI; e += 32) {
-                const long long s = idx ? idx[tile * 16 + e / NI] : (long long)tile * 16 + e / NI;
+                const long long s = batch_sample(idx, tile, e / NI, pairs);
                 act.x[e] = X[s * NI + e % NI];
             }
             __syncwarp();
@@ -211,12 +225,19 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const float* __restrict__ para
             // dY = 2/B (Y - T) on columns 0..3 (rows g, g+8; columns 2t, 2t+1)
             float dy[4] = {0.f, 0.f, 0.f, 0.f};
             if (t < 2) {
-                const long long s0 = idx ? idx[tile * 16 + g] : (long long)tile * 16 + g;
-                const long long s8 = idx ? idx[tile * 16 + g + 8] : (long long)tile * 16 + g + 8;
+                const long long s0 = batch_sample(idx, tile, g, pairs);
+                const long long s8 = batch_sample(idx, tile, g + 8, pairs);
                 const float r0 = y[0] - T[s0 * NO + 2 * t], r1 = y[1] - T[s0 * NO + 2 * t + 1];
                 const float r2 = y[2] - T[s8 * NO + 2 * t], r3 = y[3] - T[s8 * NO + 2 * t + 1];
-                lsum += r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3;
-                dy[0] = scale * r0; dy[1] = scale * r1; dy[2] = scale * r2; dy[3] = scale * r3;
+                if (pairs) {
+                    const float d0 = r2 - r0, d1 = r3 - r1, u = 1.f - pw;
+                    lsum += u * (r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3) + pw * (d0 * d0 + d1 * d1);
+                    dy[0] = scale * (u * r0 - pw * d0); dy[1] = scale * (u * r1 - pw * d1);
+                    dy[2] = scale * (u * r2 + pw * d0); dy[3] = scale * (u * r3 + pw * d1);
+                } else {
+                    lsum += r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3;
+                    dy[0] = scale * r0; dy[1] = scale * r1; dy[2] = scale * r2; dy[3] = scale * r3;
+                }
             }
             // dY as BF16 A operand [16 samples][16 outputs], columns >= 4 zero
             act.dy[g * 16 + 2 * t] = __float2bfloat16_rn(dy[0]);
@@ -352,15 +373,20 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const float* __restrict__ para
 }
 
 // Batch of sample indices for one step: splitmix64 of (seed, step, i) mod n.
+// In pair mode rows r and r + 8 of each 16-row tile draw the same pair m
+// and take its members 2m and 2m + 1.
 __global__ void k_batch_indices(long long* idx, int batch, long long n, unsigned long long seed,
-                                long long step) {
+                                long long step, int pairs) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= batch) return;
-    unsigned long long z = seed + 0x9E3779B97F4A7C15ULL * (unsigned long long)(step * batch + i + 1);
+    const int r = i & 15;
+    const long long key = pairs ? (long long)(i >> 4) * 8 + (r & 7) : i;
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ULL * (unsigned long long)(step * batch + key + 1);
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
     z ^= z >> 31;
-    idx[i] = (long long)(z % (unsigned long long)n);
+    idx[i] = pairs ? 2 * (long long)(z % (unsigned long long)(n / 2)) + (r >> 3)
+                   : (long long)(z % (unsigned long long)n);
 }
 
 // Adam (Kingma & Ba 2015) on the FP32 master parameters; zeroes the gradient.
@@ -597,6 +623,8 @@ struct gk_mlp {
     long long* idx = nullptr;
     int idx_cap = 0;
     int step = 0;
+    int pairs = 0;      // samples are neighbouring-face pairs (2m, 2m + 1)
+    float pair_w = 0.f; // weight of the pair-difference term of the loss
     cudaStream_t stream = nullptr;
 };
 
@@ -652,6 +680,13 @@ int gk_mlp_get(gk_mlp* M, float* model_host) {
 // updating; X: n x 16 BF16 device, T: n x 4 FP32 device; the first `batch`
 // samples in order.  grad_host: NPARAM floats; loss_host: the summed squared
 // error.
+int gk_mlp_set_pair_loss(gk_mlp* M, float w) {
+    if (!M || !(w <= 1.f)) return GK_ERR_INVALID;
+    M->pairs = w >= 0.f;
+    M->pair_w = w >= 0.f ? w : 0.f;
+    return GK_OK;
+}
+
 int gk_mlp_grad(gk_mlp* M, const void* X, const float* T, long long n, int batch,
                 float* grad_host, float* loss_host) {
     if (!M || !X || !T || batch <= 0 || batch % 16 || batch > n) return GK_ERR_INVALID;
@@ -659,7 +694,8 @@ int gk_mlp_grad(gk_mlp* M, const void* X, const float* T, long long n, int batch
     cudaMemsetAsync(M->loss, 0, sizeof(float), M->stream);
     const int ctas = (batch / 16 + 3) / 4 < 148 * 4 ? (batch / 16 + 3) / 4 : 148 * 4;
     k_mlp_grad<<<ctas, 128, train_smem(), M->stream>>>(M->params, (const __nv_bfloat16*)X, T, n,
-                                                       nullptr, batch, M->grad, M->loss);
+                                                       nullptr, batch, M->grad, M->loss, M->pairs,
+                                                       M->pair_w);
     if (cudaGetLastError() != cudaSuccess) return GK_ERR_CUDA;
     if (grad_host && cudaMemcpyAsync(grad_host, M->grad, sizeof(float) * NPARAM,
                                      cudaMemcpyDeviceToHost, M->stream) != cudaSuccess)
@@ -678,6 +714,7 @@ int gk_mlp_grad(gk_mlp* M, const void* X, const float* T, long long n, int batch
 int gk_mlp_train(gk_mlp* M, const void* X, const float* T, long long n, int batch, int steps,
                  float lr, unsigned long long seed, float* loss_host) {
     if (!M || !X || !T || batch <= 0 || batch % 16 || n <= 0 || steps < 0) return GK_ERR_INVALID;
+    if (M->pairs && (n < 2 || n % 2)) return GK_ERR_INVALID;
     if (M->idx_cap < batch) {
         cudaFree(M->idx);
         if (cudaMalloc(&M->idx, sizeof(long long) * batch) != cudaSuccess) return GK_ERR_CUDA;
@@ -686,11 +723,12 @@ int gk_mlp_train(gk_mlp* M, const void* X, const float* T, long long n, int batc
     const int ctas = (batch / 16 + 3) / 4 < 148 * 4 ? (batch / 16 + 3) / 4 : 148 * 4;
     for (int s = 0; s < steps; ++s) {
         ++M->step;
-        k_batch_indices<<<(batch + 255) / 256, 256, 0, M->stream>>>(M->idx, batch, n, seed, M->step);
+        k_batch_indices<<<(batch + 255) / 256, 256, 0, M->stream>>>(M->idx, batch, n, seed, M->step,
+                                                                    M->pairs);
         if (s == steps - 1) cudaMemsetAsync(M->loss, 0, sizeof(float), M->stream);
         k_mlp_grad<<<ctas, 128, train_smem(), M->stream>>>(
             M->params, (const __nv_bfloat16*)X, T, n, M->idx, batch, M->grad,
-            s == steps - 1 ? M->loss : nullptr);
+            s == steps - 1 ? M->loss : nullptr, M->pairs, M->pair_w);
         k_adam<<<(NPARAM + 255) / 256, 256, 0, M->stream>>>(M->params, M->m, M->v, M->grad, lr,
                                                             0.9f, 0.999f, 1e-8f, M->step);
     }

@@ -204,7 +204,8 @@ def perturb(p: Params, cons: np.ndarray, ratio: int, sigma: float, rng) -> np.nd
 def generate(seeds: Sequence[int], coarse: int = 256, ratio: int = 4, t_end: float = 2.0,
              snapshots: int = 16, frac: float = 0.25, mode: str = "fast",
              sample_seed: int = 0, tv_min: float = TV_GATE, noise: float = 0.0,
-             noisy: int = 1, first: float = 1.0, log=print) -> Tuple[np.ndarray, np.ndarray]:
+             noisy: int = 1, first: float = 1.0, pairs: bool = False,
+             log=print) -> Tuple[np.ndarray, np.ndarray]:
     """Training pairs from fine runs (coarse*ratio)^2 restricted to coarse^2.
 
     At `snapshots` times t_end (s + first) / (snapshots + first), s = 0 ..
@@ -222,7 +223,12 @@ def generate(seeds: Sequence[int], coarse: int = 256, ratio: int = 4, t_end: flo
     fine state perturbed by ``perturb`` (block noise of relative amplitude
     `noise` on the coarse cells): the fine solver's response to grid-scale
     perturbations, which restricted states alone never show and which a
-    correction must damp for a coarse run to stay stable."""
+    correction must damp for a coarse run to stay stable.
+
+    With pairs=True each kept face f is followed by its neighbour across the
+    next cell in the normal direction (rows 2m, 2m + 1), the layout of the
+    pair loss (Trainer.set_pair_loss); a pair is kept when f's variation is
+    at least `tv_min`."""
     from .sim import Sim
     rng = np.random.default_rng(sample_seed)
     Xs, Ys = [], []
@@ -238,8 +244,16 @@ def generate(seeds: Sequence[int], coarse: int = 256, ratio: int = 4, t_end: flo
             Y = np.stack([D[:, 0] / S[:, 0], D[:, 1] / S[:, 1], D[:, 2] / S[:, 1],
                           D[:, 3] / S[:, 2]], axis=1)
             keep = (rng.random(len(X)) < frac) & (G >= tv_min)
-            Xs.append(X[keep].astype(np.float32))
-            Ys.append(Y[keep].astype(np.float32))
+            if pairs:
+                f = np.flatnonzero(keep)
+                j, i = f // pc.nx, f % pc.nx
+                nb = j * pc.nx + (i + 1) % pc.nx if direction == 0 else ((j + 1) % pc.ny) * pc.nx + i
+                sel = np.stack([f, nb], axis=1).ravel()
+                Xs.append(X[sel].astype(np.float32))
+                Ys.append(Y[sel].astype(np.float32))
+            else:
+                Xs.append(X[keep].astype(np.float32))
+                Ys.append(Y[keep].astype(np.float32))
 
     for k, seed in enumerate(seeds):
         t0 = time.time()
@@ -330,6 +344,12 @@ class Trainer:
                                         int(steps), float(lr), int(seed), ctypes.byref(loss)))
         return loss.value
 
+    def set_pair_loss(self, w: float) -> None:
+        """w < 0: per-face squared error; 0 <= w <= 1: the data are
+        neighbouring-face pairs and the loss weights their difference by w
+        (gk_mlp_set_pair_loss)."""
+        _lib.check(self._L.gk_mlp_set_pair_loss(self.m, float(w)))
+
     def gradient(self, batch: int):
         g = np.empty(NPARAM, dtype=np.float32)
         loss = ctypes.c_float()
@@ -383,19 +403,33 @@ def detector_count(sim) -> int:
 
 
 # ------------------------------------------------------------------ evaluation
-def _timed_run(sim, times: Sequence[float]) -> Tuple[List[np.ndarray], float]:
-    """Runs to each time in `times`; returns the density at each and the GPU
-    wall time spent inside the advance calls."""
+def _timed_run(sim, times: Sequence[float],
+               max_steps: Optional[int] = None) -> Tuple[List[np.ndarray], float, bool]:
+    """Runs to each time in `times`; returns the density at each, the GPU
+    wall time spent inside the advance calls, and whether the run diverged:
+    took more than `max_steps` steps (its time step collapsed) or failed.
+    The densities after a divergence are NaN."""
     import torch
-    out, spent = [], 0.0
+    out, spent, diverged = [], 0.0, False
+    chunks = 1 if max_steps is None else 16
     for tt in times:
-        torch.cuda.synchronize()
-        a = time.perf_counter()
-        sim.advance(tt - sim.get_time())
-        torch.cuda.synchronize()
-        spent += time.perf_counter() - a
-        out.append(active2d(sim.params, sim.download())[0].copy())
-    return out, spent
+        t0 = sim.get_time()
+        for c in range(1, chunks + 1):
+            if diverged:
+                break
+            torch.cuda.synchronize()
+            a = time.perf_counter()
+            try:
+                sim.advance(t0 + (tt - t0) * c / chunks - sim.get_time())
+            except _lib.GkError:
+                diverged = True
+            torch.cuda.synchronize()
+            spent += time.perf_counter() - a
+            if max_steps is not None and sim.get_step() > max_steps:
+                diverged = True
+        rho = active2d(sim.params, sim.download())[0].copy()
+        out.append(np.full_like(rho, np.nan) if diverged else rho)
+    return out, spent, diverged
 
 
 def _restrict_rho(rho: np.ndarray, r: int) -> np.ndarray:
@@ -409,12 +443,16 @@ def evaluate(blob: np.ndarray, seeds: Sequence[int], coarse: int = 256, t_end: f
              diss_frac: float = DISS_FRAC, log=print) -> Dict:
     """L1 density error against the 4x fine plain run (the judge) for plain
     coarse, plain 2x coarse and learned coarse, each started from the
-    restriction of the same fine initial state, and their GPU times."""
+    restriction of the same fine initial state, and their GPU times.  A
+    learned run that takes more than 4x the steps of the plain run at its
+    resolution (a collapsed time step) is stopped and recorded as diverged."""
     from .sim import Sim
     rows = []
     for seed in seeds:
         pf, cf, draw = kh_instance(seed, 4 * coarse, t_end)
-        judge, _ = _timed_run(Sim(pf, cf, mode=mode), times)
+        js = Sim(pf, cf, mode=mode)
+        judge, _, _ = _timed_run(js, times)
+        js.close()
         res = {"seed": seed, **draw}
         for name, ratio, learned in (("plain_%d" % coarse, 4, False),
                                      ("plain_%d" % (2 * coarse), 2, False),
@@ -426,15 +464,17 @@ def evaluate(blob: np.ndarray, seeds: Sequence[int], coarse: int = 256, t_end: f
             s.run_steps(1)  # build the graph outside the timing
             s.set_time(0.0, 0)
             s.upload(cc)
-            rho, secs = _timed_run(s, times)
+            cap = 4 * res["plain_%d" % coarse]["steps"] if learned else None
+            rho, secs, diverged = _timed_run(s, times, cap)
             m0 = active2d(pc, cc)[0].sum()
             res[name] = {
                 "seconds": secs,
                 "steps": s.get_step(),
+                "diverged": diverged,
                 "l1": [float(np.mean(np.abs(r - _restrict_rho(j, ratio)))) for r, j in zip(rho, judge)],
                 "l1_at_%d" % coarse: [float(np.mean(np.abs(_restrict_rho(r, 4 // ratio) - _restrict_rho(j, 4))))
                                       for r, j in zip(rho, judge)],
-                "mass_drift": float(abs(rho[-1].sum() - m0) / m0),
+                "mass_drift": None if diverged else float(abs(rho[-1].sum() - m0) / m0),
             }
             if learned:
                 res[name]["detector_faces"] = detector_count(s)
@@ -454,7 +494,10 @@ def summarise(rows: List[Dict], coarse: int) -> Dict:
     keys = ["plain_%d" % coarse, "plain_%d" % (2 * coarse), "learned_%d" % coarse]
     out = {}
     for k in keys:
-        l1 = np.array([r[k]["l1_at_%d" % coarse] for r in rows])
+        ok = [r for r in rows if not r[k].get("diverged")]
+        l1 = np.array([r[k]["l1_at_%d" % coarse] for r in ok]) if ok else np.full((1, 1), np.nan)
         out[k] = {"mean_l1_at_%d" % coarse: l1.mean(axis=0).tolist(),
-                  "mean_seconds": float(np.mean([r[k]["seconds"] for r in rows]))}
+                  "median_l1_at_%d" % coarse: np.median(l1, axis=0).tolist(),
+                  "mean_seconds": float(np.mean([r[k]["seconds"] for r in ok])) if ok else None,
+                  "runs": len(ok), "diverged": len(rows) - len(ok)}
     return out

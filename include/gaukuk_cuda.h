@@ -202,6 +202,12 @@ int gk_mlp_nmodel(void);
 int gk_mlp_create(const float* model_host, gk_mlp** out);
 void gk_mlp_destroy(gk_mlp* m);
 int gk_mlp_get(gk_mlp* m, float* model_host);
+/* Loss of the training calls.  w < 0 (the default): the squared error of
+ * each sample summed over the outputs.  0 <= w <= 1: the samples come in
+ * pairs (2m, 2m + 1) of neighbouring faces and each pair's loss per output
+ * is (1 - w)(e0^2 + e1^2) + w (e1 - e0)^2, the last term being the error of
+ * the update of the cell between the two faces; n must then be even. */
+int gk_mlp_set_pair_loss(gk_mlp* m, float w);
 /* Summed gradient of the first `batch` samples (no update).  X: n x 16 BF16
  * and T: n x 4 FP32 (standardised), on the device. */
 int gk_mlp_grad(gk_mlp* m, const void* X, const float* T, long long n, int batch,

@@ -38,8 +38,11 @@ def gelu(x):
     return 0.5 * x * (1 + th), 0.5 * (1 + th) + 0.5 * x * (1 - th ** 2) * A * (1 + 3 * B * x * x)
 
 
-def forward_backward(blob, X, T, rounding=True):
-    """Loss (sum of squared errors) and the batch-summed gradient (NPARAM)."""
+def forward_backward(blob, X, T, rounding=True, pair_w=None):
+    """Loss and the batch-summed gradient (NPARAM).  pair_w None: the sum of
+    squared errors.  Otherwise samples (2m, 2m + 1) are pairs and each pair
+    contributes (1 - w)(e0^2 + e1^2) + w (e1 - e0)^2 per output
+    (gaukuk_b200/csrc/gk_mlp.cu, k_mlp_grad)."""
     r = bf16 if rounding else (lambda v: np.asarray(v, np.float64))
     w1, b1, w2, b2, w3, b3 = unpack(blob)
     w1r, w2r, w3r = r(w1), r(w2), r(w3)
@@ -53,8 +56,18 @@ def forward_backward(blob, X, T, rounding=True):
     y = h2 @ w3r.T + b3
     res = y - T
     n = len(X)
-    loss = float(np.sum(res * res))
-    dy = r(2.0 / n * res)
+    if pair_w is None:
+        loss = float(np.sum(res * res))
+        dres = res
+    else:
+        w = float(pair_w)
+        e0, e1 = res[0::2], res[1::2]
+        d = e1 - e0
+        loss = float(np.sum((1 - w) * (e0 * e0 + e1 * e1) + w * d * d))
+        dres = np.empty_like(res)
+        dres[0::2] = (1 - w) * e0 - w * d
+        dres[1::2] = (1 - w) * e1 + w * d
+    dy = r(2.0 / n * dres)
     dh2 = dy @ w3r
     dz2 = r(dh2 * d2)
     dh1 = dz2 @ w2r

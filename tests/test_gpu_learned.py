@@ -39,6 +39,24 @@ def test_gradient_matches_cpu_oracle():
     tr.close()
 
 
+def test_pair_loss_gradient_matches_cpu_oracle():
+    X, Y = _data(1024, seed=5)
+    blob = learned.init_model(X, Y, seed=6)
+    tr = learned.Trainer(blob, X, Y)
+    tr.set_pair_loss(0.8)
+    g, loss = tr.gradient(1024)
+    Xn, Yn = learned.standardise(blob, X, Y)
+    l_ref, g_ref, _ = mlp_oracle.forward_backward(blob[:learned.NPARAM], Xn, Yn, rounding=True,
+                                                  pair_w=0.8)
+    assert abs(loss - l_ref) <= 1e-3 * l_ref
+    err = np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
+    assert err < 1e-2, err
+    l0 = tr.train(1, batch=1024, lr=1e-3)
+    l1 = tr.train(300, batch=1024, lr=3e-3)
+    assert l1 < 0.5 * l0, (l0, l1)
+    tr.close()
+
+
 def test_forward_matches_cpu_oracle():
     X, Y = _data(512, seed=1)
     blob = learned.init_model(X, Y, seed=4)

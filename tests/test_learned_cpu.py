@@ -23,6 +23,26 @@ def test_oracle_backward_matches_finite_differences():
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])), (i, fd, g[i])
 
 
+def test_pair_loss_gradient_matches_finite_differences():
+    rng = np.random.default_rng(4)
+    X, T = rng.normal(size=(16, 16)), rng.normal(size=(16, 4))
+    b = learned.init_model(X, T, seed=2)[:learned.NPARAM].astype(np.float64)
+    b[-4 - 4 * 64:] = rng.normal(size=4 + 4 * 64) * 0.3  # a last layer of some size
+    for w in (0.0, 0.7, 1.0):
+        _, g, _ = mlp_oracle.forward_backward(b, X, T, False, pair_w=w)
+        for i in rng.choice(len(b), 12, replace=False):
+            eps = 1e-6
+            bp, bm = b.copy(), b.copy()
+            bp[i] += eps
+            bm[i] -= eps
+            fd = (mlp_oracle.forward_backward(bp, X, T, False, pair_w=w)[0]
+                  - mlp_oracle.forward_backward(bm, X, T, False, pair_w=w)[0]) / (2 * eps) / len(X)
+            assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])), (w, i, fd, g[i])
+    # w = 0 is the per-sample squared error
+    assert np.isclose(mlp_oracle.forward_backward(b, X, T, False, pair_w=0.0)[0],
+                      mlp_oracle.forward_backward(b, X, T, False)[0])
+
+
 def test_bf16_rounding_is_nearest_even():
     x = np.array([1.0, 1.00390625, 1.0078125, 3.14159265, -2.5e-3])
     r = mlp_oracle.bf16(x)
