@@ -433,6 +433,77 @@ def main_ensemble(args, rank, world, local_rank):
     return 0
 
 
+def main_configs(args, rank, world, local_rank):
+    """The plain-method configurations run to their end times on one GPU:
+    Sod 256 (t = 0.2, against the exact Riemann solution), KH 256^2 (t = 2,
+    conservation), RT 1024x3072 (RK3 + gravity, t = 5, mirror symmetry), in
+    both arithmetic modes, with the reference build (fast flags, OpenMP on
+    the host cores) on the same inputs -- the whole run for Sod and KH 256^2,
+    the first 200 steps for RT.  Timing: host wall clock around Sim.run with
+    a device synchronise on both sides (each config is one long sequence of
+    graph launches); the reference's is its driver's time inside Advance."""
+    import numpy as np
+    import torch
+
+    from gaukuk_b200 import problems
+    from gaukuk_b200.sim import Sim
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gk_oracle
+    import riemann_exact as rx
+
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    threads = host_threads()
+    out = []
+    cases = [("sod256", problems.sod(256)), ("kh256", problems.kh(256)),
+             ("rt1024x3072", problems.rt(1024, 3072))]
+    for name, (p, c) in cases:
+        cells = p.nx * p.ny * p.nz
+        row = {"config": name, "grid": [p.nx, p.ny, p.nz], "integrator": p.integrator, "tmax": p.tmax}
+        a0 = c[:, p.ng, p.ng:p.ng + p.ny, p.ng:p.ng + p.nx]
+        for mode in ("fast", "parity"):
+            with Sim(p, c, mode=mode) as s:
+                s.run_steps(1)  # graph and first-touch outside the timing
+                s.set_time(0.0, 0)
+                s.upload(c)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                s.run(p.tmax, p.tmax)
+                torch.cuda.synchronize()
+                secs = time.perf_counter() - t0
+                steps = s.get_step()
+                fin = s.download()
+            a = fin[:, p.ng, p.ng:p.ng + p.ny, p.ng:p.ng + p.nx]
+            r = {"steps": steps, "seconds": secs, "zone_updates_per_s": cells * steps / secs}
+            r["mass_drift"] = float(abs(a[0].sum() - a0[0].sum()) / a0[0].sum())
+            if name.startswith("sod"):
+                xl = np.arange(p.nx) / p.nx
+                rho, _, _ = rx.cell_average(xl, xl + 1.0 / p.nx, p.tmax, 0.5, (1.0, 0.0, 1.0),
+                                            (0.125, 0.0, 0.1))
+                r["l1_rho_vs_exact"] = float(np.abs(a[0, 0] - rho).mean())
+            elif name.startswith("kh"):
+                r["energy_drift"] = float(abs(a[4].sum() - a0[4].sum()) / a0[4].sum())
+            else:
+                r["mirror_asymmetry_rho"] = float(np.abs(a[0] - a[0][:, ::-1]).max() / a[0].max())
+            row[mode] = r
+        full = not name.startswith("rt")
+        try:
+            _, dts, st = gk_oracle.run_reference(p, c, stepmax=None if full else 200, flavour="fast",
+                                                 threads=threads, timeout=900)
+            row["reference"] = {"steps": st["steps"], "seconds": st["advance_seconds"],
+                                "zone_updates_per_s": cells * st["steps"] / st["advance_seconds"],
+                                "cores": threads, "sample": "whole run" if full else "first 200 steps"}
+        except Exception as e:  # the reference build is optional on the box
+            row["reference"] = {"unavailable": str(e)[:200]}
+        out.append(row)
+        print(json.dumps(row), file=sys.stderr, flush=True)
+    print(json.dumps({"workload": "configs", "metric": METRIC, "unit": UNIT, "dtype": "f64",
+                      "data": "synthetic (seeded initial conditions of the named shapes)",
+                      "runs": out}))
+    return 0
+
+
 def main_learned(args, rank, world, local_rank):
     """Pattern 4: data from 4x finer plain runs, training on the GPU with the
     project's BF16 kernels, evaluation on held-out seeds against plain coarse,
@@ -518,7 +589,7 @@ def main():
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="kh4096", choices=["kh4096", "ensemble", "learned"])
+    ap.add_argument("--workload", default="kh4096", choices=["kh4096", "ensemble", "learned", "configs"])
     ap.add_argument("--train-seeds", type=int, default=16)
     ap.add_argument("--eval-seeds", type=int, default=8)
     ap.add_argument("--coarse", type=int, default=256)
@@ -551,6 +622,8 @@ def main():
         return main_ensemble(args, rank, world, local_rank)
     if args.workload == "learned":
         return main_learned(args, rank, world, local_rank)
+    if args.workload == "configs":
+        return main_configs(args, rank, world, local_rank)
     return main_ours(args, rank, world, local_rank)
 
 

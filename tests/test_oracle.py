@@ -95,3 +95,50 @@ def test_conservation_periodic_kh():
     m1 = active(p, o.get_cons()).sum(axis=(1, 2, 3))
     assert abs(m1[0] - m0[0]) / m0[0] < 1e-14
     assert abs(m1[4] - m0[4]) / m0[4] < 1e-14
+
+
+# ------------------------------------------------------------------ exact Riemann solution (Sod)
+def _riemann():
+    return pytest.importorskip("riemann_exact")
+
+
+SOD_L, SOD_R = (1.0, 0.0, 1.0), (0.125, 0.0, 0.1)
+
+
+def test_exact_riemann_star_state_matches_toro():
+    """Toro (2009) Table 4.3, Test 1 (the Sod problem): p* 0.30313,
+    u* 0.92745, rho*L 0.42632, rho*R 0.26557."""
+    rx = _riemann()
+    ps, us = rx.star_state(SOD_L, SOD_R)
+    rl, rr = rx.star_densities(SOD_L, SOD_R)
+    assert abs(ps - 0.30313) < 5e-6 and abs(us - 0.92745) < 5e-6
+    assert abs(rl - 0.42632) < 5e-6 and abs(rr - 0.26557) < 5e-6
+
+
+def test_exact_sod_solution_conserves():
+    rx = _riemann()
+    n = 400
+    xl = np.arange(n) / n
+    rho, m, e = rx.cell_average(xl, xl + 1.0 / n, 0.2, 0.5, SOD_L, SOD_R, sub=256)
+    # the waves stay inside [0, 1] up to t = 0.2; flux in = flux out = p at the walls
+    assert abs(rho.mean() - 0.5625) < 1e-4
+    assert abs(e.mean() - 1.375) < 1e-4
+
+
+def test_sod_converges_to_the_exact_solution():
+    """The oracle's Sod run (PLM + HLLC + RK2, CFL 0.4, outflow) against the
+    exact cell averages at t = 0.2: L1(rho) about 1.8e-3 at 256 cells,
+    shrinking with resolution; mass exact."""
+    rx = _riemann()
+    from gaukuk_b200 import problems
+    errs = []
+    for n in (256, 512):
+        p, c = problems.sod(n)
+        o = gk_oracle.OracleSim(p, c)
+        o.run(0.2, 0.2)
+        a = o.get_cons()[:, p.ng, p.ng, p.ng:p.ng + n]
+        xl = np.arange(n) / n
+        rho, m, e = rx.cell_average(xl, xl + 1.0 / n, o.time, 0.5, SOD_L, SOD_R)
+        errs.append(np.abs(a[0] - rho).mean())
+        assert abs(a[0].mean() - 0.5625) < 1e-14
+    assert errs[0] < 2.5e-3 and errs[1] < 0.75 * errs[0], errs
