@@ -51,6 +51,10 @@ public:
     void Setup();
     void Advance(Real dtoutput);
     void WriteData(const int outputID, DataType dType);
+    // Restart: loads time and conserved state from the frame cons_<outputID>
+    // that WriteData wrote (the grid must match); the step counter restarts
+    // at 0, since frames do not carry it.
+    void ReadData(const int outputID);
 
     Real GetTime() { return t; }
     Real Getdt() { return dt; }

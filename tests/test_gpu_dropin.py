@@ -68,3 +68,25 @@ def test_frames_byte_identical_to_reference(name, tmp_path):
         ng = [float(v.split("=")[1]) for v in lg.split(",")]
         assert nr[0] == ng[0]
         np.testing.assert_allclose(nr[1:], ng[1:], rtol=1e-5)
+
+
+@pytest.mark.parametrize("hook", ["kh_baseline", "rt_baseline"])
+def test_restart_continues_bit_identically(hook, tmp_path):
+    """A run resumed from its own frame cons_00002 (input key restart = 2)
+    writes frames 3, 4, ... byte-identical to those of the uninterrupted run:
+    a frame holds the exact time and state, and the step is a function of
+    them alone."""
+    name = "kh_baseline" if hook == "kh_baseline" else "rt_baseline"
+    p, extra = CASES[name]
+    exe = os.path.join(BIN, f"gaukuk_{hook}.sim")
+    a, b = tmp_path / "full", tmp_path / "resumed"
+    a.mkdir(); b.mkdir()
+    (a / "run.in").write_text(p.to_in_text(extra))
+    _run(exe, ["-i", "run.in"], a)
+    (b / "cons_00002").write_bytes((a / "cons_00002").read_bytes())
+    (b / "run.in").write_text(p.to_in_text(dict(extra, restart=2)))
+    _run(exe, ["-i", "run.in"], b)
+    later = sorted(f for f in os.listdir(a) if f.startswith("cons_") and f > "cons_00002")
+    assert later and later == sorted(f for f in os.listdir(b) if f.startswith("cons_") and f > "cons_00002")
+    for f in later:
+        assert (a / f).read_bytes() == (b / f).read_bytes(), f
