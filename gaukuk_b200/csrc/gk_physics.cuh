@@ -17,29 +17,26 @@ __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b 
 // Reciprocal, quotient and square root for finite, positive, normal
 // arguments (densities, pressures, sound speeds, wave-speed differences).
 // Each starts from the hardware approximation (PTX rcp.approx.ftz.f64 /
-// rsqrt.approx.ftz.f64, about 2^-22 relative error) and applies two
-// Newton-Raphson steps, which square the relative error each time:
-//   reciprocal  y' = y + y*(1 - b*y)
-//   rsqrt       y' = y + y*(1/2 - (x/2)*y*y)
-// The square root is x*rsqrt(x) with one Newton correction of the residual
-// x - s*s (Markstein, IBM J. Res. Dev. 34(1), 1990).  The result is within a
-// few ulp of the IEEE value; there is no slow path and no branch.
+// rsqrt.approx.ftz.f64, about 2^-22 relative error) and applies one
+// third-order step of the binomial series, which cubes the relative error:
+//   reciprocal  e = 1 - b*y,    y' = y*(1 + e + e^2)
+//   rsqrt       d = 1 - x*y^2,  y' = y*(1 + d/2 + 3d^2/8)
+// (the series of (1 - e)^-1 and (1 - d)^-1/2 to second order; one step does
+// the work of two Newton steps in fewer operations).  The square root is
+// x*rsqrt(x) with one Newton correction of the residual x - s*s (Markstein,
+// IBM J. Res. Dev. 34(1), 1990).  The result is within a few ulp of the IEEE
+// value; there is no slow path and no branch.
 __device__ __forceinline__ double rcp_nr(double b) {
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
-    double e = fma(-b, y, 1.0);
-    y = fma(y, e, y);
-    e = fma(-b, y, 1.0);
-    return fma(y, e, y);
+    const double e = fma(-b, y, 1.0);
+    return fma(y, fma(e, e, e), y);
 }
 __device__ __forceinline__ double rsqrt_nr(double x) {
     double y;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    const double h = 0.5 * x;
-    double r = fma(-h, y * y, 0.5);
-    y = fma(y, r, y);
-    r = fma(-h, y * y, 0.5);
-    return fma(y, r, y);
+    const double d = fma(-x * y, y, 1.0);
+    return fma(y, d * fma(0.375, d, 0.5), y);
 }
 __device__ __forceinline__ double sqrt_nr(double x) {
     const double y = rsqrt_nr(x);
@@ -97,14 +94,18 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
 #endif
     double prePVRS = 0.5 * (prel + prer) - 0.125 * (vxr - vxl) * (denl + denr) * (al + ar);
     prePVRS = smax(prePVRS, 0.0);
-    double ql, qr;
 #if GK_FASTMATH
+    // a*q = sqrt(gamma p/rho) * sqrt(1 + cq max(p*/p - 1, 0)) = sqrt(gamma X/rho)
+    // with X = p + cq max(p* - p, 0): one root per side, no quotient.
     // Branch-free on purpose: a skip when p* <= p (as in parity mode) was
     // measured slower, because it splits the straight-line code in which the
     // x- and y-face solves of a row interleave.
-    ql = sqrt_nr(1 + ph.cq * smax(prePVRS * rcp_nr(prel) - 1, 0.0));
-    qr = sqrt_nr(1 + ph.cq * smax(prePVRS * rcp_nr(prer) - 1, 0.0));
+    const double gxl = gamma * fma(ph.cq, smax(prePVRS - prel, 0.0), prel);
+    const double gxr = gamma * fma(ph.cq, smax(prePVRS - prer, 0.0), prer);
+    double sl = vxl - gxl * rsqrt_nr(gxl * denl);
+    double sr = vxr + gxr * rsqrt_nr(gxr * denr);
 #else
+    double ql, qr;
     // q = sqrt(1 + 0.5*(1+1/gamma)*max(p*/p - 1, 0)) is exactly 1 whenever
     // p* <= p with p > 0, so the division and root are skipped there.
     ql = 1.0;
@@ -117,9 +118,9 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
         double temp = smax(prePVRS / prer - 1, 0.0);
         qr = sqrt(1 + ph.cq * temp);
     }
-#endif
     double sl = vxl - al * ql;
     double sr = vxr + ar * qr;
+#endif
     double ss = GK_DIV(prer - prel + denl * vxl * (sl - vxl) - denr * vxr * (sr - vxr),
                        denl * (sl - vxl) - denr * (sr - vxr));
     // EquationOfState::EGas (eos.hpp:30-32) + kinetic energy
@@ -156,7 +157,7 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
         const bool left = (ss >= 0);
         double d = left ? denl : denr, vn = left ? vxl : vxr, v1 = left ? vyl : vyr;
         double v2 = left ? vzl : vzr, p = left ? prel : prer, s = left ? sl : sr;
-        double k = left ? kl : kr;
+        double k = T2 ? (vn * vn + v1 * v1 + v2 * v2) : (vn * vn + v1 * v1);
         double e = p * ph.gm1Rec + 0.5 * d * k;
         double sc = left ? smin(0.0, s) : smax(0.0, s);
         double c = GK_DIV(sc * (ss - vn), s - ss);
