@@ -176,8 +176,13 @@ __global__ void k_flux(const double* __restrict__ w, double* __restrict__ F, Geo
             r1 = p[sidx(g, k, j - 1, i)]; r2 = p[sidx(g, k, j, i)]; r3 = p[sidx(g, k, j + 1, i)];
         }
         if (ph.plm) {
+#if GK_FASTMATH
+            wl[v] = l2 + vanleer_half(l2 - l1, l3 - l2);
+            wr[v] = r2 - vanleer_half(r2 - r1, r3 - r2);
+#else
             wl[v] = l2 + 0.5 * vanleer(l2 - l1, l3 - l2);
             wr[v] = r2 - 0.5 * vanleer(r2 - r1, r3 - r2);
+#endif
         } else {
             wl[v] = l2;
             wr[v] = r2;
@@ -456,6 +461,23 @@ __device__ __forceinline__ W4 c2p4(const Q4& q, const Phys& ph) {
     return w;
 }
 
+#if GK_FASTMATH
+// Fast mode: vl4 returns half slopes and the face states add them directly.
+__device__ __forceinline__ W4 vl4(const W4& a, const W4& b, const W4& c) {
+    W4 s;
+    s.r = vanleer_half(b.r - a.r, c.r - b.r);
+    s.vx = vanleer_half(b.vx - a.vx, c.vx - b.vx);
+    s.vy = vanleer_half(b.vy - a.vy, c.vy - b.vy);
+    s.p = vanleer_half(b.p - a.p, c.p - b.p);
+    return s;
+}
+__device__ __forceinline__ W4 plus_half(const W4& u, const W4& h) {
+    return W4{u.r + h.r, u.vx + h.vx, u.vy + h.vy, u.p + h.p};
+}
+__device__ __forceinline__ W4 minus_half(const W4& u, const W4& h) {
+    return W4{u.r - h.r, u.vx - h.vx, u.vy - h.vy, u.p - h.p};
+}
+#else
 __device__ __forceinline__ W4 vl4(const W4& a, const W4& b, const W4& c) {
     W4 s;
     s.r = vanleer(b.r - a.r, c.r - b.r);
@@ -464,13 +486,13 @@ __device__ __forceinline__ W4 vl4(const W4& a, const W4& b, const W4& c) {
     s.p = vanleer(b.p - a.p, c.p - b.p);
     return s;
 }
-
 __device__ __forceinline__ W4 plus_half(const W4& u, const W4& s) {
     return W4{u.r + 0.5 * s.r, u.vx + 0.5 * s.vx, u.vy + 0.5 * s.vy, u.p + 0.5 * s.p};
 }
 __device__ __forceinline__ W4 minus_half(const W4& u, const W4& s) {
     return W4{u.r - 0.5 * s.r, u.vx - 0.5 * s.vx, u.vy - 0.5 * s.vy, u.p - 0.5 * s.p};
 }
+#endif
 
 __device__ __forceinline__ Q4 ldq(const double* __restrict__ u, long long vs, long long c) {
     return Q4{__ldg(u + c), __ldg(u + vs + c), __ldg(u + 2 * vs + c), __ldg(u + 3 * vs + c)};

@@ -64,6 +64,16 @@ __device__ __forceinline__ double vanleer(double a, double b) {
 #endif
 }
 
+#if GK_FASTMATH
+// Half the van Leer slope, (a*b)/(a+b) for ab > 0 else 0: what the PLM face
+// states u +- 0.5*sigma add, without the two scalings by 2 and 1/2.
+__device__ __forceinline__ double vanleer_half(double a, double b) {
+    const double multi = a * b;
+    const double h = GK_DIV(multi, a + b);
+    return (multi <= 0.0) ? 0.0 : h;
+}
+#endif
+
 struct Flux5 {
     double d, n, t1, t2, e;  // density, normal momentum, tangential 1/2, energy
 };
