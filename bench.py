@@ -68,7 +68,7 @@ def measured_peaks():
 
 def ncu_traffic():
     """DRAM bytes per stage-kernel launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "stage2d_kh4096_traffic.json")
+    path = os.path.join(ROOT, "profiles", "stage2d_tma_kh4096_traffic.json")
     try:
         with open(path) as f:
             d = json.load(f)
