@@ -507,7 +507,7 @@ def main_configs(args, rank, world, local_rank):
 def main_learned(args, rank, world, local_rank):
     """Pattern 4: data from 4x finer plain runs, training on the GPU with the
     project's BF16 kernels, evaluation on held-out seeds against plain coarse,
-    plain 2x coarse and the 4x fine judge (L1 density error, GPU time)."""
+    plain 2x coarse and the 4x fine plain run (L1 density error, GPU time)."""
     import numpy as np
     import torch
 

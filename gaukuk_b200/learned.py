@@ -441,7 +441,7 @@ def evaluate(blob: np.ndarray, seeds: Sequence[int], coarse: int = 256, t_end: f
              times: Sequence[float] = (0.5, 1.0, 2.0), mode: str = "fast",
              shock_jump: float = 0.5, pos_frac: float = 0.02, tv_min: float = TV_GATE,
              diss_frac: float = DISS_FRAC, log=print) -> Dict:
-    """L1 density error against the 4x fine plain run (the judge) for plain
+    """L1 density error against the 4x fine plain run (the truth) for plain
     coarse, plain 2x coarse and learned coarse, each started from the
     restriction of the same fine initial state, and their GPU times.  A
     learned run that takes more than 4x the steps of the plain run at its
@@ -451,7 +451,7 @@ def evaluate(blob: np.ndarray, seeds: Sequence[int], coarse: int = 256, t_end: f
     for seed in seeds:
         pf, cf, draw = kh_instance(seed, 4 * coarse, t_end)
         js = Sim(pf, cf, mode=mode)
-        judge, _, _ = _timed_run(js, times)
+        truth, _, _ = _timed_run(js, times)
         js.close()
         res = {"seed": seed, **draw}
         for name, ratio, learned in (("plain_%d" % coarse, 4, False),
@@ -471,9 +471,9 @@ def evaluate(blob: np.ndarray, seeds: Sequence[int], coarse: int = 256, t_end: f
                 "seconds": secs,
                 "steps": s.get_step(),
                 "diverged": diverged,
-                "l1": [float(np.mean(np.abs(r - _restrict_rho(j, ratio)))) for r, j in zip(rho, judge)],
+                "l1": [float(np.mean(np.abs(r - _restrict_rho(j, ratio)))) for r, j in zip(rho, truth)],
                 "l1_at_%d" % coarse: [float(np.mean(np.abs(_restrict_rho(r, 4 // ratio) - _restrict_rho(j, 4))))
-                                      for r, j in zip(rho, judge)],
+                                      for r, j in zip(rho, truth)],
                 "mass_drift": None if diverged else float(abs(rho[-1].sum() - m0) / m0),
             }
             if learned:

@@ -1,5 +1,5 @@
 """Exact solution of the Riemann problem of the 1D Euler equations for an
-ideal gas -- test infrastructure (the judge of the Sod configuration).
+ideal gas -- test infrastructure (the exact answer for the Sod configuration).
 
 The reference claims agreement with the exact solution for its Sod run
 (README.md:30-37) but ships no solver (pypkg/plot_sod.py only overlays
