@@ -222,28 +222,12 @@ def main_ours(args, rank, world, local_rank):
     import torch
 
     from gaukuk_b200 import problems
+    from gaukuk_b200.replicas import Replicas
     from gaukuk_b200.sim import Sim
 
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    else:
-        torch.cuda.set_device(local_rank)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    torch.cuda.set_device(local_rank)
+    reps = Replicas("nccl", timeout_s=300, device_sync=torch.cuda.synchronize)
+    barrier, max_over_ranks = reps.barrier, reps.max
 
     n = args.n
     p, c = problems.kh(n, seed=rank)
@@ -368,8 +352,7 @@ def main_ours(args, rank, world, local_rank):
                "gpu_launches": launches, "kernel_shares": shares, "other_mode": other}
         print(json.dumps(out))
     sim.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    reps.close()
     return 0
 
 
