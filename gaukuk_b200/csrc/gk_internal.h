@@ -11,9 +11,20 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 
 namespace gk {
+
+// True the first time it is called for the current device with this mask:
+// kernel attributes (dynamic shared memory above 48 KB) are per device, so a
+// process that drives several GPUs sets them on each.
+inline bool first_on_device(std::atomic<unsigned long long>& mask) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    return (mask.fetch_or(bit) & bit) == 0;
+}
 
 // Device variable slots.
 enum Slot { S_DEN = 0, S_MTX = 1, S_MTY = 2, S_ENG = 3, S_MTZ = 4 };

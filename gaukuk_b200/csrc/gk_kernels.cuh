@@ -1099,12 +1099,10 @@ static void launch_stage2d_tma(const Ctx& c, const CUtensorMap& mc, const CUtens
     const int rows = c.h2d_rows;
     dim3 grid((g.nx + NT - 5) / (NT - 4), (g.ny + rows - 1) / rows);
     const size_t dyn = stage_dyn_bytes<NT, (KIND >= 1)>();
-    static bool attr_set = false;
-    if (!attr_set) {
+    static std::atomic<unsigned long long> attr_set{0};
+    if (gk::first_on_device(attr_set))
         cudaFuncSetAttribute(k_stage2d_tma<NT, KIND, PLM>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-        attr_set = true;
-    }
     k_stage2d_tma<NT, KIND, PLM><<<grid, NT, dyn, s>>>(mc, m0, out, g, c.ph, c1, c2, c3, c.tm, rows);
 }
 
@@ -1157,12 +1155,10 @@ static void launch_ens_stage_k(const gk::EnsInst* inst, const int2* tiles, int n
                                unsigned* counter, double c1, double c2, double c3, int ctas,
                                cudaStream_t s) {
     const size_t dyn = stage_dyn_bytes<NT, (KIND >= 1)>();
-    static bool attr_set = false;
-    if (!attr_set) {
+    static std::atomic<unsigned long long> attr_set{0};
+    if (gk::first_on_device(attr_set))
         cudaFuncSetAttribute(k_ens_stage<NT, KIND, PLM>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-        attr_set = true;
-    }
     k_ens_stage<NT, KIND, PLM><<<ctas, NT, dyn, s>>>(inst, tiles, ntiles, counter, c1, c2, c3);
 }
 

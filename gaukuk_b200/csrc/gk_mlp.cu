@@ -760,12 +760,10 @@ size_t flux_correct_smem() { return sizeof(InferShared); }
 void launch_flux_correct(const float* model, const double* W, double* F, const Geom& g,
                          const Phys& ph, const DevTime* tm, int dir, const FluxGate& gate,
                          unsigned* fired, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (gk::first_on_device(attr))
         cudaFuncSetAttribute(k_flux_correct, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(InferShared));
-        attr = true;
-    }
     const long long nf = dir == 0 ? (long long)(g.nx + 1) * g.ny : (long long)g.nx * (g.ny + 1);
     const long long tiles = (nf + 15) / 16;
     const int ctas = (int)((tiles + 3) / 4 < 148 * 8 ? (tiles + 3) / 4 : 148 * 8);
