@@ -11,6 +11,10 @@ computes the same initial state bits as the reference built with strict IEEE
 flags.  ``build_hook(path)`` builds a driver for any hook file written for
 the reference -- the hook's own ``#include "../sim.hpp"`` resolves to this
 layer's headers (``-I-`` stops the compiler from looking next to the hook).
+Where the reference's sources are present (``GK_REFERENCE_SRC``, default the
+reference checkout the oracle recipe also reads), its own setup files that
+need fixed boundaries and point masses are built as well, unchanged, as
+``bin/gaukuk_ref_<name>.sim``.
 """
 from __future__ import annotations
 
@@ -72,7 +76,15 @@ def build_hook(hook_src: str, name: Optional[str] = None, verbose: bool = False,
     return exe
 
 
+REFERENCE_SRC = os.environ.get("GK_REFERENCE_SRC", "/root/reference")
+REFERENCE_HOOKS = ("disk", "disk_planet")
+
+
 def build_host(verbose: bool = False, force: bool = False) -> None:
     build_host_lib(verbose=verbose, force=force)
     for hook in sorted(glob.glob(os.path.join(SETUP, "setup_*.cpp"))):
         build_hook(hook, verbose=verbose, force=force)
+    for name in REFERENCE_HOOKS:
+        src = os.path.join(REFERENCE_SRC, "src", "setup", f"setup_{name}.cpp")
+        if os.path.exists(src):
+            build_hook(src, name="ref_" + name, verbose=verbose, force=force)

@@ -116,6 +116,7 @@ struct gk_handle {
     bool tiling_set = false;  // gk_set_tiling overrides the default tiling
     float* model = nullptr;   // learned flux correction (device), or null
     gk::FluxGate gate;
+    double* fixed = nullptr;  // state at enrollment of fixed boundaries (device layout)
     unsigned* fired = nullptr;  // faces where the detector kept plain HLLC
     int tiling_rows = 0;
     cudaGraphExec_t gexec = nullptr;
@@ -182,6 +183,9 @@ int build_ctx(gk_handle* h) {
     if (gd.ny <= 1) g.dyRec = 0;
     if (gd.nz <= 1) g.dzRec = 0;
     g.drmin = smin(smin(g.dx, g.dy), g.dz);
+    g.xmin = gd.xmin;
+    g.ymin = gd.ymin;
+    g.zmin = gd.zmin;
     // EquationOfState (adiabatic.cpp:12-16), hllc.cpp:28-29
     ph.gamma = pd.gamma;
     ph.gm1 = pd.gamma - 1.0;
@@ -196,14 +200,16 @@ int build_ctx(gk_handle* h) {
     ph.integrator = pd.integrator == 1 ? 1 : (pd.integrator == 3 ? 3 : 2);
     ph.plm = pd.rc_order != 1;
     ph.stepmax = pd.stepmax;
-    // Boundary::Boundary (boundary.cpp:13-125): unknown ids copy; type 4 needs
-    // snapshot data this path does not carry.
+    // Boundary::Boundary (boundary.cpp:13-125): unknown ids copy; type 4
+    // (fixed) takes the data given by gk_set_fixed_boundary.
     for (int s = 0; s < 6; ++s) {
         int t = pd.bc[s];
-        if (t == GK_BC_FIXED) return fail(h, GK_ERR_UNSUPPORTED, "fixed (type 4) boundaries are not implemented on the device");
-        if (t < 0 || t > 3) t = 0;
+        if (t < 0 || t > 4) t = 0;
         ph.bc[s] = t;
     }
+    ph.fixed_bd = nullptr;
+    ph.fix_inner = 0;
+    ph.npoint = 0;
     ph.fill_z = 0;
     if (g.ndim == 3) {
         // z sides of type 0 run OutflowCopyYL/YR after the y fill
@@ -279,6 +285,16 @@ int stage_threads_default() {
 // many waves of CTAs, so no partial last wave dominates (measured on 4096^2:
 // 16-32 rows beat one wave of long segments by 1.5x); small grids use down
 // to 4 rows so that every SM gets work.  GK_STAGE_ROWS overrides (tuning).
+// The fused 2D path applies to 2D RK2/RK3 runs with MTZ identically zero,
+// no z gravity (it would make MTZ non-zero), no point masses (their kicks
+// run between the fused stages' CFL reduction and the epilogue) and no
+// learned correction.
+int choose_path(const gk_handle* h) {
+    const gk::Ctx& c = h->ctx;
+    return (c.g.ndim == 2 && !c.has_vz && c.ph.integrator != 1 && c.ph.grav[2] == 0 &&
+            c.ph.npoint == 0 && !h->model) ? 1 : 0;
+}
+
 int stage_rows(const gk::Geom& g) {
     int forced = env_int("GK_STAGE_ROWS", 0);
     if (forced > 0) return forced;
@@ -314,7 +330,7 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
     double* Cb = h->C;
     const int integ = c.ph.integrator;
     const double frac13 = 1.0 / 3.0;
-    if (c.ph.has_grav) GK_L(gk::K_KICK, k.kick(c, A, s));
+    if (c.ph.has_grav || c.ph.npoint) GK_L(gk::K_KICK, k.kick(c, A, 0, s));
     if (h->path == 1) {
         // the last stage also applies the second half kick, the CFL
         // reduction and the step epilogue
@@ -361,7 +377,7 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
             GK_L(gk::K_UPDATE, k.update(c, A, B, A, h->F1, h->F2, h->F3, 1, 0.5, 0.5, 0.5, s));
         }
     }
-    if (c.ph.has_grav) GK_L(gk::K_KICK, k.kick(c, A, s));
+    if (c.ph.has_grav || c.ph.npoint) GK_L(gk::K_KICK, k.kick(c, A, 1, s));
     GK_L(gk::K_CFL, k.cfl(c, A, 1, s));
 #undef GK_L
 }
@@ -397,9 +413,45 @@ int pull_time(gk_handle* h) {
     return GK_OK;
 }
 
+// A reference-layout host state (NVar x lenz x leny x lenx) into a device
+// state buffer (slots DEN, MTX, MTY, ENG, MTZ; stored planes; pitched rows).
+int copy_ref_to_device(gk_handle* h, const double* ref, double* dev) {
+    const gk::Geom& g = h->ctx.g;
+    for (int n = 0; n < 5; ++n) {
+        for (int kk = 0; kk < g.nzs; ++kk) {
+            const int k = g.kofs + kk;
+            const double* src = ref + ((size_t)(n * g.lenz + k) * g.leny) * g.lenx;
+            double* dst = dev + (size_t)kSlotOf[n] * g.vstride + (size_t)kk * g.kstride;
+            GK_CUDA(h, cudaMemcpy2DAsync(dst, sizeof(double) * g.pitch, src, sizeof(double) * g.lenx,
+                                         sizeof(double) * g.lenx, g.leny, cudaMemcpyHostToDevice,
+                                         h->stream));
+        }
+    }
+    return GK_OK;
+}
+
+// A change of the physics that kernels take by value: the captured graph
+// is rebuilt at the next launch, and the path follows.
+int physics_changed(gk_handle* h) {
+    if (h->ctx.ph.npoint) h->ctx.has_vz = 1;  // see gk_upload_cons
+    if (h->gexec) {
+        cudaGraphExecDestroy(h->gexec);
+        h->gexec = nullptr;
+        h->graph_steps = 0;
+    }
+    if (h->uploaded) {
+        h->path = choose_path(h);
+        if (h->path == 0) return alloc_generic(h);
+    }
+    return GK_OK;
+}
+
 int check_ready(gk_handle* h) {
     if (!h) return GK_ERR_INVALID;
     if (!h->uploaded) return fail(h, GK_ERR_STATE, "no state uploaded");
+    for (int s = 0; s < 6; ++s)
+        if (h->ctx.ph.bc[s] == 4 && !h->ctx.ph.fixed_bd)
+            return fail(h, GK_ERR_STATE, "fixed (type 4) boundary data not set (gk_set_fixed_boundary)");
     GK_CUDA(h, cudaSetDevice(h->device));
     return GK_OK;
 }
@@ -444,7 +496,7 @@ void gk_destroy(gk_handle* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
-    for (double* p : {h->A, h->B, h->C, h->W, h->F1, h->F2, h->F3, h->dlog}) cudaFree(p);
+    for (double* p : {h->A, h->B, h->C, h->W, h->F1, h->F2, h->F3, h->dlog, h->fixed}) cudaFree(p);
     cudaFree(h->model);
     cudaFree(h->fired);
     cudaFree(h->tm);
@@ -464,16 +516,8 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
     if (!h || !cons) return GK_ERR_INVALID;
     GK_CUDA(h, cudaSetDevice(h->device));
     const gk::Geom& g = h->ctx.g;
-    for (int n = 0; n < 5; ++n) {
-        for (int kk = 0; kk < g.nzs; ++kk) {
-            const int k = g.kofs + kk;
-            const double* src = cons + ((size_t)(n * g.lenz + k) * g.leny) * g.lenx;
-            double* dst = h->A + (size_t)kSlotOf[n] * g.vstride + (size_t)kk * g.kstride;
-            GK_CUDA(h, cudaMemcpy2DAsync(dst, sizeof(double) * g.pitch, src, sizeof(double) * g.lenx,
-                                         sizeof(double) * g.lenx, g.leny, cudaMemcpyHostToDevice,
-                                         h->stream));
-        }
-    }
+    int rc0 = copy_ref_to_device(h, cons, h->A);
+    if (rc0 != GK_OK) return rc0;
     // Path: the fused kernel evolves four variables; it applies when the run
     // is 2D and MTZ is zero on every active cell (it then stays zero).
     h->ctx.has_vz = 1;
@@ -485,9 +529,9 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
         GK_CUDA(h, cudaStreamSynchronize(h->stream));
         h->ctx.has_vz = flag;
     }
-    // (gz != 0 would make MTZ non-zero in the kick, so it also needs the generic path)
-    h->path = (g.ndim == 2 && !h->ctx.has_vz && h->ctx.ph.integrator != 1 &&
-               h->ctx.ph.grav[2] == 0 && !h->model) ? 1 : 0;
+    // a point mass off the mid-plane makes MTZ non-zero during the run
+    if (h->ctx.ph.npoint) h->ctx.has_vz = 1;
+    h->path = choose_path(h);
     h->ctx.h2d_rows = stage_rows(g);
     h->ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
     if (!h->tiling_set) h->ctx.stage_threads = stage_threads_default();
@@ -727,10 +771,11 @@ int gk_graph_info(gk_handle* h, int* steps_per_graph, int* launches_per_step) {
     const gk::Ctx& c = h->ctx;
     const int stages = c.ph.integrator;  // 1, 2 or 3 stages
     int per;
+    const int inner = c.ph.fix_inner ? 1 : 0;  // inner reset after each ghost fill
     if (h->path == 1) {
-        per = (c.ph.has_grav ? 1 : 0) + 2 * stages;  // kick, (ghost fill + stage) per stage
+        per = (c.ph.has_grav ? 1 : 0) + (2 + inner) * stages;  // kick, (ghost fill + stage) per stage
     } else {
-        per = (c.ph.has_grav ? 2 : 0) + stages * (3 + c.g.ndim) + 1;  // + CFL/epilogue
+        per = (c.ph.has_grav || c.ph.npoint ? 2 : 0) + stages * (3 + inner + c.g.ndim) + 1;
     }
     if (steps_per_graph) *steps_per_graph = steps_per_graph_of(c.g);
     if (launches_per_step) *launches_per_step = per;
@@ -975,7 +1020,7 @@ int gk_ens_create(gk_handle* const* handles, int n, gk_ensemble** out) {
     for (int i = 0; i < n; ++i) {
         gk_handle* h = handles[i];
         if (!h || !h->uploaded) return GK_ERR_STATE;
-        if (h->path != 1 || h->ctx.ph.integrator != 2) return GK_ERR_UNSUPPORTED;
+        if (h->path != 1 || h->ctx.ph.integrator != 2 || h->ctx.ph.fix_inner) return GK_ERR_UNSUPPORTED;
         if (h->ks != handles[0]->ks || h->device != handles[0]->device ||
             h->ctx.ph.plm != handles[0]->ctx.ph.plm)
             return GK_ERR_INVALID;
@@ -1182,6 +1227,44 @@ extern "C" int gk_tap_substeps(gk_handle* h, int nsub, double dt_sub, int ratio,
     return pull_time(h);
 }
 
+// ------------------------------------------------------------ fixed boundaries, point masses
+extern "C" int gk_set_fixed_boundary(gk_handle* h, const double* snapshot, int fix_inner) {
+    if (!h) return GK_ERR_INVALID;
+    GK_CUDA(h, cudaSetDevice(h->device));
+    gk::Phys& ph = h->ctx.ph;
+    const gk::Geom& g = h->ctx.g;
+    if (!snapshot) {
+        ph.fixed_bd = nullptr;
+        ph.fix_inner = 0;
+        return physics_changed(h);
+    }
+    if (!h->fixed) {
+        const size_t bytes = sizeof(double) * 5 * (size_t)g.vstride;
+        GK_CUDA(h, cudaMalloc(&h->fixed, bytes));
+        GK_CUDA(h, cudaMemsetAsync(h->fixed, 0, bytes, h->stream));
+    }
+    int rc = copy_ref_to_device(h, snapshot, h->fixed);
+    if (rc != GK_OK) return rc;
+    GK_CUDA(h, cudaStreamSynchronize(h->stream));
+    ph.fixed_bd = h->fixed;
+    ph.fix_inner = fix_inner ? 1 : 0;
+    // the index box of Boundary::FixedBDInner (fixed.cpp:182-185)
+    ph.inner[0] = static_cast<int>(g.ib + 0.25 * (g.ie - g.ib));
+    ph.inner[1] = static_cast<int>(g.ib + 0.75 * (g.ie - g.ib));
+    ph.inner[2] = static_cast<int>(g.jb + 0.25 * (g.je - g.jb));
+    ph.inner[3] = static_cast<int>(g.jb + 0.75 * (g.je - g.jb));
+    return physics_changed(h);
+}
+
+extern "C" int gk_set_point_gravity(gk_handle* h, int n, const double* params) {
+    if (!h || n < 0 || n > 2 || (n > 0 && !params)) return GK_ERR_INVALID;
+    gk::Phys& ph = h->ctx.ph;
+    ph.npoint = n;
+    for (int i = 0; i < 11; ++i) ph.pm[i] = 0.0;
+    for (int i = 0; i < (n == 2 ? 11 : (n == 1 ? 5 : 0)); ++i) ph.pm[i] = params[i];
+    return physics_changed(h);
+}
+
 // ------------------------------------------------------------ learned correction on a handle
 extern "C" int gk_set_flux_model(gk_handle* h, const float* model_host, int nmodel,
                                  float shock_jump, float pos_frac, float tv_min,
@@ -1210,8 +1293,7 @@ extern "C" int gk_set_flux_model(gk_handle* h, const float* model_host, int nmod
     // the path and the graph follow the model
     if (h->uploaded) {
         const gk::Geom& g = h->ctx.g;
-        h->path = (g.ndim == 2 && !h->ctx.has_vz && h->ctx.ph.integrator != 1 &&
-                   h->ctx.ph.grav[2] == 0 && !h->model) ? 1 : 0;
+        h->path = choose_path(h);
         if (h->path == 0) {
             int rc = alloc_generic(h);
             if (rc != GK_OK) return rc;

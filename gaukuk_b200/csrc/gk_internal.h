@@ -45,6 +45,7 @@ struct Geom {
     int fpitch;
     long long fkstride, fvstride;
     double dx, dy, dz, dxRec, dyRec, dzRec, drmin;
+    double xmin, ymin, zmin;  // cell centres: xmin - ng*dx + 0.5*dx + i*dx (sim.cpp:36-41)
 };
 
 struct Phys {
@@ -57,6 +58,16 @@ struct Phys {
     int bc[6];        // effective ghost-fill type per side (after the z->y copy mapping)
     int fill_z;       // 3D only: whether z sides are filled (per side bit 0/1)
     int stepmax;
+    // Fixed (type 4) sides and the inner reset (fixed.cpp): the state at
+    // enrollment in device layout (null when none), and the index box
+    // [inner[0], inner[1]) x [inner[2], inner[3]) of FixedBDInner.
+    const double* fixed_bd;
+    int fix_inner;
+    int inner[4];
+    // Point masses (point_gravity.cpp, binary_gravity.cpp): npoint 0, 1 or
+    // 2; pm = gm0, x0, y0, z0, rs0, gm1, z1, rs1, omega, ab, theta1.
+    int npoint;
+    double pm[11];
 };
 
 // Device-resident clock of Sim::Advance (sim.cpp:69-117).  Written by the
@@ -146,7 +157,7 @@ static const char* const kClassNames[K_NCLASS] = {
     void launch_update(const gk::Ctx& c, const double* u0, const double* uc, double* out,      \
                        const double* F1, const double* F2, const double* F3, int three,        \
                        double c1, double c2, double c3, cudaStream_t s);                       \
-    void launch_kick(const gk::Ctx& c, double* u, cudaStream_t s);                             \
+    void launch_kick(const gk::Ctx& c, double* u, int which, cudaStream_t s);                  \
     void launch_cfl(const gk::Ctx& c, const double* u, int epilogue, cudaStream_t s);          \
     void launch_stage2d(const gk::Ctx& c, const double* uc, const double* u0, double* out,     \
                         int kind, double c1, double c2, double c3, cudaStream_t s);            \

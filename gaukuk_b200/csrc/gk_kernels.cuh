@@ -75,6 +75,12 @@ __device__ __forceinline__ void bc_fill_one(double* __restrict__ u, const Geom& 
     else if (dir == 1) { cj = gc; sj = sc; ci = si = g.ib + a; ck = sk = g.kb + b; }
     else { ck = gc; sk = sc; ci = si = g.ib + a; cj = sj = g.jb + b; }
     const long long dst = sidx(g, ck, cj, ci), src = sidx(g, sk, sj, si);
+    if (type == 4) {
+        // FixedBD* (fixed.cpp:16-176): the ghost keeps its value at enrollment
+#pragma unroll
+        for (int v = 0; v < 5; ++v) u[v * g.vstride + dst] = ph.fixed_bd[v * g.vstride + dst];
+        return;
+    }
     double q[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) q[v] = u[v * g.vstride + src];
@@ -111,6 +117,30 @@ __global__ void k_bc(double* __restrict__ u, Geom g, Phys ph, const DevTime* __r
     const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= count) return;
     bc_fill_one(u, g, ph, dir, side, id);
+}
+
+// Cell centres in Domain's order of operations (sim.cpp:36-41).
+__device__ __forceinline__ double centre(double lo, int ng, double d, int i) {
+    return lo - ng * d + 0.5 * d + i * d;
+}
+
+// Boundary::FixedBDInner (fixed.cpp:180-206): inside the index box, cells
+// with x^2 + y^2 + z^2 < 0.5^2 get back their values at enrollment; run
+// after the sides (boundary.cpp:127-142).
+__global__ void k_fix_inner(double* __restrict__ u, Geom g, Phys ph, const DevTime* __restrict__ tm) {
+    if (!tm->active) return;
+    const int i = ph.inner[0] + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = ph.inner[2] + blockIdx.y;
+    const int k = g.kb + blockIdx.z;
+    if (i >= ph.inner[1]) return;
+    const double x = centre(g.xmin, g.ng, g.dx, i);
+    const double y = centre(g.ymin, g.ng, g.dy, j);
+    const double z = centre(g.zmin, g.ng, g.dz, k);
+    const double r2 = x * x + y * y + z * z;
+    if (!(r2 < 0.5 * 0.5)) return;
+    const long long c = sidx(g, k, j, i);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) u[v * g.vstride + c] = ph.fixed_bd[v * g.vstride + c];
 }
 
 // ------------------------------------------------------------ ConsToPrim
@@ -274,7 +304,13 @@ __global__ void k_update(const double* u0, const double* uc, double* out,
 // ------------------------------------------------------------ gravity kick
 // SourceTerm::ConstGravity (const_gravity.cpp:10-69) with dt/2, applied
 // before and after the integrator (sim.cpp:85-91): E += m*g*dt; m += rho*g*dt.
-__global__ void k_kick(double* __restrict__ u, Geom g, Phys ph, const DevTime* __restrict__ tm) {
+// SourceTerm::UpdateSource (source.cpp:12-21) for one half step dt/2 of
+// the Strang splitting (sim.cpp:85-91): constant gravity, then one point
+// mass (point_gravity.cpp:11-92) or two (binary_gravity.cpp), whose second
+// mass orbits at angle omega*t + theta1 with t = t_n + dt/2 for the first
+// half kick (which = 0) and t_n + dt for the second (which = 1).
+__global__ void k_kick(double* __restrict__ u, Geom g, Phys ph, const DevTime* __restrict__ tm,
+                       int which) {
     if (!tm->active) return;
     const int i = g.ib + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = g.jb + blockIdx.y;
@@ -292,6 +328,44 @@ __global__ void k_kick(double* __restrict__ u, Geom g, Phys ph, const DevTime* _
         E += m * gd * hdt;
         m += u[gk::S_DEN * g.vstride + c] * gd * hdt;
     }
+    if (ph.npoint == 0) return;
+    const double xnow = centre(g.xmin, g.ng, g.dx, i);
+    const double ynow = centre(g.ymin, g.ng, g.dy, j);
+    const double znow = centre(g.zmin, g.ng, g.dz, k);
+    double gxdt, gydt, gzdt;
+    {
+        const double delx = xnow - ph.pm[1], dely = ynow - ph.pm[2], delz = znow - ph.pm[3];
+        const double r2 = delx * delx + dely * dely + delz * delz;
+        const double rs = ph.pm[4];
+        const double rInv = 1.0 / sqrt(r2 + rs * rs);
+        const double gv = -(ph.pm[0] * hdt) * rInv * rInv * rInv;
+        gxdt = gv * delx;
+        gydt = gv * dely;
+        gzdt = gv * delz;
+        if (ph.npoint == 2) {
+            const double t = which == 0 ? tm->t + 0.5 * tm->dt : tm->t + tm->dt;
+            const double theta = ph.pm[8] * t + ph.pm[10];
+            const double x1 = ph.pm[9] * cos(theta), y1 = ph.pm[9] * sin(theta), z1 = ph.pm[6];
+            const double dx1 = xnow - x1, dy1 = ynow - y1, dz1 = znow - z1;
+            const double r1 = dx1 * dx1 + dy1 * dy1 + dz1 * dz1;
+            const double rs1 = ph.pm[7];
+            const double r1Inv = 1.0 / sqrt(r1 + rs1 * rs1);
+            const double g1 = -(ph.pm[5] * hdt) * r1Inv * r1Inv * r1Inv;
+            const double gInd = 0.0;  // the indirect term, zeroed in binary_gravity.cpp
+            gxdt = gv * delx + g1 * dx1 + gInd * x1;
+            gydt = gv * dely + g1 * dy1 + gInd * y1;
+            gzdt = gv * delz + g1 * dz1 + gInd * z1;
+        }
+    }
+    double& D = u[gk::S_DEN * g.vstride + c];
+    double& E = u[gk::S_ENG * g.vstride + c];
+    double& MX = u[gk::S_MTX * g.vstride + c];
+    double& MY = u[gk::S_MTY * g.vstride + c];
+    double& MZ = u[gk::S_MTZ * g.vstride + c];
+    E += MX * gxdt + MY * gydt + MZ * gzdt;
+    MX += D * gxdt;
+    MY += D * gydt;
+    MZ += D * gzdt;
 }
 
 // ------------------------------------------------------------ CFL + epilogue
@@ -1054,6 +1128,10 @@ void launch_bc(const Ctx& c, double* u, cudaStream_t s) {
     const int sides = (g.nz > 1 && c.ph.fill_z) ? 6 : 4;
     dim3 grid((unsigned)((m + 127) / 128), sides);
     k_bc<<<grid, 128, 0, s>>>(u, g, c.ph, c.tm);
+    if (c.ph.fix_inner && c.ph.inner[1] > c.ph.inner[0] && c.ph.inner[3] > c.ph.inner[2]) {
+        dim3 gi((c.ph.inner[1] - c.ph.inner[0] + 127) / 128, c.ph.inner[3] - c.ph.inner[2], g.nz);
+        k_fix_inner<<<gi, 128, 0, s>>>(u, g, c.ph, c.tm);
+    }
 }
 
 void launch_c2p(const Ctx& c, const double* u, double* w, cudaStream_t s) {
@@ -1078,8 +1156,8 @@ void launch_update(const Ctx& c, const double* u0, const double* uc, double* out
                                                  c3, c.tm);
 }
 
-void launch_kick(const Ctx& c, double* u, cudaStream_t s) {
-    k_kick<<<cell_grid(c.g, 128), 128, 0, s>>>(u, c.g, c.ph, c.tm);
+void launch_kick(const Ctx& c, double* u, int which, cudaStream_t s) {
+    k_kick<<<cell_grid(c.g, 128), 128, 0, s>>>(u, c.g, c.ph, c.tm, which);
 }
 
 void launch_cfl(const Ctx& c, const double* u, int epilogue, cudaStream_t s) {

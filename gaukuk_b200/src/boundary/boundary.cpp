@@ -72,9 +72,25 @@ Boundary::Boundary() {
         int type = static_cast<int>(Config::getInstance().get(keys[s]));
         types_[s] = type;
         if (type == 4) {
-            fixed_ = true;
-            *fn[s] = [](TArray<Real>&, const Grid&, const EquationOfState&) {
-                throw std::runtime_error("fixed (type 4) boundary data are not available");
+            // FixedBD* (fixed.cpp:16-176): ghosts of the side's active
+            // rows/columns from the state at enrollment, same index
+            int dir = s / 2;
+            const int side = s % 2;
+            *fn[s] = [this, dir, side](TArray<Real>& u, const Grid& g, const EquationOfState&) {
+                if (!fixedEnrolled_)
+                    throw std::invalid_argument(
+                        "fixed boundary is not initialized. call "
+                        "'Boundary::EnrollFixedBoundaryData(const TArray<Real>& cons, const Grid& "
+                        "grid)' in your setup");
+                const int len[3] = {g.lenx, g.leny, g.lenz};
+                const int n[3] = {g.nx, g.ny, g.nz};
+                int lo[3] = {g.ib, g.jb, g.kb}, hi[3] = {g.ie, g.je, g.ke};
+                lo[dir] = side == 0 ? 0 : g.nGhost + n[dir];
+                hi[dir] = side == 0 ? g.nGhost : len[dir];
+                for (int v = DEN; v <= ENG; v++)
+                    for (int k = lo[2]; k < hi[2]; k++)
+                        for (int j = lo[1]; j < hi[1]; j++)
+                            for (int i = lo[0]; i < hi[0]; i++) u(v, k, j, i) = fixedData_(v, k, j, i);
             };
             continue;
         }
@@ -89,7 +105,7 @@ Boundary::Boundary() {
     if (Config::getInstance().get("enableImmersed", 0) != 0) immersed_ = true;
 }
 
-void Boundary::UpdateBD(TArray<Real>& cons, const Grid& grid, const Domain&,
+void Boundary::UpdateBD(TArray<Real>& cons, const Grid& grid, const Domain& domain,
                         const EquationOfState& eos) {
     Bdxl(cons, grid, eos);
     Bdxr(cons, grid, eos);
@@ -100,17 +116,40 @@ void Boundary::UpdateBD(TArray<Real>& cons, const Grid& grid, const Domain&,
         Bdzr(cons, grid, eos);
     }
     if (immersed_) throw std::runtime_error("immersed boundaries are not available");
+    if (fixInner_) FixedInner(cons, grid, domain);
+}
+
+// Boundary::FixedBDInner (fixed.cpp:180-206).
+void Boundary::FixedInner(TArray<Real>& cons, const Grid& grid, const Domain& domain) const {
+    const int il = static_cast<int>(grid.ib + 0.25 * (grid.ie - grid.ib));
+    const int ir = static_cast<int>(grid.ib + 0.75 * (grid.ie - grid.ib));
+    const int jl = static_cast<int>(grid.jb + 0.25 * (grid.je - grid.jb));
+    const int jr = static_cast<int>(grid.jb + 0.75 * (grid.je - grid.jb));
+    for (int v = DEN; v <= ENG; ++v)
+        for (int k = grid.kb; k < grid.ke; ++k)
+            for (int j = jl; j < jr; ++j)
+                for (int i = il; i < ir; ++i) {
+                    const Real x = domain.xc(i), y = domain.yc(j), z = domain.zc(k);
+                    const Real r2 = x * x + y * y + z * z;
+                    if (r2 < 0.5 * 0.5) cons(v, k, j, i) = fixedData_(v, k, j, i);
+                }
 }
 
 void Boundary::SetupImmersedShell(const Grid&, const Domain&, Real, Real, Real, Real) {
     immersed_ = true;
 }
 
-void Boundary::EnrollFixedBoundaryData(const TArray<Real>&, const Grid&, bool) { fixed_ = true; }
+// Boundary::EnrollFixedBoundaryData (fixed.cpp:226-268): the sides read the
+// state as it is now; every side reads the same index it fills, so one copy
+// of the whole state serves all sides and the inner reset.
+void Boundary::EnrollFixedBoundaryData(const TArray<Real>& cons, const Grid&, bool fixInner) {
+    fixedEnrolled_ = true;
+    fixedData_ = cons;
+    if (fixInner) fixInner_ = true;
+}
 
 const char* Boundary::DeviceBlocker() const {
     if (custom_) return "self-defined boundary routines run on the host only";
-    if (fixed_) return "fixed (type 4) boundaries are not implemented on the device";
     if (immersed_) return "immersed boundaries are not implemented on the device";
     return "";
 }

@@ -2,12 +2,13 @@
 //
 // Interface of the reference's Boundary (src/boundary/boundary.hpp:15-111):
 // one std::function per side chosen from xleft..zright (0 copy, 1 periodic,
-// 2 reflective, 3 outflow), UpdateBD, and the Enroll* hooks with which a
-// setup file installs its own static SelfDefineBD* routines.  The host fill
-// is used for the state a setup hook produces (main.cpp:30) and for output;
-// during Sim::Advance the device fills ghosts with the same rules.  Problems
-// that enroll their own routines, fixed (type 4) data or an immersed body
-// run on the host only and Sim::Advance rejects them.
+// 2 reflective, 3 outflow, 4 fixed), UpdateBD, and the Enroll* hooks with
+// which a setup file installs its own static SelfDefineBD* routines or the
+// fixed-boundary data.  The host fill is used for the state a setup hook
+// produces (main.cpp:30) and for output; during Sim::Advance the device fills
+// ghosts with the same rules, fixed sides and the inner reset included.
+// Problems that enroll their own routines or an immersed body run on the
+// host only and Sim::Advance rejects them.
 #pragma once
 
 #include <functional>
@@ -41,6 +42,10 @@ public:
 
     // The configured type of side s (xleft, xright, yleft, yright, zleft, zright).
     int Type(int s) const { return types_[s]; }
+    // The state at EnrollFixedBoundaryData (empty when not enrolled).
+    const TArray<Real>& FixedData() const { return fixedData_; }
+    bool HasFixedData() const { return fixedEnrolled_; }
+    bool FixInner() const { return fixInner_; }
     // Why the device path cannot take this configuration ("" when it can).
     const char* DeviceBlocker() const;
 
@@ -54,7 +59,10 @@ private:
 
     int types_[6] = {0, 0, 0, 0, 0, 0};
     int custom_ = 0;
-    bool fixed_ = false, immersed_ = false;
+    bool immersed_ = false;
+    bool fixedEnrolled_ = false, fixInner_ = false;
+    TArray<Real> fixedData_;
+    void FixedInner(TArray<Real>& cons, const Grid& grid, const Domain& domain) const;
 };
 
 }  // namespace Gaukuk

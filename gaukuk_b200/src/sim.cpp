@@ -75,8 +75,6 @@ void Sim::EnsureDevice() {
     if (dev_) return;
     const char* why = boundary.DeviceBlocker();
     if (*why) throw std::runtime_error(why);
-    if (srcTerm.HasPointGravity())
-        throw std::runtime_error("point/binary gravity is not implemented on the device");
     gk_grid_desc gd{};
     gd.nx = grid.nx; gd.ny = grid.ny; gd.nz = grid.nz; gd.nghost = grid.nGhost;
     gd.xmin = domain.xmin; gd.xmax = domain.xmax;
@@ -97,6 +95,54 @@ void Sim::EnsureDevice() {
     pd.mode = gpuMode_ == 1 ? GK_MODE_FAST : GK_MODE_PARITY;
     pd.device = gpuDevice_;
     Check(nullptr, gk_create(&gd, &pd, &dev_), "gk_create");
+    if (boundary.HasFixedData())
+        Check(dev_, gk_set_fixed_boundary(dev_, boundary.FixedData().data(), boundary.FixInner()),
+              "gk_set_fixed_boundary");
+    double pm[11];
+    const int npoint = srcTerm.PointParams(pm);
+    if (npoint > 0) Check(dev_, gk_set_point_gravity(dev_, npoint, pm), "gk_set_point_gravity");
+}
+
+// The reference's integrators end with cons.Swap(consTemp) (rk2.cpp:21,
+// rk3.cpp:27), so its two arrays alternate as the state.  A cell that no
+// ghost fill and no update ever writes keeps each array's own value: the
+// setup's in cons, zero in consTemp (zero-initialised, sim.cpp:45-67), and
+// the written state shows one or the other with the parity of the step
+// count.  These cells: in the stored planes (all in 3D, the active one in
+// 1D/2D), ghost in two or more directions, or ghost in a direction that is
+// not filled (one cell wide, or a 3D z side of type 0, whose fill goes to the
+// y ghosts, boundary.cpp:92-121).
+void Sim::SwapUnwritten() {
+    if (integratorType == 1) return;  // forward Euler updates in place
+    if (unwritten_.empty() && spare_.empty()) {
+        const int n[3] = {grid.nx, grid.ny, grid.nz};
+        bool filled[3][2];
+        for (int d = 0; d < 3; ++d)
+            for (int s = 0; s < 2; ++s) filled[d][s] = n[d] > 1;
+        if (grid.nz > 1)
+            for (int s = 0; s < 2; ++s) filled[2][s] = boundary.Type(4 + s) != 0;
+        const int k0 = grid.nz > 1 ? 0 : grid.kb, k1 = grid.nz > 1 ? grid.lenz : grid.ke;
+        const int lo[3] = {grid.ib, grid.jb, grid.kb}, hi[3] = {grid.ie, grid.je, grid.ke};
+        for (int v = 0; v < NVar; ++v)
+            for (int k = k0; k < k1; ++k)
+                for (int j = 0; j < grid.leny; ++j)
+                    for (int i = 0; i < grid.lenx; ++i) {
+                        const int c[3] = {i, j, k};
+                        int ghosts = 0, gdir = -1, gside = 0;
+                        for (int d = 0; d < 3; ++d)
+                            if (c[d] < lo[d] || c[d] >= hi[d]) {
+                                ++ghosts;
+                                gdir = d;
+                                gside = c[d] < lo[d] ? 0 : 1;
+                            }
+                        if (ghosts == 0) continue;
+                        if (ghosts == 1 && filled[gdir][gside]) continue;
+                        unwritten_.push_back(&cons(v, k, j, i) - cons.data());
+                    }
+        spare_.assign(unwritten_.size(), 0.0);
+    }
+    Real* u = cons.data();
+    for (size_t q = 0; q < unwritten_.size(); ++q) std::swap(u[unwritten_[q]], spare_[q]);
 }
 
 void Sim::Advance(Real dtoutput) {
@@ -120,6 +166,7 @@ void Sim::Advance(Real dtoutput) {
     }
     Check(dev_, rc, "gk_advance");
     Check(dev_, gk_download_cons(dev_, cons.data()), "gk_download_cons");
+    if ((st - step0) % 2 != 0) SwapUnwritten();
     double tdev = 0, dtdev = 0;
     int sdev = 0, cdev = 1;
     Check(dev_, gk_get_time(dev_, &tdev, &dtdev, &sdev, &cdev), "gk_get_time");

@@ -22,6 +22,9 @@
 #include "source_term/source.hpp"
 #include "template_array.hpp"
 
+#include <cstddef>
+#include <vector>
+
 struct gk_handle;
 
 namespace Gaukuk {
@@ -67,6 +70,11 @@ private:
     int gpuMode_, gpuDevice_;
     gk_handle* dev_ = nullptr;
     void EnsureDevice();
+    // Cells that no ghost fill or update writes (corner and edge ghosts,
+    // ghost rows of unused directions) and consTemp's values of them.
+    std::vector<size_t> unwritten_;
+    std::vector<Real> spare_;
+    void SwapUnwritten();
 };
 
 }  // namespace Gaukuk

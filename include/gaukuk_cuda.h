@@ -83,6 +83,25 @@ int gk_create(const gk_grid_desc* grid, const gk_phys_desc* phys, gk_handle** ou
 /* Releases the handle, its stream, graphs and device memory. */
 void gk_destroy(gk_handle* h);
 
+/* Fixed (type 4) boundaries: Boundary::EnrollFixedBoundaryData
+ * (fixed.cpp:226-268) and FixedBD* (fixed.cpp:16-176).  `snapshot` is the
+ * reference-layout state at enrollment; every ghost cell of a type-4 side
+ * then gets its value from it at each ghost fill.  fix_inner != 0 also runs
+ * Boundary::FixedBDInner (fixed.cpp:180-206) after the sides: in the central
+ * index box, cells with x^2 + y^2 + z^2 < 0.25 get back their snapshot
+ * values.  NULL removes the data.  A run with a type-4 side refuses to
+ * advance until the data are set. */
+int gk_set_fixed_boundary(gk_handle* h, const double* snapshot, int fix_inner);
+
+/* Point masses: SourceTerm::EnrollPointGravity (source.cpp:33-68) as the
+ * Strang half kicks of PointGravity (point_gravity.cpp:11-92, n = 1) or
+ * BinaryGravity (binary_gravity.cpp, n = 2), after the constant gravity.
+ * params: gm0, x0, y0, z0, rs0 (n = 1); then gm1, z1, rs1, omega, ab,
+ * theta1 (n = 2; the second mass sits at ab (cos, sin)(omega t + theta1), z1),
+ * with omega, ab and theta1 as EnrollPointGravity computes them.  n = 0
+ * removes them.  Runs with point masses take the generic path. */
+int gk_set_point_gravity(gk_handle* h, int n, const double* params);
+
 /* Number of doubles in one reference-layout state: 5*lenz*leny*lenx. */
 long long gk_state_size(const gk_handle* h);
 
