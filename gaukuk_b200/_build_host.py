@@ -13,7 +13,7 @@ the reference -- the hook's own ``#include "../sim.hpp"`` resolves to this
 layer's headers (``-I-`` stops the compiler from looking next to the hook).
 Where the reference's sources are present (``GK_REFERENCE_SRC``, default the
 reference checkout the oracle recipe also reads), its own setup files that
-need fixed boundaries and point masses are built as well, unchanged, as
+run on the device path are built as well, unchanged, as
 ``bin/gaukuk_ref_<name>.sim``.
 """
 from __future__ import annotations
@@ -77,7 +77,7 @@ def build_hook(hook_src: str, name: Optional[str] = None, verbose: bool = False,
 
 
 REFERENCE_SRC = os.environ.get("GK_REFERENCE_SRC", "/root/reference")
-REFERENCE_HOOKS = ("disk", "disk_planet")
+REFERENCE_HOOKS = ("blast", "disk", "disk_planet", "example", "kh", "rt", "shock_tube", "wave_test")
 
 
 def build_host(verbose: bool = False, force: bool = False) -> None:
