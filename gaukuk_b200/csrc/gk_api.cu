@@ -69,6 +69,8 @@ struct KernelSet {
     decltype(&gk_parity::launch_ens_stage) ens_stage;
     decltype(&gk_parity::launch_ens_bc) ens_bc;
     decltype(&gk_parity::launch_ens_begin) ens_begin;
+    decltype(&gk_parity::launch_zflux) zflux;
+    decltype(&gk_parity::launch_stage3d) stage3d;
 };
 
 const KernelSet kParity = {gk_parity::launch_bc,     gk_parity::launch_c2p,
@@ -76,11 +78,13 @@ const KernelSet kParity = {gk_parity::launch_bc,     gk_parity::launch_c2p,
                            gk_parity::launch_kick,   gk_parity::launch_cfl,
                            gk_parity::launch_stage2d, gk_parity::launch_begin,
                            gk_parity::launch_mtz_check, gk_parity::launch_ens_stage,
-                           gk_parity::launch_ens_bc,  gk_parity::launch_ens_begin};
+                           gk_parity::launch_ens_bc,  gk_parity::launch_ens_begin,
+                           gk_parity::launch_zflux,   gk_parity::launch_stage3d};
 const KernelSet kFast = {gk_fast::launch_bc,     gk_fast::launch_c2p,     gk_fast::launch_flux,
                          gk_fast::launch_update, gk_fast::launch_kick,    gk_fast::launch_cfl,
                          gk_fast::launch_stage2d, gk_fast::launch_begin,  gk_fast::launch_mtz_check,
-                         gk_fast::launch_ens_stage, gk_fast::launch_ens_bc, gk_fast::launch_ens_begin};
+                         gk_fast::launch_ens_stage, gk_fast::launch_ens_bc, gk_fast::launch_ens_begin,
+                         gk_fast::launch_zflux, gk_fast::launch_stage3d};
 
 constexpr int kLogCap = 1 << 20;
 
@@ -285,12 +289,15 @@ int stage_threads_default() {
 // many waves of CTAs, so no partial last wave dominates (measured on 4096^2:
 // 16-32 rows beat one wave of long segments by 1.5x); small grids use down
 // to 4 rows so that every SM gets work.  GK_STAGE_ROWS overrides (tuning).
-// The fused 2D path applies to 2D RK2/RK3 runs with MTZ identically zero,
-// no z gravity (it would make MTZ non-zero), no point masses (their kicks
-// run between the fused stages' CFL reduction and the epilogue) and no
-// learned correction.
+// Path 1, the fused 2D stage, applies to 2D RK2/RK3 runs with MTZ
+// identically zero, no z gravity (it would make MTZ non-zero), no point
+// masses (their kicks run between the fused stages' CFL reduction and the
+// epilogue) and no learned correction.  Path 2, the 3D stage (z fluxes, then
+// one fused x-y stage per plane), applies to 3D RK2/RK3 runs (forward Euler
+// updates in place, which the fused stage cannot).  Path 0 is generic.
 int choose_path(const gk_handle* h) {
     const gk::Ctx& c = h->ctx;
+    if (c.g.ndim == 3 && c.ph.integrator != 1 && env_int("GK_STAGE3D", 1) != 0) return 2;
     return (c.g.ndim == 2 && !c.has_vz && c.ph.integrator != 1 && c.ph.grav[2] == 0 &&
             c.ph.npoint == 0 && !h->model) ? 1 : 0;
 }
@@ -331,6 +338,25 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
     const int integ = c.ph.integrator;
     const double frac13 = 1.0 / 3.0;
     if (c.ph.has_grav || c.ph.npoint) GK_L(gk::K_KICK, k.kick(c, A, 0, s));
+    if (h->path == 2) {
+        // z fluxes of the stage's state into F3, then the fused x-y stage
+        GK_L(gk::K_BC, k.bc(c, A, s));
+        GK_L(gk::K_FLUX, k.zflux(c, A, h->F3, s));
+        GK_L(gk::K_STAGE, k.stage3d(c, A, nullptr, B, h->F3, 0, 1.0, 1.0, 0.0, s));
+        GK_L(gk::K_BC, k.bc(c, B, s));
+        GK_L(gk::K_FLUX, k.zflux(c, B, h->F3, s));
+        if (integ == 3) {
+            GK_L(gk::K_STAGE, k.stage3d(c, B, A, Cb, h->F3, 1, 0.75, 0.25, 0.25, s));
+            GK_L(gk::K_BC, k.bc(c, Cb, s));
+            GK_L(gk::K_FLUX, k.zflux(c, Cb, h->F3, s));
+            GK_L(gk::K_STAGE, k.stage3d(c, Cb, A, A, h->F3, 1, frac13, 2 * frac13, 2 * frac13, s));
+        } else {
+            GK_L(gk::K_STAGE, k.stage3d(c, B, A, A, h->F3, 1, 0.5, 0.5, 0.5, s));
+        }
+        if (c.ph.has_grav || c.ph.npoint) GK_L(gk::K_KICK, k.kick(c, A, 1, s));
+        GK_L(gk::K_CFL, k.cfl(c, A, 1, s));
+        return;
+    }
     if (h->path == 1) {
         // the last stage also applies the second half kick, the CFL
         // reduction and the step epilogue
@@ -441,7 +467,7 @@ int physics_changed(gk_handle* h) {
     }
     if (h->uploaded) {
         h->path = choose_path(h);
-        if (h->path == 0) return alloc_generic(h);
+        if (h->path != 1) return alloc_generic(h);
     }
     return GK_OK;
 }
@@ -536,7 +562,7 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
     h->ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
     if (!h->tiling_set) h->ctx.stage_threads = stage_threads_default();
     else h->ctx.h2d_rows = h->tiling_rows;
-    if (h->path == 0) {
+    if (h->path != 1) {
         int rc = alloc_generic(h);
         if (rc != GK_OK) return rc;
     }
@@ -587,7 +613,7 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
     // and 1D y rows follow the reference's in-place order, so both keep A's.
     const double* donor = nullptr;
     if (h->htm->step > h->upload_step && h->ctx.ph.integrator != 1)
-        donor = (h->path == 1 && h->ctx.ph.integrator == 3) ? h->C : h->B;
+        donor = (h->path >= 1 && h->ctx.ph.integrator == 3) ? h->C : h->B;
     if (donor) {
         const size_t rowb = sizeof(double) * g.lenx, prow = sizeof(double) * g.pitch;
         for (int n = 0; n < 5; ++n) {
@@ -774,6 +800,8 @@ int gk_graph_info(gk_handle* h, int* steps_per_graph, int* launches_per_step) {
     const int inner = c.ph.fix_inner ? 1 : 0;  // inner reset after each ghost fill
     if (h->path == 1) {
         per = (c.ph.has_grav ? 1 : 0) + (2 + inner) * stages;  // kick, (ghost fill + stage) per stage
+    } else if (h->path == 2) {
+        per = (c.ph.has_grav || c.ph.npoint ? 2 : 0) + (3 + inner) * stages + 1;
     } else {
         per = (c.ph.has_grav || c.ph.npoint ? 2 : 0) + stages * (3 + inner + c.g.ndim) + 1;
     }
@@ -1294,7 +1322,7 @@ extern "C" int gk_set_flux_model(gk_handle* h, const float* model_host, int nmod
     if (h->uploaded) {
         const gk::Geom& g = h->ctx.g;
         h->path = choose_path(h);
-        if (h->path == 0) {
+        if (h->path != 1) {
             int rc = alloc_generic(h);
             if (rc != GK_OK) return rc;
         }

@@ -158,6 +158,10 @@ static const char* const kClassNames[K_NCLASS] = {
                        const double* F1, const double* F2, const double* F3, int three,        \
                        double c1, double c2, double c3, cudaStream_t s);                       \
     void launch_kick(const gk::Ctx& c, double* u, int which, cudaStream_t s);                  \
+    void launch_zflux(const gk::Ctx& c, const double* u, double* F3, cudaStream_t s);          \
+    void launch_stage3d(const gk::Ctx& c, const double* uc, const double* u0, double* out,     \
+                        const double* F3, int three, double c1, double c2, double c3,          \
+                        cudaStream_t s);                                                       \
     void launch_cfl(const gk::Ctx& c, const double* u, int epilogue, cudaStream_t s);          \
     void launch_stage2d(const gk::Ctx& c, const double* uc, const double* u0, double* out,     \
                         int kind, double c1, double c2, double c3, cudaStream_t s);            \

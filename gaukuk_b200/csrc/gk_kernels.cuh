@@ -1113,6 +1113,8 @@ __global__ void k_ens_begin(const gk::EnsInst* __restrict__ inst, int n, double 
 }
 
 // ------------------------------------------------------------ launchers
+#include "gk_stage3d.cuh"
+
 static inline dim3 cell_grid(const Geom& g, int threads) {
     return dim3((g.nx + threads - 1) / threads, g.ny, g.nz);
 }
@@ -1154,6 +1156,58 @@ void launch_update(const Ctx& c, const double* u0, const double* uc, double* out
                    double c2, double c3, cudaStream_t s) {
     k_update<<<cell_grid(c.g, 128), 128, 0, s>>>(u0, uc, out, F1, F2, F3, c.g, c.ph, three, c1, c2,
                                                  c3, c.tm);
+}
+
+// 3D stage: rows per CTA segment and the CTA width (64, 96 or 128 threads,
+// whichever wastes the fewest lanes on the last strip of columns).
+static inline int stage3d_rows(const Geom& g) { return g.ny < 16 ? g.ny : 16; }
+static inline int stage3d_nt(const Geom& g) {
+    int best = 128;
+    long long best_lanes = 1LL << 62;
+    for (int nt : {128, 96, 64}) {
+        const long long lanes = (long long)((g.nx + nt - 5) / (nt - 4)) * nt;
+        if (lanes < best_lanes) {
+            best_lanes = lanes;
+            best = nt;
+        }
+    }
+    return best;
+}
+
+void launch_zflux(const Ctx& c, const double* u, double* F3, cudaStream_t s) {
+    const Geom& g = c.g;
+    const int rows = stage3d_rows(g);
+    dim3 grid((g.nx + 127) / 128, (g.ny + rows - 1) / rows, g.nz + 1);
+    if (c.ph.plm) k_zflux<true><<<grid, 128, 0, s>>>(u, F3, g, c.ph, c.tm, rows);
+    else k_zflux<false><<<grid, 128, 0, s>>>(u, F3, g, c.ph, c.tm, rows);
+}
+
+template <int NT>
+static void launch_stage3d_nt(const Ctx& c, const double* uc, const double* u0, double* out,
+                              const double* F3, bool three, double c1, double c2, double c3,
+                              cudaStream_t s) {
+    const Geom& g = c.g;
+    const int rows = stage3d_rows(g);
+    dim3 grid((g.nx + NT - 5) / (NT - 4), (g.ny + rows - 1) / rows, g.nz);
+#define GK_S3(TH, PL) \
+    k_stage3d<NT, TH, PL><<<grid, NT, 0, s>>>(uc, u0, out, F3, g, c.ph, c1, c2, c3, c.tm, rows)
+    if (three) {
+        if (c.ph.plm) GK_S3(true, true);
+        else GK_S3(true, false);
+    } else {
+        if (c.ph.plm) GK_S3(false, true);
+        else GK_S3(false, false);
+    }
+#undef GK_S3
+}
+
+void launch_stage3d(const Ctx& c, const double* uc, const double* u0, double* out, const double* F3,
+                    int three, double c1, double c2, double c3, cudaStream_t s) {
+    switch (stage3d_nt(c.g)) {
+        case 64: launch_stage3d_nt<64>(c, uc, u0, out, F3, three != 0, c1, c2, c3, s); break;
+        case 96: launch_stage3d_nt<96>(c, uc, u0, out, F3, three != 0, c1, c2, c3, s); break;
+        default: launch_stage3d_nt<128>(c, uc, u0, out, F3, three != 0, c1, c2, c3, s); break;
+    }
 }
 
 void launch_kick(const Ctx& c, double* u, int which, cudaStream_t s) {

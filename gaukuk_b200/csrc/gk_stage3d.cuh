@@ -1,0 +1,221 @@
+// gk_stage3d.cuh -- the 3D RK stage in two kernels (included by
+// gk_kernels.cuh inside the mode namespace).
+//
+// k_zflux: the z-face fluxes of a state into F3.  The reference forms the
+// z-face states with ReconstructYZPLM, whose slope is along y
+// (recon_piecewise_linear.cpp:29-50): the left state of face (k-1|k) is the
+// upper y state of cell (k-1, j), the right state the lower y state of cell
+// (k, j).  A thread owns a column i of one face plane and marches up a
+// segment of rows, converting the rows of the two planes to primitives once
+// (ConsToPrim, adiabatic.cpp:18-61) and keeping three rows of each in
+// registers.
+//
+// k_stage3d: one z-plane of the stage, as the fused 2D stage does it --
+// a CTA owns NT-4 columns plus a 2-cell halo, marches up a segment of rows,
+// exchanges x neighbours through shared memory and solves each x and y face
+// once -- with all five variables, and adds the z-flux divergence from F3.
+// Face states, Riemann solver, flux divergence, RK combine and floors are the
+// generic path's expressions (k_c2p, k_flux, k_update), so both paths give
+// the same bits.
+#pragma once
+
+// PLM face states of one variable from three cells, as k_flux forms them.
+__device__ __forceinline__ double plm_up(double a, double b, double c) {
+#if GK_FASTMATH
+    return b + vanleer_half(b - a, c - b);
+#else
+    return b + 0.5 * vanleer(b - a, c - b);
+#endif
+}
+__device__ __forceinline__ double plm_down(double a, double b, double c) {
+#if GK_FASTMATH
+    return b - vanleer_half(b - a, c - b);
+#else
+    return b - 0.5 * vanleer(b - a, c - b);
+#endif
+}
+
+struct W5 {
+    double v[5];  // primitive slots: rho, vx, vy, p, vz
+};
+
+__device__ __forceinline__ W5 c2p_at(const double* __restrict__ u, const Geom& g, const Phys& ph,
+                                     long long c) {
+    W5 w;
+    cons_to_prim5(u[gk::S_DEN * g.vstride + c], u[gk::S_MTX * g.vstride + c],
+                  u[gk::S_MTY * g.vstride + c], u[gk::S_MTZ * g.vstride + c],
+                  u[gk::S_ENG * g.vstride + c], ph, w.v);
+    return w;
+}
+
+// Riemann problem of an x face (vx | vy, vz) and a y face (vy | vz, vx),
+// hllc.cpp:25-27; the fluxes land in slot order (DEN, MTX, MTY, ENG, MTZ).
+__device__ __forceinline__ void hllc5_x(const double (&l)[5], const double (&r)[5], const Phys& ph,
+                                        double (&F)[5]) {
+    Flux5 f;
+    hllc<true, kSel>(l[gk::P_RHO], l[gk::P_VX], l[gk::P_VY], l[gk::P_VZ], l[gk::P_PRE], r[gk::P_RHO],
+                     r[gk::P_VX], r[gk::P_VY], r[gk::P_VZ], r[gk::P_PRE], ph, f);
+    F[gk::S_DEN] = f.d;
+    F[gk::S_MTX] = f.n;
+    F[gk::S_MTY] = f.t1;
+    F[gk::S_MTZ] = f.t2;
+    F[gk::S_ENG] = f.e;
+}
+__device__ __forceinline__ void hllc5_y(const double (&l)[5], const double (&r)[5], const Phys& ph,
+                                        double (&F)[5]) {
+    Flux5 f;
+    hllc<true, kSel>(l[gk::P_RHO], l[gk::P_VY], l[gk::P_VZ], l[gk::P_VX], l[gk::P_PRE], r[gk::P_RHO],
+                     r[gk::P_VY], r[gk::P_VZ], r[gk::P_VX], r[gk::P_PRE], ph, f);
+    F[gk::S_DEN] = f.d;
+    F[gk::S_MTY] = f.n;
+    F[gk::S_MTZ] = f.t1;
+    F[gk::S_MTX] = f.t2;
+    F[gk::S_ENG] = f.e;
+}
+
+// ------------------------------------------------------------ z faces
+template <bool PLM>
+__global__ void __launch_bounds__(128)
+    k_zflux(const double* __restrict__ u, double* __restrict__ F3, Geom g, Phys ph,
+            const DevTime* __restrict__ tm, int rows) {
+    if (!tm->active) return;
+    const int i = g.ib + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.ie) return;
+    const int k = g.kb + blockIdx.z;  // face (k-1 | k), k = kb .. ke
+    const int y0 = g.jb + blockIdx.y * rows;
+    const int y1 = min(y0 + rows, g.je);
+    // rows j-1, j, j+1 of the planes below (L) and above (R) the face
+    W5 Lm = c2p_at(u, g, ph, sidx(g, k - 1, y0 - 1, i)), L0 = c2p_at(u, g, ph, sidx(g, k - 1, y0, i));
+    W5 Rm = c2p_at(u, g, ph, sidx(g, k, y0 - 1, i)), R0 = c2p_at(u, g, ph, sidx(g, k, y0, i));
+    for (int j = y0; j < y1; ++j) {
+        const W5 Lp = c2p_at(u, g, ph, sidx(g, k - 1, j + 1, i));
+        const W5 Rp = c2p_at(u, g, ph, sidx(g, k, j + 1, i));
+        double wl[5], wr[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            if (PLM) {
+                wl[v] = plm_up(Lm.v[v], L0.v[v], Lp.v[v]);
+                wr[v] = plm_down(Rm.v[v], R0.v[v], Rp.v[v]);
+            } else {
+                wl[v] = L0.v[v];
+                wr[v] = R0.v[v];
+            }
+        }
+        // z face: (vz | vx, vy)
+        Flux5 f;
+        hllc<true, kSel>(wl[gk::P_RHO], wl[gk::P_VZ], wl[gk::P_VX], wl[gk::P_VY], wl[gk::P_PRE],
+                         wr[gk::P_RHO], wr[gk::P_VZ], wr[gk::P_VX], wr[gk::P_VY], wr[gk::P_PRE], ph, f);
+        const long long c = fidx(g, k, j, i);
+        F3[gk::S_DEN * g.fvstride + c] = f.d;
+        F3[gk::S_MTZ * g.fvstride + c] = f.n;
+        F3[gk::S_MTX * g.fvstride + c] = f.t1;
+        F3[gk::S_MTY * g.fvstride + c] = f.t2;
+        F3[gk::S_ENG * g.fvstride + c] = f.e;
+        Lm = L0; L0 = Lp;
+        Rm = R0; R0 = Rp;
+    }
+}
+
+// ------------------------------------------------------------ x-y plane stage
+// THREE = false: out = c1*uc - c2*dF (stage 1); true: out = c1*u0 + c2*uc -
+// c3*dF.  out never aliases uc (neighbours of uc are read while out is
+// written); u0 may alias out (read pointwise, before the write).
+template <int NT, bool THREE, bool PLM>
+__global__ void __launch_bounds__(NT, 2)
+    k_stage3d(const double* __restrict__ uc, const double* u0, double* out,
+              const double* __restrict__ F3, Geom g, Phys ph, double c1, double c2, double c3,
+              const DevTime* __restrict__ tm, int rows) {
+    if (!tm->active) return;
+    __shared__ double sP[5][NT];
+    __shared__ double sXL[5][NT];
+    __shared__ double sF[5][NT];
+    const double dt = tm->dt;
+    const double dtdx = dt * g.dxRec, dtdy = dt * g.dyRec, dtdz = dt * g.dzRec;
+    const int t = threadIdx.x;
+    const int tl = t > 0 ? t - 1 : 0;
+    const int tr = t < NT - 1 ? t + 1 : t;
+    const int xi = g.ib - 2 + blockIdx.x * (NT - 4) + t;
+    const int xl = xi < g.lenx ? xi : g.lenx - 1;  // clamped load column
+    const bool do_cell = t >= 2 && t <= NT - 3 && xi < g.ie;
+    const int k = g.kb + blockIdx.z;
+    const int y0 = g.jb + blockIdx.y * rows;
+    const int y1 = min(y0 + rows, g.je);
+    auto at = [&](int j) { return sidx(g, k, j, xl); };
+
+    // primitives of rows y0-2, y0-1, y0 and y0+1
+    const W5 Pm2 = c2p_at(uc, g, ph, at(y0 - 2));
+    W5 Pm1 = c2p_at(uc, g, ph, at(y0 - 1));
+    W5 P0 = c2p_at(uc, g, ph, at(y0));
+    double wlNext[5], fyPrev[5];
+    // lower state of y face y0 (upper y state of cell y0-1), then that face
+    {
+        const W5 P1 = c2p_at(uc, g, ph, at(y0 + 1));
+        double wr[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            wlNext[v] = PLM ? plm_up(Pm2.v[v], Pm1.v[v], P0.v[v]) : Pm1.v[v];
+            wr[v] = PLM ? plm_down(Pm1.v[v], P0.v[v], P1.v[v]) : P0.v[v];
+        }
+        hllc5_y(wlNext, wr, ph, fyPrev);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) wlNext[v] = PLM ? plm_up(Pm1.v[v], P0.v[v], P1.v[v]) : P0.v[v];
+        Pm1 = P0;
+        P0 = P1;
+    }
+    // row f: the x faces of cell row f-1 and the y face f above it; update row f-1
+    for (int f = y0 + 1; f <= y1; ++f) {
+        const W5 P1 = c2p_at(uc, g, ph, at(f + 1));
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sP[v][t] = Pm1.v[v];
+        __syncthreads();
+        double xr[5], wr[5], wlNew[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const double a = sP[v][tl], c = sP[v][tr];
+            if (PLM) {
+                sXL[v][t] = plm_up(a, Pm1.v[v], c);
+                xr[v] = plm_down(a, Pm1.v[v], c);
+                wr[v] = plm_down(Pm1.v[v], P0.v[v], P1.v[v]);
+                wlNew[v] = plm_up(Pm1.v[v], P0.v[v], P1.v[v]);
+            } else {
+                sXL[v][t] = Pm1.v[v];
+                xr[v] = Pm1.v[v];
+                wr[v] = P0.v[v];
+                wlNew[v] = P0.v[v];
+            }
+        }
+        __syncthreads();
+        double xlst[5], fx[5], fy[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) xlst[v] = sXL[v][tl];
+        hllc5_x(xlst, xr, ph, fx);
+        hllc5_y(wlNext, wr, ph, fy);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sF[v][t] = fx[v];
+        __syncthreads();
+        if (do_cell) {
+            // update_cons.cpp (3D): (Fx(i+1)-Fx(i))*dtdx + (Fy(j+1)-Fy(j))*dtdy + (Fz(k+1)-Fz(k))*dtdz
+            const long long c = at(f - 1);
+            const long long fc = fidx(g, k, f - 1, xi);
+            double r[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                double dF = (sF[v][tr] - fx[v]) * dtdx;
+                dF = dF + (fy[v] - fyPrev[v]) * dtdy +
+                     (F3[v * g.fvstride + fc + g.fkstride] - F3[v * g.fvstride + fc]) * dtdz;
+                if (THREE) r[v] = c1 * u0[v * g.vstride + c] + c2 * uc[v * g.vstride + c] - c3 * dF;
+                else r[v] = c1 * uc[v * g.vstride + c] - c2 * dF;
+            }
+            floors5(r, ph);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) out[v * g.vstride + c] = r[v];
+        }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            fyPrev[v] = fy[v];
+            wlNext[v] = wlNew[v];
+        }
+        Pm1 = P0;
+        P0 = P1;
+    }
+}

@@ -152,7 +152,7 @@ class Sim:
     def path(self) -> str:
         p = ctypes.c_int()
         _lib.check(self._L.gk_path(self.h, ctypes.byref(p)), self.h)
-        return {0: "generic", 1: "fused2d"}[p.value]
+        return {0: "generic", 1: "fused2d", 2: "stage3d"}[p.value]
 
     def set_tiling(self, threads: int, rows: int) -> None:
         """Tile shape of the fused 2D stage kernel (threads per CTA 64/128/256,
