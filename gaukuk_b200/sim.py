@@ -10,7 +10,7 @@ main.cpp:44-52.  States cross the boundary in the reference's TArray layout,
 from __future__ import annotations
 
 import ctypes
-from typing import Dict, List, Optional, Tuple
+from typing import Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -153,6 +153,41 @@ class Sim:
         p = ctypes.c_int()
         _lib.check(self._L.gk_path(self.h, ctypes.byref(p)), self.h)
         return {0: "generic", 1: "fused2d", 2: "stage3d"}[p.value]
+
+    def set_fixed_boundary(self, snapshot: Optional[np.ndarray], fix_inner: bool = False) -> None:
+        """Data of the fixed (type 4) sides: the reference-layout state at
+        enrollment (Boundary::EnrollFixedBoundaryData); fix_inner also resets
+        the inner disk (FixedBDInner).  None removes them."""
+        if snapshot is None:
+            _lib.check(self._L.gk_set_fixed_boundary(self.h, None, 0), self.h)
+            return
+        a = np.ascontiguousarray(snapshot, dtype=np.float64)
+        if a.shape != self.params.shape:
+            raise ValueError(f"snapshot shape {a.shape} != {self.params.shape}")
+        _lib.check(self._L.gk_set_fixed_boundary(self.h, a.ctypes.data_as(ctypes.c_void_p),
+                                                 int(bool(fix_inner))), self.h)
+
+    def set_point_gravity(self, masses: Sequence[Sequence[float]]) -> None:
+        """Point masses as SourceTerm::EnrollPointGravity takes them, each
+        (gm, x, y, z, rs); none, one, or two (a binary: the second orbits the
+        first with the separation, angular speed and phase the reference's
+        EnrollPointGravity computes)."""
+        import math
+        if len(masses) > 2:
+            raise ValueError("at most two point masses")
+        p = np.zeros(11)
+        if masses:
+            p[0:5] = masses[0]
+        if len(masses) == 2:
+            gm0, x0, y0, z0, _ = masses[0]
+            gm, x, y, z, rs = masses[1]
+            ab = math.sqrt((x - x0) * (x - x0) + (y - y0) * (y - y0) + (z - z0) * (z - z0))
+            p[5:8] = (gm, z, rs)
+            p[8] = math.sqrt((gm0 + gm) / (ab * ab * ab))
+            p[9] = ab
+            p[10] = math.atan2(y - y0, x - x0)
+        _lib.check(self._L.gk_set_point_gravity(self.h, len(masses),
+                                                p.ctypes.data_as(ctypes.c_void_p)), self.h)
 
     def set_tiling(self, threads: int, rows: int) -> None:
         """Tile shape of the fused 2D stage kernel (threads per CTA 64/128/256,

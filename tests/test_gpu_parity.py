@@ -63,6 +63,11 @@ def _cases():
     yield "box16x12x10", p, problems.random_smooth(p, seed=3, with_vz=True)
     p = Params(nx=24, ny=20, nz=1, integrator=2, tmax=1.0, dtoutput=1.0, stepmax=15)
     yield "kh_with_vz", p, problems.random_smooth(p, seed=4, with_vz=True)
+    p = Params(nx=30, ny=18, nz=14, bc=(1,) * 6, integrator=2, tmax=1.0, dtoutput=1.0, stepmax=12)
+    yield "box30x18x14_rk2", p, problems.random_smooth(p, seed=6, with_vz=True)
+    p = Params(nx=20, ny=16, nz=12, bc=(3, 2, 0, 1, 2, 3), integrator=2, rc_order=1, tmax=1.0,
+               dtoutput=1.0, stepmax=10)
+    yield "box20x16x12_rc1_bcs", p, problems.random_smooth(p, seed=7, with_vz=True)
 
 
 @pytest.mark.parametrize("case", list(_cases()), ids=lambda c: c[0])
@@ -78,8 +83,44 @@ def test_parity_mode_bitwise(case):
 def test_paths_selected():
     p, c = problems.kh(32)
     assert _sim(p, c).path == "fused2d"
+    s = _sim(p, c)
+    s.set_point_gravity([(1.0, 0.0, 0.0, 0.0, 0.1)])  # point masses run on the generic path
+    assert s.path == "generic"
     p, c = problems.sod(64)
     assert _sim(p, c).path == "generic"
+    p = Params(nx=16, ny=16, nz=16, bc=(1,) * 6, integrator=2, tmax=1.0, dtoutput=1.0)
+    c = problems.random_smooth(p, seed=1, with_vz=True)
+    assert _sim(p, c).path == "stage3d"
+    assert _sim(dataclasses.replace(p, integrator=1), c).path == "generic"  # Euler: in place
+
+
+def test_stage3d_equals_generic_path_bitwise(monkeypatch):
+    """The 3D stage (z fluxes + fused x-y stage per plane) uses the generic
+    path's expressions: both give the same bits in parity mode."""
+    p = Params(nx=40, ny=36, nz=32, bc=(1, 3, 1, 1, 2, 1), integrator=3, tmax=1.0, dtoutput=1.0,
+               stepmax=6)
+    c = problems.random_smooth(p, seed=8, with_vz=True)
+    a = _sim(p, c)
+    monkeypatch.setenv("GK_STAGE3D", "0")
+    b = _sim(p, c)
+    monkeypatch.delenv("GK_STAGE3D")
+    assert a.path == "stage3d" and b.path == "generic"
+    a.run(p.tmax, p.dtoutput)
+    b.run(p.tmax, p.dtoutput)
+    assert a.dt_log() == b.dt_log()
+    assert np.array_equal(a.download(), b.download())
+
+
+def test_fast_mode_3d_within_tolerance():
+    p = Params(nx=32, ny=32, nz=32, bc=(1,) * 6, integrator=2, tmax=1.0, dtoutput=1.0, stepmax=60)
+    c = problems.random_smooth(p, seed=9, with_vz=True)
+    ref, ref_dts, _ = _oracle_run(p, c)
+    s = _sim(p, c, mode="fast")
+    assert s.path == "stage3d"
+    s.run(p.tmax, p.dtoutput)
+    assert len(s.dt_log()) == 60
+    errs = rel_linf(active(p, s.download()), ref)
+    assert max(errs) <= FAST_TOL, errs
 
 
 @pytest.mark.parametrize("n", [256])
