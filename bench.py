@@ -230,14 +230,22 @@ def main_ours(args, rank, world, local_rank):
     barrier, max_over_ranks = reps.barrier, reps.max
 
     n = args.n
-    p, c = problems.kh(n, seed=rank)
+    if args.ncu_case and args.box3d:
+        # a 3D case for profilers: periodic box with a smooth random state, RK2
+        from gaukuk_b200.config import Params
+        m = args.box3d
+        p = Params(nx=m, ny=m, nz=m, bc=(1,) * 6, integrator=2, tmax=1.0, dtoutput=1.0)
+        c = problems.random_smooth(p, seed=rank, with_vz=True)
+    else:
+        p, c = problems.kh(n, seed=rank)
     cells = p.nx * p.ny
     sim = Sim(p, c, mode=args.mode, device=local_rank)
     if args.ncu_case:
         # a short run for profilers: upload + `steps` steps, nothing else
         sim.run_steps(args.steps)
         if rank == 0:
-            print(json.dumps({"ncu_case": True, "n": n, "steps": args.steps, "mode": args.mode,
+            print(json.dumps({"ncu_case": True, "n": n, "box3d": args.box3d, "path": sim.path,
+                              "steps": args.steps, "mode": args.mode,
                               "t": sim.get_time()}))
         sim.close()
         return 0
@@ -590,6 +598,8 @@ def main():
     ap.add_argument("--ens-tmax", type=float, default=1.0)
     ap.add_argument("--ncu-case", action="store_true",
                     help="upload and run --steps steps only (for ncu captures)")
+    ap.add_argument("--box3d", type=int, default=0,
+                    help="with --ncu-case: a periodic N^3 box (the 3D stage) instead of KH")
     args = ap.parse_args()
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
