@@ -48,6 +48,24 @@ __device__ __forceinline__ W5 c2p_at(const double* __restrict__ u, const Geom& g
     return w;
 }
 
+// Raw conserved values of one cell (slot order), loaded ahead of their use
+// so that the loads of the next row are in flight while this row computes.
+struct Q5 {
+    double q[5];
+};
+__device__ __forceinline__ Q5 load5(const double* __restrict__ u, const Geom& g, long long c) {
+    Q5 r;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) r.q[v] = __ldg(u + v * g.vstride + c);
+    return r;
+}
+__device__ __forceinline__ W5 c2p_q(const Q5& a, const Phys& ph) {
+    W5 w;
+    cons_to_prim5(a.q[gk::S_DEN], a.q[gk::S_MTX], a.q[gk::S_MTY], a.q[gk::S_MTZ], a.q[gk::S_ENG], ph,
+                  w.v);
+    return w;
+}
+
 // Riemann problem of an x face (vx | vy, vz) and a y face (vy | vz, vx),
 // hllc.cpp:25-27; the fluxes land in slot order (DEN, MTX, MTY, ENG, MTZ).
 __device__ __forceinline__ void hllc5_x(const double (&l)[5], const double (&r)[5], const Phys& ph,
@@ -87,9 +105,18 @@ __global__ void __launch_bounds__(128)
     // rows j-1, j, j+1 of the planes below (L) and above (R) the face
     W5 Lm = c2p_at(u, g, ph, sidx(g, k - 1, y0 - 1, i)), L0 = c2p_at(u, g, ph, sidx(g, k - 1, y0, i));
     W5 Rm = c2p_at(u, g, ph, sidx(g, k, y0 - 1, i)), R0 = c2p_at(u, g, ph, sidx(g, k, y0, i));
+    Q5 qL = load5(u, g, sidx(g, k - 1, y0 + 1, i)), qR = load5(u, g, sidx(g, k, y0 + 1, i));
     for (int j = y0; j < y1; ++j) {
-        const W5 Lp = c2p_at(u, g, ph, sidx(g, k - 1, j + 1, i));
-        const W5 Rp = c2p_at(u, g, ph, sidx(g, k, j + 1, i));
+        // raw row j+2 in flight while row j+1 is converted and face j solved
+        Q5 nL = qL, nR = qR;
+        if (j + 2 <= y1) {
+            nL = load5(u, g, sidx(g, k - 1, j + 2, i));
+            nR = load5(u, g, sidx(g, k, j + 2, i));
+        }
+        const W5 Lp = c2p_q(qL, ph);
+        const W5 Rp = c2p_q(qR, ph);
+        qL = nL;
+        qR = nR;
         double wl[5], wr[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
@@ -162,9 +189,13 @@ __global__ void __launch_bounds__(NT, 2)
         Pm1 = P0;
         P0 = P1;
     }
-    // row f: the x faces of cell row f-1 and the y face f above it; update row f-1
+    // row f: the x faces of cell row f-1 and the y face f above it; update row f-1.
+    // The raw row f+2 is loaded one row ahead of its conversion.
+    Q5 Qn = load5(uc, g, at(y0 + 2));
     for (int f = y0 + 1; f <= y1; ++f) {
-        const W5 P1 = c2p_at(uc, g, ph, at(f + 1));
+        const Q5 Q1 = Qn;
+        if (f + 2 <= y1 + 1) Qn = load5(uc, g, at(f + 2));
+        const W5 P1 = c2p_q(Q1, ph);
 #pragma unroll
         for (int v = 0; v < 5; ++v) sP[v][t] = Pm1.v[v];
         __syncthreads();
