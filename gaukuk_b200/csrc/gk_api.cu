@@ -1049,6 +1049,9 @@ int gk_ens_create(gk_handle* const* handles, int n, gk_ensemble** out) {
         gk_handle* h = handles[i];
         if (!h || !h->uploaded) return GK_ERR_STATE;
         if (h->path != 1 || h->ctx.ph.integrator != 2 || h->ctx.ph.fix_inner) return GK_ERR_UNSUPPORTED;
+        // an instance's physics is copied here: fixed data must already be set
+        for (int s = 0; s < 6; ++s)
+            if (h->ctx.ph.bc[s] == 4 && !h->ctx.ph.fixed_bd) return GK_ERR_STATE;
         if (h->ks != handles[0]->ks || h->device != handles[0]->device ||
             h->ctx.ph.plm != handles[0]->ctx.ph.plm)
             return GK_ERR_INVALID;

@@ -77,6 +77,8 @@ __device__ __forceinline__ void bc_fill_one(double* __restrict__ u, const Geom& 
     const long long dst = sidx(g, ck, cj, ci), src = sidx(g, sk, sj, si);
     if (type == 4) {
         // FixedBD* (fixed.cpp:16-176): the ghost keeps its value at enrollment
+        // (the host refuses to run a type-4 side without data; never read null)
+        if (!ph.fixed_bd) return;
 #pragma unroll
         for (int v = 0; v < 5; ++v) u[v * g.vstride + dst] = ph.fixed_bd[v * g.vstride + dst];
         return;

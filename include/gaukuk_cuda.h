@@ -188,8 +188,9 @@ int gk_set_tiling(gk_handle* h, int threads, int rows);
  * in a CUDA graph of whole steps; each instance keeps its own handle, clock
  * and dt, and its results equal those of running it alone.  The handles
  * stay valid for upload, download and time queries; they must outlive the
- * ensemble.  No counterpart in the reference, which runs one problem per
- * process. */
+ * ensemble.  A handle with a fixed (type 4) side must have its data set
+ * (gk_set_fixed_boundary) before it joins: GK_ERR_STATE otherwise.  No
+ * counterpart in the reference, which runs one problem per process. */
 typedef struct gk_ensemble gk_ensemble;
 int gk_ens_create(gk_handle* const* handles, int n, gk_ensemble** out);
 void gk_ens_destroy(gk_ensemble* e);

@@ -85,3 +85,26 @@ def test_autotuner_applies_a_candidate():
     s = Sim(p, c, mode="fast")
     th, rows, ms = autotune.tune_single(s, steps=2, use_cache=False)
     assert th in autotune.THREADS and rows in autotune.ROWS and ms > 0
+
+
+def test_ensemble_refuses_fixed_sides_without_data():
+    """An instance's physics is copied when the ensemble is made, so a
+    handle with a fixed (type 4) side must have its data set first: without
+    them creation fails with a state error; with them the ensemble runs and
+    equals the same problem run alone."""
+    from gaukuk_b200._lib import GkError
+    from gaukuk_b200.ensemble import Ensemble
+    from gaukuk_b200.sim import Sim
+    p, c = problems.kh(64, seed=2)
+    p = dataclasses.replace(p, bc=(4, 4) + tuple(p.bc[2:]), tmax=0.03, dtoutput=0.03)
+    s = Sim(p, c, mode="parity")
+    with pytest.raises(GkError) as e:
+        Ensemble([s])
+    assert e.value.code == -5
+    s.set_fixed_boundary(c)
+    Ensemble([s]).run(p.tmax)
+    got = active(p, s.download())
+    ref = Sim(p, c, mode="parity")
+    ref.set_fixed_boundary(c)
+    ref.run(p.tmax, p.dtoutput)
+    assert np.array_equal(got, active(p, ref.download()))
