@@ -77,7 +77,8 @@ def build_hook(hook_src: str, name: Optional[str] = None, verbose: bool = False,
 
 
 REFERENCE_SRC = os.environ.get("GK_REFERENCE_SRC", "/root/reference")
-REFERENCE_HOOKS = ("blast", "disk", "disk_planet", "example", "kh", "rt", "shock_tube", "wave_test")
+REFERENCE_HOOKS = ("blast", "disk", "disk_planet", "example", "kh", "rt", "shock_tube", "solid_body",
+                   "wave_test")
 
 
 def build_host(verbose: bool = False, force: bool = False) -> None:

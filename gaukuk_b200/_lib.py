@@ -80,6 +80,7 @@ SIGNATURES = {
                                     ctypes.c_float, ctypes.c_ulonglong, _vp]),
     "gk_mlp_forward": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _vp]),
     "gk_set_fixed_boundary": (ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    "gk_set_immersed": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp]),
     "gk_set_point_gravity": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "gk_set_flux_model": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                          ctypes.c_float, ctypes.c_float]),

@@ -121,6 +121,8 @@ struct gk_handle {
     float* model = nullptr;   // learned flux correction (device), or null
     gk::FluxGate gate;
     double* fixed = nullptr;  // state at enrollment of fixed boundaries (device layout)
+    gk::Shell* shells = nullptr;  // immersed body's shell table (device)
+    int shell_cap = 0;
     unsigned* fired = nullptr;  // faces where the detector kept plain HLLC
     int tiling_rows = 0;
     cudaGraphExec_t gexec = nullptr;
@@ -214,6 +216,8 @@ int build_ctx(gk_handle* h) {
     ph.fixed_bd = nullptr;
     ph.fix_inner = 0;
     ph.npoint = 0;
+    ph.shells = nullptr;
+    ph.nshell = 0;
     ph.fill_z = 0;
     if (g.ndim == 3) {
         // z sides of type 0 run OutflowCopyYL/YR after the y fill
@@ -459,7 +463,7 @@ int copy_ref_to_device(gk_handle* h, const double* ref, double* dev) {
 // A change of the physics that kernels take by value: the captured graph
 // is rebuilt at the next launch, and the path follows.
 int physics_changed(gk_handle* h) {
-    if (h->ctx.ph.npoint) h->ctx.has_vz = 1;  // see gk_upload_cons
+    if (h->ctx.ph.npoint || h->ctx.ph.nshell) h->ctx.has_vz = 1;  // see gk_upload_cons
     if (h->gexec) {
         cudaGraphExecDestroy(h->gexec);
         h->gexec = nullptr;
@@ -525,6 +529,7 @@ void gk_destroy(gk_handle* h) {
     for (double* p : {h->A, h->B, h->C, h->W, h->F1, h->F2, h->F3, h->dlog, h->fixed}) cudaFree(p);
     cudaFree(h->model);
     cudaFree(h->fired);
+    cudaFree(h->shells);
     cudaFree(h->tm);
     cudaFree(h->dflag);
     if (h->htm) cudaFreeHost(h->htm);
@@ -555,8 +560,9 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
         GK_CUDA(h, cudaStreamSynchronize(h->stream));
         h->ctx.has_vz = flag;
     }
-    // a point mass off the mid-plane makes MTZ non-zero during the run
-    if (h->ctx.ph.npoint) h->ctx.has_vz = 1;
+    // a point mass off the mid-plane makes MTZ non-zero during the run; an
+    // immersed body writes MTZ (signed zeros in 2D) into its shell cells
+    if (h->ctx.ph.npoint || h->ctx.ph.nshell) h->ctx.has_vz = 1;
     h->path = choose_path(h);
     h->ctx.h2d_rows = stage_rows(g);
     h->ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
@@ -1284,6 +1290,56 @@ extern "C" int gk_set_fixed_boundary(gk_handle* h, const double* snapshot, int f
     ph.inner[1] = static_cast<int>(g.ib + 0.75 * (g.ie - g.ib));
     ph.inner[2] = static_cast<int>(g.jb + 0.25 * (g.je - g.jb));
     ph.inner[3] = static_cast<int>(g.jb + 0.75 * (g.je - g.jb));
+    return physics_changed(h);
+}
+
+extern "C" int gk_set_immersed(gk_handle* h, int n, const int* ids, const int* ntar,
+                               const double* dir, const double* w) {
+    if (!h || n < 0 || (n > 0 && (!ids || !ntar || !dir || !w))) return GK_ERR_INVALID;
+    GK_CUDA(h, cudaSetDevice(h->device));
+    gk::Phys& ph = h->ctx.ph;
+    const gk::Geom& g = h->ctx.g;
+    if (n > 0 && (g.nx <= 1 || g.ny <= 1))
+        return fail(h, GK_ERR_INVALID, "an immersed body needs a 2D or 3D grid (immersed.cpp:90-92)");
+    // The table in device layout.  Every cell must be active: the reference's
+    // setup rejects bodies whose search reaches outside (immersed.cpp:201-205),
+    // and the kernel relies on it for its indices.
+    std::vector<gk::Shell> tab((size_t)n);
+    auto id = [&](int c, int s, int t) { return ids[((size_t)c * n + s) * 9 + t]; };
+    auto index = [&](int s, int t, long long* out) {
+        const int i = id(0, s, t), j = id(1, s, t), k = id(2, s, t);
+        if (i < g.ib || i >= g.ie || j < g.jb || j >= g.je || k < g.kb || k >= g.ke) return false;
+        *out = (long long)(k - g.kofs) * g.kstride + (long long)j * g.pitch + i;
+        return true;
+    };
+    for (int s = 0; s < n; ++s) {
+        gk::Shell& sh = tab[s];
+        std::memset(&sh, 0, sizeof(sh));
+        sh.ntar = ntar[s];
+        if (sh.ntar < 0 || sh.ntar > 8)
+            return fail(h, GK_ERR_INVALID, "immersed shell: target count outside [0, 8]");
+        if (!index(s, 0, &sh.cell)) return fail(h, GK_ERR_INVALID, "immersed shell cell not active");
+        for (int t = 1; t <= sh.ntar; ++t)
+            if (!index(s, t, &sh.tgt[t - 1]))
+                return fail(h, GK_ERR_INVALID, "immersed shell target not active");
+        for (int c = 0; c < 4; ++c) sh.dir[c] = dir[(size_t)c * n + s];
+        for (int t = 0; t < 9; ++t) sh.w[t] = w[(size_t)s * 9 + t];
+    }
+    if (n > h->shell_cap) {
+        GK_CUDA(h, cudaStreamSynchronize(h->stream));
+        cudaFree(h->shells);
+        h->shells = nullptr;
+        h->shell_cap = 0;
+        GK_CUDA(h, cudaMalloc(&h->shells, sizeof(gk::Shell) * (size_t)n));
+        h->shell_cap = n;
+    }
+    if (n > 0) {
+        GK_CUDA(h, cudaMemcpyAsync(h->shells, tab.data(), sizeof(gk::Shell) * (size_t)n,
+                                   cudaMemcpyHostToDevice, h->stream));
+        GK_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    ph.shells = n > 0 ? h->shells : nullptr;
+    ph.nshell = n;
     return physics_changed(h);
 }
 

@@ -48,6 +48,18 @@ struct Geom {
     double xmin, ymin, zmin;  // cell centres: xmin - ng*dx + 0.5*dx + i*dx (sim.cpp:36-41)
 };
 
+// One shell cell of an immersed body (Boundary::SetupImmersedShell,
+// immersed.cpp:89-241), indices in device layout: the cell, its image-point
+// targets tgt[0..ntar), the direction cosines cos(phi), sin(phi),
+// cos(theta), sin(theta) and the weights disGamma(s, 0..8).
+struct Shell {
+    long long cell;
+    long long tgt[8];
+    double dir[4];
+    double w[9];
+    int ntar;
+};
+
 struct Phys {
     double gamma, gm1, gm1Rec, gmRec, cq;  // cq = 0.5*(1+1/gamma) (hllc.cpp:55-58)
     double cfl, dmin, pmin;
@@ -68,6 +80,9 @@ struct Phys {
     // 2; pm = gm0, x0, y0, z0, rs0, gm1, z1, rs1, omega, ab, theta1.
     int npoint;
     double pm[11];
+    // Immersed body (immersed.cpp): nshell shell cells (0 = none).
+    const Shell* shells;
+    int nshell;
 };
 
 // Device-resident clock of Sim::Advance (sim.cpp:69-117).  Written by the

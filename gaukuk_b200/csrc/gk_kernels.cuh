@@ -145,6 +145,55 @@ __global__ void k_fix_inner(double* __restrict__ u, Geom g, Phys ph, const DevTi
     for (int v = 0; v < 5; ++v) u[v * g.vstride + c] = ph.fixed_bd[v * g.vstride + c];
 }
 
+// Boundary::ImmersedReflective (immersed.cpp:243-303), run after the sides
+// and before the inner reset (boundary.cpp:127-142): each shell cell of an
+// immersed body takes the weighted state at its image point, with the
+// radial velocity reversed.  Targets lie outside the body and shell cells
+// inside it, so no cell is both read and written: one thread per shell cell
+// gives the reference's serial result.  Expression order is the reference's
+// (CarToLocal / LocalToCar at immersed.cpp:72-85 inlined).
+__global__ void k_immersed(double* __restrict__ u, Geom g, Phys ph, const DevTime* __restrict__ tm) {
+    if (!tm->active) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ph.nshell) return;
+    const gk::Shell& sh = ph.shells[s];
+    const double cosp = sh.dir[0], sinp = sh.dir[1], cost = sh.dir[2], sint = sh.dir[3];
+    const double w0 = sh.w[0];
+    const long long vs = g.vstride;
+    double dens = 0, vr = 0, vp = 0, vt = 0, pres = 0;
+    for (int n = 1; n <= sh.ntar; ++n) {
+        const long long c = sh.tgt[n - 1];
+        const double wn = sh.w[n];
+        const double denTar = smax(u[gk::S_DEN * vs + c], ph.dmin);
+        const double denInv = GK_RCP(denTar);
+        dens += GK_RCP(1 - w0) * wn * denTar;
+        const double vx = u[gk::S_MTX * vs + c] * denInv;
+        const double vy = u[gk::S_MTY * vs + c] * denInv;
+        const double vz = u[gk::S_MTZ * vs + c] * denInv;
+        const double vrloc = vx * cosp * sint + vy * sinp * sint + vz * cost;
+        const double vploc = -vx * sinp + vy * cosp;
+        const double vtloc = vx * cosp * cost + vy * sinp * cost - vz * sint;
+        vr += GK_RCP(-1. - w0) * wn * vrloc;
+        vp += GK_RCP(1. - w0) * wn * vploc;
+        vt += GK_RCP(1. - w0) * wn * vtloc;
+        const double engTar = u[gk::S_ENG * vs + c];
+        const double engKin = 0.5 * denTar * (vx * vx + vy * vy + vz * vz);
+        double preTar = ph.gm1 * (engTar - engKin);
+        preTar = (preTar > ph.pmin) ? preTar : ph.pmin;
+        pres += GK_RCP(1. - w0) * wn * preTar;
+    }
+    const double vx = vr * sint * cosp + vt * cost * cosp - vp * sinp;
+    const double vy = vr * sint * sinp + vt * cost * sinp + vp * cosp;
+    const double vz = vr * cost - vt * sint;
+    const long long c = sh.cell;
+    u[gk::S_DEN * vs + c] = dens;
+    u[gk::S_MTX * vs + c] = dens * vx;
+    u[gk::S_MTY * vs + c] = dens * vy;
+    u[gk::S_MTZ * vs + c] = dens * vz;
+    const double engKin = 0.5 * dens * (vx * vx + vy * vy + vz * vz);
+    u[gk::S_ENG * vs + c] = engKin + pres * ph.gm1Rec;
+}
+
 // ------------------------------------------------------------ ConsToPrim
 // EquationOfState::ConsToPrim (adiabatic.cpp:18-61) over every stored cell.
 __device__ __forceinline__ void cons_to_prim5(double d, double mx, double my, double mz, double e,
@@ -1132,6 +1181,8 @@ void launch_bc(const Ctx& c, double* u, cudaStream_t s) {
     const int sides = (g.nz > 1 && c.ph.fill_z) ? 6 : 4;
     dim3 grid((unsigned)((m + 127) / 128), sides);
     k_bc<<<grid, 128, 0, s>>>(u, g, c.ph, c.tm);
+    if (c.ph.nshell > 0 && c.ph.shells)
+        k_immersed<<<(c.ph.nshell + 127) / 128, 128, 0, s>>>(u, g, c.ph, c.tm);
     if (c.ph.fix_inner && c.ph.inner[1] > c.ph.inner[0] && c.ph.inner[3] > c.ph.inner[2]) {
         dim3 gi((c.ph.inner[1] - c.ph.inner[0] + 127) / 128, c.ph.inner[3] - c.ph.inner[2], g.nz);
         k_fix_inner<<<gi, 128, 0, s>>>(u, g, c.ph, c.tm);

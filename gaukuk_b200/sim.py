@@ -189,6 +189,31 @@ class Sim:
         _lib.check(self._L.gk_set_point_gravity(self.h, len(masses),
                                                 p.ctypes.data_as(ctypes.c_void_p)), self.h)
 
+    def set_immersed(self, ids: Optional[np.ndarray], ntar: Optional[np.ndarray] = None,
+                     direction: Optional[np.ndarray] = None,
+                     weights: Optional[np.ndarray] = None) -> None:
+        """An immersed solid body as the table Boundary::SetupImmersedShell
+        builds: ids int (3, n, 9) of shell cells (t = 0) and targets
+        (reference indices i, j, k), ntar int (n,), direction (4, n) =
+        cos(phi), sin(phi), cos(theta), sin(theta), weights (n, 9) =
+        disGamma.  None removes the body."""
+        if ids is None:
+            _lib.check(self._L.gk_set_immersed(self.h, 0, None, None, None, None), self.h)
+            return
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        n = ids.shape[1]
+        ntar = np.ascontiguousarray(ntar, dtype=np.int32)
+        direction = np.ascontiguousarray(direction, dtype=np.float64)
+        weights = np.ascontiguousarray(weights, dtype=np.float64)
+        if (ids.shape != (3, n, 9) or ntar.shape != (n,) or direction.shape != (4, n)
+                or weights.shape != (n, 9)):
+            raise ValueError("immersed table shapes: ids (3, n, 9), ntar (n,), direction (4, n), "
+                             "weights (n, 9)")
+        vp = ctypes.c_void_p
+        _lib.check(self._L.gk_set_immersed(self.h, n, ids.ctypes.data_as(vp), ntar.ctypes.data_as(vp),
+                                           direction.ctypes.data_as(vp),
+                                           weights.ctypes.data_as(vp)), self.h)
+
     def set_tiling(self, threads: int, rows: int) -> None:
         """Tile shape of the fused 2D stage kernel (threads per CTA 64/128/256,
         rows per segment); see gaukuk_b200.autotune."""

@@ -8,6 +8,10 @@
 // the in-place result is the same even when a direction has fewer cells than
 // ghosts.
 #include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
 #include <stdexcept>
 
 #include "../utils/utils.hpp"
@@ -115,7 +119,7 @@ void Boundary::UpdateBD(TArray<Real>& cons, const Grid& grid, const Domain& doma
         Bdzl(cons, grid, eos);
         Bdzr(cons, grid, eos);
     }
-    if (immersed_) throw std::runtime_error("immersed boundaries are not available");
+    if (immersed_) ImmersedReflective(cons, eos);
     if (fixInner_) FixedInner(cons, grid, domain);
 }
 
@@ -135,8 +139,186 @@ void Boundary::FixedInner(TArray<Real>& cons, const Grid& grid, const Domain& do
                 }
 }
 
-void Boundary::SetupImmersedShell(const Grid&, const Domain&, Real, Real, Real, Real) {
+namespace {
+
+// FindLeftId / FindRightId (immersed.cpp:19-47): the first active index
+// whose centre is at or past centre - 1.2 r (from below), or at or before
+// centre + 1.2 r (from above); the body's reach must lie in the domain.
+int FirstFrom(const TArray<Real>& xc, int b, int e, Real centre, Real r, Real lo) {
+    const Real edge = centre - 1.2 * r;
+    if (edge < lo) throw std::invalid_argument("immersed boundary out of domain");
+    for (int i = b; i < e; i++)
+        if (xc(i) >= edge) return i;
+    return e;
+}
+int LastFrom(const TArray<Real>& xc, int b, int e, Real centre, Real r, Real hi) {
+    const Real edge = centre + 1.2 * r;
+    if (edge > hi) throw std::invalid_argument("immersed boundary out of domain");
+    for (int i = e - 1; i >= b; i--)
+        if (xc(i) <= edge) return i;
+    return b;
+}
+
+Real Norm3(Real a, Real b, Real c) { return std::sqrt(a * a + b * b + c * c); }
+
+// IsShellCell (immersed.cpp:49-68): inside the body, with one of the six
+// cells two ghost widths away along an axis outside it.
+bool IsShell(Real dx, Real dy, Real dz, Real r, Real sx, Real sy, Real sz) {
+    if (!(Norm3(dx, dy, dz) < r)) return false;
+    const Real shift[6][3] = {{sx, 0, 0}, {-sx, 0, 0}, {0, sy, 0}, {0, -sy, 0}, {0, 0, sz}, {0, 0, -sz}};
+    for (const auto& s : shift)
+        if (Norm3(dx + s[0], dy + s[1], dz + s[2]) > r) return true;
+    return false;
+}
+
+}  // namespace
+
+// Boundary::SetupImmersedShell (immersed.cpp:89-241): the shell cells of a
+// sphere (a cylinder through the plane in 2D) and, for each, the active
+// cells within one cell of its image point across the surface that lie
+// outside the body, with inverse-square-distance weights in which the cell
+// itself (distance twice its depth) takes part.  Cells are listed in k, j, i
+// order; targets in the reference's search order (i, then j, then k offset).
+void Boundary::SetupImmersedShell(const Grid& grid, const Domain& domain, Real xShell, Real yShell,
+                                  Real zShell, Real rShell) {
+    if (grid.nx <= 1 || grid.ny <= 1)
+        throw std::invalid_argument("immersed boundary has to be at least 2D. ");
     immersed_ = true;
+    const int il = FirstFrom(domain.xc, grid.ib, grid.ie, xShell, rShell, domain.xmin);
+    const int ir = LastFrom(domain.xc, grid.ib, grid.ie, xShell, rShell, domain.xmax);
+    const int jl = FirstFrom(domain.yc, grid.jb, grid.je, yShell, rShell, domain.ymin);
+    const int jr = LastFrom(domain.yc, grid.jb, grid.je, yShell, rShell, domain.ymax);
+    int kl = grid.kb, kr = grid.ke;
+    if (grid.nz > 1) {
+        kl = FirstFrom(domain.zc, grid.kb, grid.ke, zShell, rShell, domain.zmin);
+        kr = LastFrom(domain.zc, grid.kb, grid.ke, zShell, rShell, domain.zmax);
+    }
+    nShell_ = 0;
+    if (il > ir || jl > jr || kl > kr) throw std::invalid_argument("immersed boundary out of domain");
+    const Real sx = grid.nGhost * domain.dx, sy = grid.nGhost * domain.dy,
+               sz = grid.nGhost * domain.dz;
+    std::vector<int> cells;  // (i, j, k) triples
+    for (int k = kl; k < kr; k++)
+        for (int j = jl; j < jr; j++)
+            for (int i = il; i < ir; i++)
+                if (IsShell(domain.xc(i) - xShell, domain.yc(j) - yShell, domain.zc(k) - zShell,
+                            rShell, sx, sy, sz)) {
+                    cells.push_back(i);
+                    cells.push_back(j);
+                    cells.push_back(k);
+                }
+    const int n = static_cast<int>(cells.size() / 3);
+    const int W = kTarMax + 1;
+    shellIds_.assign((size_t)3 * n * W, 0);
+    nTars_.assign(n, 0);
+    shellDir_.assign((size_t)4 * n, 0.0);
+    disGamma_.assign((size_t)n * W, 0.0);
+    auto id = [&](int c, int s, int t) -> int& { return shellIds_[((size_t)c * n + s) * W + t]; };
+    const int rx = 2 * grid.nGhost, ry = 2 * grid.nGhost, rz = grid.nz > 1 ? 2 * grid.nGhost : 0;
+    for (int s = 0; s < n; s++) {
+        const int i = cells[3 * s], j = cells[3 * s + 1], k = cells[3 * s + 2];
+        id(0, s, 0) = i;
+        id(1, s, 0) = j;
+        id(2, s, 0) = k;
+        const Real delx = domain.xc(i) - xShell, dely = domain.yc(j) - yShell,
+                   delz = domain.zc(k) - zShell;
+        const Real rnow = Norm3(delx, dely, delz);
+        const Real rxy = std::sqrt(delx * delx + dely * dely);
+        Real cosp = 1.0, sinp = 0.0, cost = 1.0, sint = 0.0;
+        if (!(rxy < 1e-15)) {
+            cosp = delx / rxy;
+            sinp = dely / rxy;
+        }
+        if (!(rnow < 1e-15)) {
+            cost = delz / rnow;
+            sint = rxy / rnow;
+        }
+        shellDir_[0 * (size_t)n + s] = cosp;
+        shellDir_[1 * (size_t)n + s] = sinp;
+        shellDir_[2 * (size_t)n + s] = cost;
+        shellDir_[3 * (size_t)n + s] = sint;
+        // the image point: the cell reflected through the surface
+        const Real xImg = sint * cosp * (2 * rShell - rnow) + xShell;
+        const Real yImg = sint * sinp * (2 * rShell - rnow) + yShell;
+        const Real zImg = cost * (2 * rShell - rnow) + zShell;
+        Real dist[kTarMax + 1];
+        dist[0] = 2 * (rShell - rnow);
+        int nt = 0;
+        for (int a = -rx; a < rx + 1; ++a)
+            for (int b = -ry; b < ry + 1; ++b)
+                for (int c = -rz; c < rz + 1; ++c) {
+                    const int it = i + a, jt = j + b, kt = k + c;
+                    if (it < grid.ib || it >= grid.ie || jt < grid.jb || jt >= grid.je ||
+                        kt < grid.kb || kt >= grid.ke)
+                        throw std::invalid_argument(
+                            "immersed body is too close to the domain boundary, neighboor search "
+                            "out of range.");
+                    const Real xt = domain.xc(it), yt = domain.yc(jt), zt = domain.zc(kt);
+                    if (!(std::abs(xt - xImg) <= domain.dx && std::abs(yt - yImg) <= domain.dy &&
+                          std::abs(zt - zImg) <= domain.dz))
+                        continue;
+                    if (!(Norm3(xt - xShell, yt - yShell, zt - zShell) > rShell)) continue;
+                    if (++nt > kTarMax)
+                        throw std::logic_error("n of imagine points is more than nTarMax");
+                    id(0, s, nt) = it;
+                    id(1, s, nt) = jt;
+                    id(2, s, nt) = kt;
+                    dist[nt] = Norm3(xt - xImg, yt - yImg, zt - zImg);
+                }
+        nTars_[s] = nt;
+        Real sum = 0.;
+        for (int t = 0; t < nt + 1; t++) sum = sum + 1. / (dist[t] * dist[t]);
+        for (int t = 0; t < nt + 1; t++) disGamma_[(size_t)s * W + t] = 1. / (dist[t] * dist[t] * sum);
+    }
+    nShell_ = n;
+}
+
+// Boundary::ImmersedReflective (immersed.cpp:243-303): every shell cell gets
+// the weighted image-point state of its targets, radial velocity reversed.
+// Targets are outside the body and shell cells inside, so the order of the
+// cells does not matter.
+void Boundary::ImmersedReflective(TArray<Real>& cons, const EquationOfState& eos) const {
+    const Real gm1 = eos.GetGamma() - 1;
+    const int n = nShell_, W = kTarMax + 1;
+    auto id = [&](int c, int s, int t) { return shellIds_[((size_t)c * n + s) * W + t]; };
+    for (int s = 0; s < n; s++) {
+        const Real cosp = shellDir_[s], sinp = shellDir_[(size_t)n + s],
+                   cost = shellDir_[2 * (size_t)n + s], sint = shellDir_[3 * (size_t)n + s];
+        const Real w0 = disGamma_[(size_t)s * W];
+        Real dens = 0, vr = 0, vp = 0, vt = 0, pres = 0;
+        for (int t = 1; t <= nTars_[s]; t++) {
+            const int it = id(0, s, t), jt = id(1, s, t), kt = id(2, s, t);
+            const Real wt = disGamma_[(size_t)s * W + t];
+            const Real denTar = std::max(cons(DEN, kt, jt, it), DENSITY_FLOOR);
+            const Real denInv = 1.0 / denTar;
+            dens += 1. / (1 - w0) * wt * denTar;
+            const Real vx = cons(MTX, kt, jt, it) * denInv;
+            const Real vy = cons(MTY, kt, jt, it) * denInv;
+            const Real vz = cons(MTZ, kt, jt, it) * denInv;
+            // velocity in the local (r, phi, theta) frame (immersed.cpp:72-77)
+            const Real vrl = vx * cosp * sint + vy * sinp * sint + vz * cost;
+            const Real vpl = -vx * sinp + vy * cosp;
+            const Real vtl = vx * cosp * cost + vy * sinp * cost - vz * sint;
+            vr += 1. / (-1. - w0) * wt * vrl;
+            vp += 1. / (1. - w0) * wt * vpl;
+            vt += 1. / (1. - w0) * wt * vtl;
+            const Real engKin = 0.5 * denTar * (vx * vx + vy * vy + vz * vz);
+            Real pre = gm1 * (cons(ENG, kt, jt, it) - engKin);
+            pre = (pre > PRESSURE_FLOOR) ? pre : PRESSURE_FLOOR;
+            pres += 1. / (1. - w0) * wt * pre;
+        }
+        // back to Cartesian (immersed.cpp:80-85)
+        const Real vx = vr * sint * cosp + vt * cost * cosp - vp * sinp;
+        const Real vy = vr * sint * sinp + vt * cost * sinp + vp * cosp;
+        const Real vz = vr * cost - vt * sint;
+        const int i = id(0, s, 0), j = id(1, s, 0), k = id(2, s, 0);
+        cons(DEN, k, j, i) = dens;
+        cons(MTX, k, j, i) = dens * vx;
+        cons(MTY, k, j, i) = dens * vy;
+        cons(MTZ, k, j, i) = dens * vz;
+        const Real engKin = 0.5 * dens * (vx * vx + vy * vy + vz * vz);
+        cons(ENG, k, j, i) = engKin + eos.EGas(dens, pres);
+    }
 }
 
 // Boundary::EnrollFixedBoundaryData (fixed.cpp:226-268): the sides read the
@@ -148,10 +330,90 @@ void Boundary::EnrollFixedBoundaryData(const TArray<Real>& cons, const Grid&, bo
     if (fixInner) fixInner_ = true;
 }
 
-const char* Boundary::DeviceBlocker() const {
-    if (custom_) return "self-defined boundary routines run on the host only";
-    if (immersed_) return "immersed boundaries are not implemented on the device";
-    return "";
+namespace {
+
+bool SameBits(Real a, Real b) {
+    std::uint64_t x, y;
+    std::memcpy(&x, &a, sizeof x);
+    std::memcpy(&y, &b, sizeof y);
+    return x == y;
+}
+
+}  // namespace
+
+// A self-defined side (a setup's SelfDefineBD* routine) is run three times
+// on copies of the state: the state itself, every value -1e300, every value
+// NaN.  It is stationary when it writes exactly the cells a fixed side of
+// that side fills (the ghosts of the active rows or columns), each with the
+// same bits in all three runs, and nothing else: then its writes depend on
+// the state in no way the probes can see, and the device fills the side as
+// a fixed side from the values captured.  A cell it skips keeps -1e300 in one
+// run and NaN in the other, so partial fills are caught; so are routines
+// that copy or scale state values.  A routine that throws, or anything else,
+// keeps the run on the host.
+bool Boundary::PrepareDevice(const TArray<Real>& cons, const Grid& grid,
+                             const EquationOfState& eos, std::string* why) {
+    static const char* names[6] = {"x left", "x right", "y left", "y right", "z left", "z right"};
+    const BoundaryFunc* fn[6] = {&Bdxl, &Bdxr, &Bdyl, &Bdyr, &Bdzl, &Bdzr};
+    for (int s = 0; s < 6; ++s) deviceTypes_[s] = types_[s];
+    deviceFixedSet_ = fixedEnrolled_;
+    if (fixedEnrolled_) deviceFixed_ = fixedData_;
+    const int sides = grid.nz > 1 ? 6 : 4;  // UpdateBD fills z sides in 3D only
+    for (int s = 0; s < sides; ++s) {
+        if (!((custom_ >> s) & 1)) continue;
+        const int dir = s / 2, side = s % 2;
+        const int len[3] = {grid.lenx, grid.leny, grid.lenz};
+        const int n[3] = {grid.nx, grid.ny, grid.nz};
+        int lo[3] = {grid.ib, grid.jb, grid.kb}, hi[3] = {grid.ie, grid.je, grid.ke};
+        lo[dir] = side == 0 ? 0 : grid.nGhost + n[dir];
+        hi[dir] = side == 0 ? grid.nGhost : len[dir];
+        auto inside = [&](int k, int j, int i) {
+            return i >= lo[0] && i < hi[0] && j >= lo[1] && j < hi[1] && k >= lo[2] && k < hi[2];
+        };
+        TArray<Real> probe[3] = {cons, cons, cons};
+        const Real fill[2] = {-1e300, std::numeric_limits<Real>::quiet_NaN()};
+        for (int p = 1; p < 3; ++p) {
+            Real* d = probe[p].data();
+            for (size_t q = 0; q < probe[p].GetSize(); ++q) d[q] = fill[p - 1];
+        }
+        try {
+            for (auto& a : probe) (*fn[s])(a, grid, eos);
+        } catch (const std::exception& e) {
+            *why = std::string("the self-defined ") + names[s] +
+                   " boundary cannot be probed for the device (" + e.what() + ")";
+            return false;
+        }
+        bool ok = true;
+        for (int v = 0; v < NVar && ok; ++v)
+            for (int k = 0; k < grid.lenz && ok; ++k)
+                for (int j = 0; j < grid.leny && ok; ++j)
+                    for (int i = 0; i < grid.lenx && ok; ++i) {
+                        const Real a = probe[0](v, k, j, i), b = probe[1](v, k, j, i),
+                                   c = probe[2](v, k, j, i);
+                        if (inside(k, j, i)) {
+                            ok = SameBits(a, b) && SameBits(a, c);
+                        } else {
+                            ok = SameBits(a, cons(v, k, j, i)) && SameBits(b, fill[0]) &&
+                                 SameBits(c, fill[1]);
+                        }
+                    }
+        if (!ok) {
+            *why = std::string("the self-defined ") + names[s] +
+                   " boundary depends on the state or writes outside its ghost strip; it runs "
+                   "on the host only";
+            return false;
+        }
+        if (!deviceFixedSet_) {
+            deviceFixed_.NewArray(NVar, grid.lenz, grid.leny, grid.lenx);
+            deviceFixedSet_ = true;
+        }
+        for (int v = 0; v < NVar; ++v)
+            for (int k = lo[2]; k < hi[2]; ++k)
+                for (int j = lo[1]; j < hi[1]; ++j)
+                    for (int i = lo[0]; i < hi[0]; ++i) deviceFixed_(v, k, j, i) = probe[0](v, k, j, i);
+        deviceTypes_[s] = 4;
+    }
+    return true;
 }
 
 }  // namespace Gaukuk

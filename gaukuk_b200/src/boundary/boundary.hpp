@@ -4,14 +4,17 @@
 // one std::function per side chosen from xleft..zright (0 copy, 1 periodic,
 // 2 reflective, 3 outflow, 4 fixed), UpdateBD, and the Enroll* hooks with
 // which a setup file installs its own static SelfDefineBD* routines or the
-// fixed-boundary data.  The host fill is used for the state a setup hook
-// produces (main.cpp:30) and for output; during Sim::Advance the device fills
-// ghosts with the same rules, fixed sides and the inner reset included.
-// Problems that enroll their own routines or an immersed body run on the
-// host only and Sim::Advance rejects them.
+// fixed-boundary data, and the immersed solid body (immersed.cpp).  The host
+// fill is used for the state a setup hook produces (main.cpp:30) and for
+// output; during Sim::Advance the device fills ghosts with the same rules:
+// fixed sides, the immersed body and the inner reset included.  The device
+// cannot call a hook's own routine: PrepareDevice turns one whose writes do
+// not depend on the state into a fixed side, and rejects the others.
 #pragma once
 
 #include <functional>
+#include <string>
+#include <vector>
 
 #include "../eos/eos.hpp"
 #include "../gaukuk.hpp"
@@ -46,8 +49,26 @@ public:
     const TArray<Real>& FixedData() const { return fixedData_; }
     bool HasFixedData() const { return fixedEnrolled_; }
     bool FixInner() const { return fixInner_; }
-    // Why the device path cannot take this configuration ("" when it can).
-    const char* DeviceBlocker() const;
+    // Readies the device's view of the ghost fill from the state `cons`:
+    // every self-defined side must be stationary (see boundary.cpp) and then
+    // becomes a fixed side with the values it writes.  False with the reason
+    // in *why when a side cannot run on the device.
+    bool PrepareDevice(const TArray<Real>& cons, const Grid& grid, const EquationOfState& eos,
+                       std::string* why);
+    // After PrepareDevice: the ghost-fill type of side s on the device, and
+    // the fixed-side data (the enrolled snapshot with captured sides written
+    // in; empty when no side is fixed).
+    int DeviceType(int s) const { return deviceTypes_[s]; }
+    const TArray<Real>& DeviceFixedData() const { return deviceFixed_; }
+    bool HasDeviceFixedData() const { return deviceFixedSet_; }
+
+    // The immersed body's table in the reference's layout (immersed.cpp:146-150):
+    // ids (3, nShell, 9), nTars (nShell), direction (4, nShell), disGamma (nShell, 9).
+    int ShellCount() const { return nShell_; }
+    const int* ShellIds() const { return shellIds_.data(); }
+    const int* ShellTargets() const { return nTars_.data(); }
+    const Real* ShellDirection() const { return shellDir_.data(); }
+    const Real* ShellWeights() const { return disGamma_.data(); }
 
 private:
     static void SelfDefineBDXL(TArray<Real>& cons, const Grid& grid, const EquationOfState& eos);
@@ -63,6 +84,16 @@ private:
     bool fixedEnrolled_ = false, fixInner_ = false;
     TArray<Real> fixedData_;
     void FixedInner(TArray<Real>& cons, const Grid& grid, const Domain& domain) const;
+
+    static constexpr int kTarMax = 8;  // nTarMax (boundary.hpp:109)
+    int nShell_ = 0;
+    std::vector<int> shellIds_, nTars_;
+    std::vector<Real> shellDir_, disGamma_;
+    void ImmersedReflective(TArray<Real>& cons, const EquationOfState& eos) const;
+
+    int deviceTypes_[6] = {0, 0, 0, 0, 0, 0};
+    bool deviceFixedSet_ = false;
+    TArray<Real> deviceFixed_;
 };
 
 }  // namespace Gaukuk

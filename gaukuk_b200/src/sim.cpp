@@ -1,6 +1,9 @@
 // sim.cpp -- Domain and Sim of the host interface.
 //
-// Domain geometry is the reference's (src/sim.cpp:16-42).  Sim::Sim reads
+// Domain geometry is the reference's (src/sim.cpp:16-42).  The device is
+// set up at the first Advance from the state then in cons: boundaries
+// (self-defined sides captured as fixed ones, fixed data, the immersed
+// body's table) and point masses.  Sim::Sim reads
 // the same keys (sim.cpp:45-67).  Sim::Advance replaces the reference's host
 // loop (sim.cpp:69-117) with one call into libgk_cuda.so: the state is
 // uploaded, the device runs every step up to the output time, and the state
@@ -73,8 +76,8 @@ void Check(gk_handle* h, int rc, const char* what) {
 
 void Sim::EnsureDevice() {
     if (dev_) return;
-    const char* why = boundary.DeviceBlocker();
-    if (*why) throw std::runtime_error(why);
+    std::string why;
+    if (!boundary.PrepareDevice(cons, grid, eos, &why)) throw std::runtime_error(why);
     gk_grid_desc gd{};
     gd.nx = grid.nx; gd.ny = grid.ny; gd.nz = grid.nz; gd.nghost = grid.nGhost;
     gd.xmin = domain.xmin; gd.xmax = domain.xmax;
@@ -85,7 +88,7 @@ void Sim::EnsureDevice() {
     pd.cfl = CFL;
     pd.integrator = integratorType;
     pd.rc_order = rcOrder;
-    for (int s = 0; s < 6; ++s) pd.bc[s] = boundary.Type(s);
+    for (int s = 0; s < 6; ++s) pd.bc[s] = boundary.DeviceType(s);
     pd.grav[0] = srcTerm.Gx();
     pd.grav[1] = srcTerm.Gy();
     pd.grav[2] = srcTerm.Gz();
@@ -95,9 +98,14 @@ void Sim::EnsureDevice() {
     pd.mode = gpuMode_ == 1 ? GK_MODE_FAST : GK_MODE_PARITY;
     pd.device = gpuDevice_;
     Check(nullptr, gk_create(&gd, &pd, &dev_), "gk_create");
-    if (boundary.HasFixedData())
-        Check(dev_, gk_set_fixed_boundary(dev_, boundary.FixedData().data(), boundary.FixInner()),
+    if (boundary.HasDeviceFixedData())
+        Check(dev_, gk_set_fixed_boundary(dev_, boundary.DeviceFixedData().data(), boundary.FixInner()),
               "gk_set_fixed_boundary");
+    if (boundary.ShellCount() > 0)
+        Check(dev_, gk_set_immersed(dev_, boundary.ShellCount(), boundary.ShellIds(),
+                                    boundary.ShellTargets(), boundary.ShellDirection(),
+                                    boundary.ShellWeights()),
+              "gk_set_immersed");
     double pm[11];
     const int npoint = srcTerm.PointParams(pm);
     if (npoint > 0) Check(dev_, gk_set_point_gravity(dev_, npoint, pm), "gk_set_point_gravity");
@@ -120,7 +128,7 @@ void Sim::SwapUnwritten() {
         for (int d = 0; d < 3; ++d)
             for (int s = 0; s < 2; ++s) filled[d][s] = n[d] > 1;
         if (grid.nz > 1)
-            for (int s = 0; s < 2; ++s) filled[2][s] = boundary.Type(4 + s) != 0;
+            for (int s = 0; s < 2; ++s) filled[2][s] = boundary.DeviceType(4 + s) != 0;
         const int k0 = grid.nz > 1 ? 0 : grid.kb, k1 = grid.nz > 1 ? grid.lenz : grid.ke;
         const int lo[3] = {grid.ib, grid.jb, grid.kb}, hi[3] = {grid.ie, grid.je, grid.ke};
         for (int v = 0; v < NVar; ++v)

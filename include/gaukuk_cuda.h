@@ -102,6 +102,24 @@ int gk_set_fixed_boundary(gk_handle* h, const double* snapshot, int fix_inner);
  * removes them.  Runs with point masses take the generic path. */
 int gk_set_point_gravity(gk_handle* h, int n, const double* params);
 
+/* Immersed solid body: the table Boundary::SetupImmersedShell builds
+ * (immersed.cpp:89-241), applied as Boundary::ImmersedReflective
+ * (immersed.cpp:243-303) at every ghost fill, after the sides and before
+ * the inner reset (boundary.cpp:127-142).  The arrays are the reference's
+ * own, for n shell cells (nTarMax = 8):
+ *   ids  int[3 * n * 9]   shellIDs(3, nShell, 9): ids[(c*n + s)*9 + t] is
+ *                         coordinate c (i, j, k; reference indices) of shell
+ *                         cell s (t = 0) and of its targets t = 1..ntar[s]
+ *   ntar int[n]           nTars
+ *   dir  double[4 * n]    shellDirection(4, nShell): cos(phi), sin(phi),
+ *                         cos(theta), sin(theta) at dir[c*n + s]
+ *   w    double[n * 9]    disGamma(nShell, 9)
+ * Every cell named must be active (GK_ERR_INVALID otherwise); n = 0 removes
+ * the body.  Needs nx > 1 and ny > 1; runs with a body take the generic
+ * path in 2D. */
+int gk_set_immersed(gk_handle* h, int n, const int* ids, const int* ntar, const double* dir,
+                    const double* w);
+
 /* Number of doubles in one reference-layout state: 5*lenz*leny*lenx. */
 long long gk_state_size(const gk_handle* h);
 

@@ -90,3 +90,36 @@ def test_restart_continues_bit_identically(hook, tmp_path):
     assert later and later == sorted(f for f in os.listdir(b) if f.startswith("cons_") and f > "cons_00002")
     for f in later:
         assert (a / f).read_bytes() == (b / f).read_bytes(), f
+
+
+def test_immersed_table_is_checked_and_switches_the_path():
+    """gk_set_immersed takes the reference's shell table; a cell outside the
+    active region is refused (the kernel indexes with it), a body sends a 2D
+    run to the generic path, and without it the next upload (which checks
+    MTZ again) brings the fused path back."""
+    from gaukuk_b200 import problems
+    from gaukuk_b200._lib import GkError
+    from gaukuk_b200.sim import Sim
+    p, c = problems.kh(32, seed=4)
+    g = p.ng
+    ids = np.zeros((3, 1, 9), dtype=np.int32)
+    ids[:, 0, 0] = (g + 10, g + 10, g)    # the shell cell (i, j, k)
+    ids[:, 0, 1] = (g + 14, g + 10, g)    # one target, outside the body
+    direction = np.array([[1.0], [0.0], [0.0], [1.0]])
+    w = np.zeros((1, 9))
+    w[0, :2] = (0.8, 0.2)
+    with Sim(p, c, mode="parity") as s:
+        assert s.path == "fused2d"
+        bad = ids.copy()
+        bad[0, 0, 1] = 1                  # a ghost column
+        with pytest.raises(GkError) as e:
+            s.set_immersed(bad, [1], direction, w)
+        assert e.value.code == -1
+        s.set_immersed(ids, [1], direction, w)
+        assert s.path == "generic"
+        s.run_steps(2)
+        a = s.download()
+        assert np.isfinite(a).all()
+        s.set_immersed(None)
+        s.upload(c)
+        assert s.path == "fused2d"

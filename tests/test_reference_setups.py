@@ -4,9 +4,11 @@ against the host layer (bin/gaukuk_ref_<name>.sim), run on the same .in
 parameters: blast (3D), disk (one point mass, fixed boundaries),
 disk_planet (a binary, fixed boundaries with the inner reset), example and
 kh (2D shear), rt (constant gravity, reflecting walls), shock_tube (3D
-slab), wave_test.  On the CPU the first frame (setup and host ghost fill)
-is byte-identical to the reference build's.  On the GPU every frame of the
-run is byte-identical in parity mode, except disk_planet: its orbit uses
+slab), solid_body (an immersed sphere in a flow from a self-defined inflow
+side; 2D, and 3D as solid_body@3d), wave_test.  On the CPU the first frame
+(setup and host ghost fill) is byte-identical to the reference build's.  On
+the GPU every frame of the run is byte-identical in parity mode, except
+disk_planet: its orbit uses
 cos/sin, which need not round alike on GPU and host, so it is held to
 1e-12."""
 import os
@@ -33,6 +35,7 @@ PLANET = (Params(nx=48, ny=48, xmin=-3.2, xmax=3.2, ymin=-3.2, ymax=3.2, zmin=-0
           {"GM": 1.0, "rs0": 0.01, "GMp": 0.001, "rp": 1.0, "rs1": 0.05, "r0": 1.0, "rho0": 1.0,
            "p": 1.0, "cs0": 0.1, "q": 1.0, "r_inner": 0.3})
 P3 = dict(xmin=-0.5, xmax=0.5, ymin=-0.5, ymax=0.5, zmin=-0.5, zmax=0.5)
+SOLID = {"r_solid": 1.0, "y0": 0.0, "z0": 0.0, "rho": 1.0, "p": 1.0, "vxIn": 4.0}
 CASES = {
     "disk": DISK,
     "disk_planet": PLANET,
@@ -55,6 +58,12 @@ CASES = {
                           bc=(2, 2, 1, 1, 1, 1), tmax=0.05, dtoutput=0.025, **P3),
                    {"pressureLeft": 1.0, "pressureRight": 0.1, "rhoLeft": 1.0, "rhoRight": 0.125,
                     "x0": 0.0}),
+    "solid_body": (Params(nx=64, ny=64, xmin=-5.0, xmax=5.0, ymin=-5.0, ymax=5.0, zmin=-0.5,
+                          zmax=0.5, cfl=0.5, integrator=2, rc_order=2, bc=(3, 3, 3, 3, 1, 1),
+                          tmax=0.2, dtoutput=0.1), dict(SOLID, x0=-3.0)),
+    "solid_body@3d": (Params(nx=32, ny=32, nz=16, xmin=-4.0, xmax=4.0, ymin=-4.0, ymax=4.0,
+                             zmin=-2.0, zmax=2.0, cfl=0.5, integrator=2, rc_order=2,
+                             bc=(3,) * 6, tmax=0.1, dtoutput=0.05), dict(SOLID, x0=-1.5)),
     "wave_test": (Params(nx=32, ny=32, cfl=0.5, integrator=2, rc_order=2, bc=(1,) * 6,
                          tmax=0.05, dtoutput=0.025, **P3),
                   {"addVel": 0.1, "amp": 0.01, "p0": 1.0, "rho0": 1.0, "sigma": 0.1, "x0": 0.0}),
@@ -68,6 +77,7 @@ def _run(exe, args, cwd):
 
 
 def _exes(name):
+    name = name.split("@")[0]  # variants run the same setup file
     ref = os.path.join(REF, f"ref_strict_ref_{name}")
     ours = os.path.join(BIN, f"gaukuk_ref_{name}.sim")
     if not (os.path.exists(ref) and os.path.exists(ours)):
@@ -114,3 +124,26 @@ def test_runs_match_the_reference(name, tmp_path):
                 scale = np.abs(x.data[v]).max() or 1.0
                 err = np.abs(x.data[v] - y.data[v]).max() / scale
                 assert err <= 1e-12, (f, v, err)
+
+
+@pytest.mark.parametrize("copies", [1, 0])
+def test_self_defined_sides_run_on_the_device_only_when_stationary(copies, tmp_path):
+    """A setup's own boundary routine cannot run on the device.  One that
+    writes a constant inflow (tests/setups/setup_inflow_sides.cpp) is captured
+    as a fixed side; one that copies the state (inflowCopies = 1) is refused
+    with a message, before any device work, so this runs on the CPU too."""
+    from gaukuk_b200 import _build_host
+    src = os.path.join(ROOT, "tests", "setups", "setup_inflow_sides.cpp")
+    exe = _build_host.build_hook(src, name="inflow_sides", out_dir=str(tmp_path))
+    p = Params(nx=16, ny=12, cfl=0.4, integrator=2, rc_order=2, bc=(3, 3, 3, 3, 1, 1),
+               tmax=0.02, dtoutput=0.01, **P3)
+    (tmp_path / "run.in").write_text(p.to_in_text({"inflowCopies": copies}))
+    r = subprocess.run([exe, "-i", "run.in"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=300)
+    refused = "depends on the state" in r.stderr
+    if copies:
+        assert r.returncode != 0 and refused, r.stderr[-2000:]
+    else:
+        # past the probe: it runs on a GPU, or fails later for want of one
+        assert not refused, r.stderr[-2000:]
+        assert (tmp_path / "cons_00000").exists()
