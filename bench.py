@@ -13,7 +13,9 @@ ours (default):
     buffer) is larger than L2, so no flush is needed between steps.
   * e2e: the same metric through the public C ABI with host buffers: every
     step uploads the state from pinned host memory (gk_upload_cons), runs one
-    time step (gk_run_steps) and downloads it (gk_download_planes).
+    time step (gk_run_steps) and downloads it (gk_download_planes).  The
+    z-momentum plane, zero in this 2D problem, is checked on the host and
+    stays put, so four planes cross the bus each way (gk_io_bytes).
   * roofline: the fused stage kernel's algorithmic HBM bytes per launch
     (80 B per cell on average: stage 1 reads and writes 4 doubles, stage 2
     reads 8 and writes 4) over its average launch time, measured with CUDA
@@ -314,11 +316,10 @@ def main_ours(args, rank, world, local_rank):
     host = torch.empty(p.shape, dtype=torch.float64, pin_memory=True).numpy()
     host[...] = c
     g = p.ng
-    h2d = 5 * p.lenx * p.leny * 8
-    d2h = 5 * p.lenx * p.leny * 8
     sim.upload(host)
     sim.run_steps(1)
     sim.download(host, planes_only=True)
+    h2d, d2h = sim.io_bytes()  # what crossed the bus per step (the zero MTZ plane stays put)
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):

@@ -44,6 +44,8 @@ SIGNATURES = {
     "gk_upload_cons": (ctypes.c_int, [_vp, _vp]),
     "gk_download_cons": (ctypes.c_int, [_vp, _vp]),
     "gk_download_planes": (ctypes.c_int, [_vp, _vp]),
+    "gk_io_bytes": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong),
+                                   ctypes.POINTER(ctypes.c_longlong)]),
     "gk_advance": (ctypes.c_int, [_vp, ctypes.c_double, _dp, _ip, _ip]),
     "gk_run_steps": (ctypes.c_int, [_vp, ctypes.c_int, _ip]),
     "gk_enqueue_steps": (ctypes.c_int, [_vp, ctypes.c_int]),

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -123,6 +124,8 @@ struct gk_handle {
     double* fixed = nullptr;  // state at enrollment of fixed boundaries (device layout)
     gk::Shell* shells = nullptr;  // immersed body's shell table (device)
     int shell_cap = 0;
+    bool mtz_plane_zero = false;  // 1D/2D: every stored MTZ value was +0.0 at upload
+    long long io_up = 0, io_down = 0;  // bytes the last upload / download moved
     unsigned* fired = nullptr;  // faces where the detector kept plain HLLC
     int tiling_rows = 0;
     cudaGraphExec_t gexec = nullptr;
@@ -445,9 +448,11 @@ int pull_time(gk_handle* h) {
 
 // A reference-layout host state (NVar x lenz x leny x lenx) into a device
 // state buffer (slots DEN, MTX, MTY, ENG, MTZ; stored planes; pitched rows).
-int copy_ref_to_device(gk_handle* h, const double* ref, double* dev) {
+// Stored planes of reference variable n (all five when n < 0).
+int copy_ref_to_device(gk_handle* h, const double* ref, double* dev, int only = -1) {
     const gk::Geom& g = h->ctx.g;
     for (int n = 0; n < 5; ++n) {
+        if (only >= 0 && n != only) continue;
         for (int kk = 0; kk < g.nzs; ++kk) {
             const int k = g.kofs + kk;
             const double* src = ref + ((size_t)(n * g.lenz + k) * g.leny) * g.lenx;
@@ -458,6 +463,31 @@ int copy_ref_to_device(gk_handle* h, const double* ref, double* dev) {
         }
     }
     return GK_OK;
+}
+
+// Whether every one of the n doubles at p has the bit pattern of +0.0; a
+// few host threads share the scan (it runs while the other planes copy).
+bool host_all_zero(const double* p, size_t n) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t parts = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, 8));
+    std::vector<unsigned char> zero(parts, 1);
+    auto scan = [&](size_t part) {
+        const size_t lo = n * part / parts, hi = n * (part + 1) / parts;
+        unsigned long long acc = 0;
+        for (size_t i = lo; i < hi; ++i) {
+            unsigned long long b;
+            std::memcpy(&b, p + i, sizeof b);
+            acc |= b;
+        }
+        zero[part] = acc == 0;
+    };
+    std::vector<std::thread> pool;
+    for (size_t part = 1; part < parts; ++part) pool.emplace_back(scan, part);
+    scan(0);
+    for (auto& t : pool) t.join();
+    for (unsigned char z : zero)
+        if (!z) return false;
+    return true;
 }
 
 // A change of the physics that kernels take by value: the captured graph
@@ -547,12 +577,37 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
     if (!h || !cons) return GK_ERR_INVALID;
     GK_CUDA(h, cudaSetDevice(h->device));
     const gk::Geom& g = h->ctx.g;
-    int rc0 = copy_ref_to_device(h, cons, h->A);
-    if (rc0 != GK_OK) return rc0;
+    const size_t plane_bytes = sizeof(double) * (size_t)g.lenx * g.leny;
+    // In 1D/2D the z momentum is usually zero everywhere: the other four
+    // variables are copied while the host checks its plane, and a plane that
+    // is +0.0 in every stored cell is cleared on the device instead of copied.
+    h->mtz_plane_zero = false;
+    h->io_up = 5LL * g.nzs * (long long)plane_bytes;
+    if (g.ndim <= 2 && g.nzs == 1) {
+        for (int n : {0, 1, 2, 4}) {
+            int rc = copy_ref_to_device(h, cons, h->A, n);
+            if (rc != GK_OK) return rc;
+        }
+        const double* mz = cons + ((size_t)(3 * g.lenz + g.kofs) * g.leny) * g.lenx;
+        if (host_all_zero(mz, (size_t)g.lenx * g.leny)) {
+            h->mtz_plane_zero = true;
+            h->io_up -= (long long)plane_bytes;
+            GK_CUDA(h, cudaMemsetAsync(h->A + (size_t)gk::S_MTZ * g.vstride, 0,
+                                       sizeof(double) * (size_t)g.vstride, h->stream));
+        } else {
+            int rc = copy_ref_to_device(h, cons, h->A, 3);
+            if (rc != GK_OK) return rc;
+        }
+    } else {
+        int rc0 = copy_ref_to_device(h, cons, h->A);
+        if (rc0 != GK_OK) return rc0;
+    }
     // Path: the fused kernel evolves four variables; it applies when the run
     // is 2D and MTZ is zero on every active cell (it then stays zero).
     h->ctx.has_vz = 1;
-    if (g.ndim <= 2) {
+    if (g.ndim <= 2 && h->mtz_plane_zero) {
+        h->ctx.has_vz = 0;
+    } else if (g.ndim <= 2) {
         GK_CUDA(h, cudaMemsetAsync(h->dflag, 0, sizeof(int), h->stream));
         h->ks->mtz_check(h->ctx, h->A, h->dflag, h->stream);
         int flag = 0;
@@ -601,7 +656,14 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
     rc = pull_time(h);
     if (rc != GK_OK) return rc;
     const gk::Geom& g = h->ctx.g;
+    // The fused 2D path never writes MTZ, so a plane cleared at upload is
+    // still +0.0 everywhere (no fixed data can fill its ghosts): a planes-only
+    // download leaves the caller's plane as it is.
+    const bool skip_mtz = !zero_other_planes && h->mtz_plane_zero && h->path == 1 &&
+                          !h->ctx.ph.fixed_bd;
+    h->io_down = 0;
     for (int n = 0; n < 5; ++n) {
+        if (skip_mtz && n == 3) continue;
         for (int kk = 0; kk < g.nzs; ++kk) {
             const int k = g.kofs + kk;
             double* dst = cons + ((size_t)(n * g.lenz + k) * g.leny) * g.lenx;
@@ -609,6 +671,7 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
             GK_CUDA(h, cudaMemcpy2DAsync(dst, sizeof(double) * g.lenx, src, sizeof(double) * g.pitch,
                                          sizeof(double) * g.lenx, g.leny, cudaMemcpyDeviceToHost,
                                          h->stream));
+            h->io_down += (long long)sizeof(double) * g.lenx * g.leny;
         }
     }
     // Ghost strips as the reference leaves them after a step: Sim's integrators
@@ -623,6 +686,7 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
     if (donor) {
         const size_t rowb = sizeof(double) * g.lenx, prow = sizeof(double) * g.pitch;
         for (int n = 0; n < 5; ++n) {
+            if (skip_mtz && n == 3) continue;
             for (int kk = 0; kk < g.nzs; ++kk) {
                 const int k = g.kofs + kk;
                 if (k < g.kb || k >= g.ke) continue;
@@ -635,6 +699,7 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
                                                      src + (size_t)g.jb * g.pitch + i0, prow,
                                                      sizeof(double) * g.ng, g.ny,
                                                      cudaMemcpyDeviceToHost, h->stream));
+                        h->io_down += (long long)sizeof(double) * g.ng * g.ny;
                     }
                 }
                 if (g.ny > 1) {
@@ -644,6 +709,7 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
                                                      src + (size_t)j0 * g.pitch + g.ib, prow,
                                                      sizeof(double) * g.nx, g.ng,
                                                      cudaMemcpyDeviceToHost, h->stream));
+                        h->io_down += (long long)sizeof(double) * g.nx * g.ng;
                     }
                 }
             }
@@ -659,6 +725,7 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
                                                      src + (size_t)g.jb * g.pitch + g.ib, prow,
                                                      sizeof(double) * g.nx, g.ny,
                                                      cudaMemcpyDeviceToHost, h->stream));
+                        h->io_down += (long long)sizeof(double) * g.nx * g.ny;
                     }
                 }
             }
@@ -676,6 +743,13 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
 
 int gk_download_cons(gk_handle* h, double* cons) { return download(h, cons, true); }
 int gk_download_planes(gk_handle* h, double* cons) { return download(h, cons, false); }
+
+int gk_io_bytes(const gk_handle* h, long long* upload, long long* download) {
+    if (!h) return GK_ERR_INVALID;
+    if (upload) *upload = h->io_up;
+    if (download) *download = h->io_down;
+    return GK_OK;
+}
 
 static int run_loop(gk_handle* h, double dtoutput, int nsteps, bool wait) {
     int rc = ensure_graph(h);

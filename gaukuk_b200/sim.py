@@ -78,7 +78,8 @@ class Sim:
 
     def download(self, out: Optional[np.ndarray] = None, planes_only: bool = False) -> np.ndarray:
         """The state in the reference layout.  planes_only leaves the planes the
-        device does not hold (1D/2D: k != nghost) as they are in ``out``."""
+        device does not hold (1D/2D: k != nghost) as they are in ``out``, and on
+        the fused 2D path a z-momentum plane that was zero at upload too."""
         if out is None:
             out = np.empty(self.params.shape, dtype=np.float64)
             planes_only = False
@@ -86,6 +87,12 @@ class Sim:
         fn = self._L.gk_download_planes if planes_only else self._L.gk_download_cons
         _lib.check(fn(self.h, out.ctypes.data_as(ctypes.c_void_p)), self.h)
         return out
+
+    def io_bytes(self) -> Tuple[int, int]:
+        """Bytes the last upload and the last download moved across the bus."""
+        up, down = ctypes.c_longlong(), ctypes.c_longlong()
+        _lib.check(self._L.gk_io_bytes(self.h, ctypes.byref(up), ctypes.byref(down)), self.h)
+        return up.value, down.value
 
     # -- time loop -------------------------------------------------------
     def advance(self, dtoutput: float) -> Tuple[float, int, bool]:

@@ -127,7 +127,9 @@ long long gk_state_size(const gk_handle* h);
  * the whole array, ghosts included, is copied to the device (the host array
  * is not retained), the dt log is cleared and the CFL reduction of
  * EquationOfState::CalCmax (adiabatic.cpp:115-160) is evaluated so that the
- * next step's dt is ready. */
+ * next step's dt is ready.  In 1D/2D a z-momentum plane that is +0.0 in every
+ * stored cell (checked on the host while the other planes copy) is cleared
+ * on the device instead of copied. */
 int gk_upload_cons(gk_handle* h, const double* cons);
 
 /* Copies the device state back into a reference-layout host array, as
@@ -139,8 +141,16 @@ int gk_download_cons(gk_handle* h, double* cons);
 /* As gk_download_cons, but writes only the planes the device holds (in 1D/2D
  * the active plane k = nghost) and leaves the caller's other planes as they
  * are -- the copy Sim::WriteData needs when Sim::cons is reused between
- * frames, since the reference never writes those planes. */
+ * frames, since the reference never writes those planes.  When the fused 2D
+ * path runs (gk_path = 1), the z-momentum plane was +0.0 everywhere at upload
+ * and no fixed data are set, nothing on the device writes that plane and it
+ * is left as it is in `cons` too: a caller that uploaded from the same array
+ * has the same bits there. */
 int gk_download_planes(gk_handle* h, double* cons);
+
+/* Bytes the last gk_upload_cons and the last download moved across the bus
+ * (either pointer may be NULL). */
+int gk_io_bytes(const gk_handle* h, long long* upload, long long* download);
 
 /* Replaces Sim::Advance (sim.cpp:69-117, sim.hpp:39): runs time steps on the
  * device until the output time t + dtoutput is reached (tolerance 1e-12),

@@ -123,3 +123,37 @@ def test_immersed_table_is_checked_and_switches_the_path():
         s.set_immersed(None)
         s.upload(c)
         assert s.path == "fused2d"
+
+
+def test_zero_z_momentum_plane_stays_on_the_host():
+    """A 2D state whose z-momentum plane is +0.0 everywhere uploads four
+    planes; a planes-only download on the fused path leaves that plane in the
+    caller's array, and the full download returns it as zeros.  A plane with
+    one non-zero ghost value is copied both ways (the run still takes the
+    fused path: only active cells decide that)."""
+    from gaukuk_b200 import problems
+    from gaukuk_b200.sim import Sim
+    p, c = problems.kh(48, seed=2)
+    plane = p.lenx * p.leny * 8
+    k = p.ng
+    with Sim(p, c, mode="parity") as s:
+        up, _ = s.io_bytes()
+        assert up == 4 * plane and s.path == "fused2d"
+        s.run_steps(2)
+        out = np.full(p.shape, 7.0)
+        s.download(out, planes_only=True)
+        assert (out[3, k] == 7.0).all()           # left as it was
+        full = s.download()
+        assert (full[3, k] == 0.0).all()
+        np.testing.assert_array_equal(out[[0, 1, 2, 4], k], full[[0, 1, 2, 4], k])
+        _, down = s.io_bytes()
+        strips = 5 * 2 * p.ng * (p.nx + p.ny) * 8  # ghost strips from the stage buffer
+        assert down == 5 * plane + strips
+    c2 = c.copy()
+    c2[3, k, 0, 0] = 1.0                          # a corner ghost
+    with Sim(p, c2, mode="parity") as s:
+        up, _ = s.io_bytes()
+        assert up == 5 * plane and s.path == "fused2d"
+        out = np.full(p.shape, 7.0)
+        s.download(out, planes_only=True)
+        assert out[3, k, 0, 0] == 1.0 and out[3, k, p.ng, p.ng] == 0.0
