@@ -321,6 +321,23 @@ __device__ __forceinline__ void floors4(double (&r)[4], const Phys& ph) {
     }
 }
 
+// floors4 that also returns the reciprocal density of the result (for the
+// CFL speed of the same cell).
+__device__ __forceinline__ double floors4_inv(double (&r)[4], const Phys& ph) {
+    if (r[0] < ph.dmin) {
+        r[0] = ph.dmin;
+        r[1] = 0.0;
+        r[2] = 0.0;
+        r[3] = ph.pmin / ph.gm1 + 0.0;
+        return GK_RCP(ph.dmin);
+    }
+    double inv_den = GK_RCP(r[0]);
+    double ke = 0.5 * inv_den * (r[1] * r[1] + r[2] * r[2]);
+    double press = ph.gm1 * (r[3] - ke);
+    if (press < ph.pmin) r[3] = ph.pmin / ph.gm1 + ke;
+    return inv_den;
+}
+
 __global__ void k_update(const double* u0, const double* uc, double* out,
                          const double* __restrict__ F1, const double* __restrict__ F2,
                          const double* __restrict__ F3, Geom g, Phys ph, int three, double c1,
@@ -438,6 +455,21 @@ __device__ __forceinline__ double cell_cmax(double d, double mx, double my, doub
     double local = fabs(vx) + cs;
     local = smax(local, fabs(vy) + cs);
     if (has_z) local = smax(local, fabs(vz) + cs);
+    return local;
+}
+
+// cell_cmax of a 2D cell (vz = 0) whose density is at least the floor,
+// given its reciprocal density: the same operations as cell_cmax without
+// recomputing 1/rho.
+__device__ __forceinline__ double cell_cmax_inv(double mx, double my, double e, double denInv,
+                                                const Phys& ph) {
+    double vx = mx * denInv, vy = my * denInv;
+    double engKin = 0.5 * (vx * mx + vy * my);
+    double pres = ph.gm1 * (e - engKin);
+    pres = (pres > ph.pmin) ? pres : ph.pmin;
+    double cs = GK_SQRT(ph.gamma * pres * denInv);
+    double local = fabs(vx) + cs;
+    local = smax(local, fabs(vy) + cs);
     return local;
 }
 
@@ -866,11 +898,14 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned phase, int* st
     atomicOr(status, gk::STATUS_TMA_TIMEOUT);
 }
 
+// Row exchanges of the stage: each thread's four values as two 16-byte
+// pairs, [pair][thread], so a warp's 16-byte accesses are conflict-free and
+// each exchange is two loads instead of four.
 template <int NT>
 struct StageShared {
-    double sP[4][NT];
-    double sXL[4][NT];
-    double sF[4][NT];
+    double2 sP[2][NT];
+    double2 sXL[2][NT];
+    double2 sF[2][NT];
     uint64_t bar[kRing];
     uint64_t bar0[kRing0];
     unsigned long long wmax[NT / 32];
@@ -905,6 +940,7 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
     constexpr int RD = 4 * NT;
     constexpr unsigned RB = RD * sizeof(double);
     unsigned long long cbest = 0ull;
+    const bool unit = !THREE && c1 == 1.0 && c2 == 1.0;
 
     const double dt = tm->dt;
     const double dtdx = dt * g.dxRec, dtdy = dt * g.dyRec;
@@ -986,7 +1022,7 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
     for (int f = y0 + 1; f <= y1; ++f) {
         wait(f + 1);
         const W4 P1 = c2p4(rowq(f + 1), ph);
-        sm.sP[0][t] = Pm1.r; sm.sP[1][t] = Pm1.vx; sm.sP[2][t] = Pm1.vy; sm.sP[3][t] = Pm1.p;
+        sm.sP[0][t] = make_double2(Pm1.r, Pm1.vx); sm.sP[1][t] = make_double2(Pm1.vy, Pm1.p);
         __syncthreads();
         if (t == 0) {
             // raw row f-2 and base-state row f-2 were last read in iteration f-1
@@ -996,32 +1032,36 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
         }
         W4 xr = Pm1, wr = P0, wlNew = P0;
         if (PLM) {
-            const W4 a{sm.sP[0][tl], sm.sP[1][tl], sm.sP[2][tl], sm.sP[3][tl]};
-            const W4 c{sm.sP[0][tr], sm.sP[1][tr], sm.sP[2][tr], sm.sP[3][tr]};
+            const double2 a0 = sm.sP[0][tl], a1 = sm.sP[1][tl];
+            const double2 c0 = sm.sP[0][tr], c1v = sm.sP[1][tr];
+            const W4 a{a0.x, a0.y, a1.x, a1.y};
+            const W4 c{c0.x, c0.y, c1v.x, c1v.y};
             const W4 sx = vl4(a, Pm1, c);
             const W4 sy = vl4(Pm1, P0, P1);
             const W4 xlft = plus_half(Pm1, sx);
             xr = minus_half(Pm1, sx);
             wr = minus_half(P0, sy);
             wlNew = plus_half(P0, sy);
-            sm.sXL[0][t] = xlft.r; sm.sXL[1][t] = xlft.vx; sm.sXL[2][t] = xlft.vy; sm.sXL[3][t] = xlft.p;
+            sm.sXL[0][t] = make_double2(xlft.r, xlft.vx); sm.sXL[1][t] = make_double2(xlft.vy, xlft.p);
         } else {
-            sm.sXL[0][t] = Pm1.r; sm.sXL[1][t] = Pm1.vx; sm.sXL[2][t] = Pm1.vy; sm.sXL[3][t] = Pm1.p;
+            sm.sXL[0][t] = make_double2(Pm1.r, Pm1.vx); sm.sXL[1][t] = make_double2(Pm1.vy, Pm1.p);
         }
         __syncthreads();
-        const W4 xl_state{sm.sXL[0][tl], sm.sXL[1][tl], sm.sXL[2][tl], sm.sXL[3][tl]};
+        const double2 x0v = sm.sXL[0][tl], x1v = sm.sXL[1][tl];
+        const W4 xl_state{x0v.x, x0v.y, x1v.x, x1v.y};
         Flux5 fx, fy;
         hllc_x(xl_state, xr, ph, fx);
         hllc_y(wlNext, wr, ph, fy);
-        sm.sF[0][t] = fx.d; sm.sF[1][t] = fx.n; sm.sF[2][t] = fx.t1; sm.sF[3][t] = fx.e;
+        sm.sF[0][t] = make_double2(fx.d, fx.n); sm.sF[1][t] = make_double2(fx.t1, fx.e);
         __syncthreads();
         if (THREE) wait0(f - 1);
         if (do_cell) {
             const Q4 Qm1 = rowq(f - 1);
-            double dF0 = (sm.sF[0][tr] - fx.d) * dtdx + (fy.d - fyPrev.d) * dtdy;
-            double dF1 = (sm.sF[1][tr] - fx.n) * dtdx + (fy.t1 - fyPrev.t1) * dtdy;
-            double dF2 = (sm.sF[2][tr] - fx.t1) * dtdx + (fy.n - fyPrev.n) * dtdy;
-            double dF3 = (sm.sF[3][tr] - fx.e) * dtdx + (fy.e - fyPrev.e) * dtdy;
+            const double2 fr0 = sm.sF[0][tr], fr1 = sm.sF[1][tr];
+            double dF0 = (fr0.x - fx.d) * dtdx + (fy.d - fyPrev.d) * dtdy;
+            double dF1 = (fr0.y - fx.n) * dtdx + (fy.t1 - fyPrev.t1) * dtdy;
+            double dF2 = (fr1.x - fx.t1) * dtdx + (fy.n - fyPrev.n) * dtdy;
+            double dF3 = (fr1.y - fx.e) * dtdx + (fy.e - fyPrev.e) * dtdy;
             double r[4];
             if (THREE) {
                 const Q4 U0 = rowq0(f - 1);
@@ -1029,13 +1069,19 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
                 r[1] = c1 * U0.mx + c2 * Qm1.mx - c3 * dF1;
                 r[2] = c1 * U0.my + c2 * Qm1.my - c3 * dF2;
                 r[3] = c1 * U0.e + c2 * Qm1.e - c3 * dF3;
+            } else if (unit) {
+                // c1 = c2 = 1 (every integrator's first stage): the products are exact
+                r[0] = Qm1.d - dF0;
+                r[1] = Qm1.mx - dF1;
+                r[2] = Qm1.my - dF2;
+                r[3] = Qm1.e - dF3;
             } else {
                 r[0] = c1 * Qm1.d - c2 * dF0;
                 r[1] = c1 * Qm1.mx - c2 * dF1;
                 r[2] = c1 * Qm1.my - c2 * dF2;
                 r[3] = c1 * Qm1.e - c2 * dF3;
             }
-            floors4(r, ph);
+            const double invk = floors4_inv(r, ph);  // r[0] >= dmin after it
             if (LAST) {
                 if (ph.has_grav) {
                     const double hdt = 0.5 * dt;
@@ -1048,7 +1094,7 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
                         r[2] += r[0] * ph.grav[1] * hdt;
                     }
                 }
-                const double local = cell_cmax(r[0], r[1], r[2], 0.0, r[3], ph, false);
+                const double local = cell_cmax_inv(r[1], r[2], r[3], invk, ph);
                 const unsigned long long b = (unsigned long long)__double_as_longlong(local);
                 cbest = b > cbest ? b : cbest;
             }
