@@ -310,14 +310,17 @@ int choose_path(const gk_handle* h) {
 }
 
 // Rows per tile of the fused 2D stage: enough tiles for every resident CTA
-// slot (148 SMs x 4), at most 32 rows (each tile repeats a 4-row prologue;
-// KH 4096^2 ran 1% faster at 20-48 rows than at 16, flat beyond 20).
+// slot (148 SMs x 4), at most 24 rows.  Each tile repeats a 4-row prologue,
+// so longer tiles do less work; but few waves of tiles leave a tail.
+// Measured (G zone-updates/s, 16 / 24 / 32 rows): KH 4096^2 fast 17.6 /
+// 17.8 / 17.8, parity 7.37 / 7.40 / 7.31; RT 1024x3072 (9 strips) fast
+// 9.10 / 9.10 / 9.04, parity 4.09 / 4.01 / 3.45 (1.5 waves at 32 rows).
 int stage_rows(const gk::Geom& g) {
     int forced = env_int("GK_STAGE_ROWS", 0);
     if (forced > 0) return forced;
     long long strips = (g.nx + 123) / 124;
     long long per_slot = (long long)g.ny * strips / (148 * 4);
-    return (int)std::max(4LL, std::min(32LL, per_slot));
+    return (int)std::max(4LL, std::min(24LL, per_slot));
 }
 
 // One time step.  Kernel order per RK stage follows Sim::RK2_/RK3_/
