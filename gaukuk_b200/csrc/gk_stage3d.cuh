@@ -5,10 +5,10 @@
 // z-face states with ReconstructYZPLM, whose slope is along y
 // (recon_piecewise_linear.cpp:29-50): the left state of face (k-1|k) is the
 // upper y state of cell (k-1, j), the right state the lower y state of cell
-// (k, j).  A thread owns a column i of one face plane and marches up a
-// segment of rows, converting the rows of the two planes to primitives once
-// (ConsToPrim, adiabatic.cpp:18-61) and keeping three rows of each in
-// registers.
+// (k, j).  A thread owns a column (i, j) and marches up a segment of faces,
+// converting each plane's three rows to primitives (ConsToPrim,
+// adiabatic.cpp:18-61) and sloping them once for the two faces the cell
+// touches.
 //
 // k_stage3d: one z-plane of the stage, as the fused 2D stage does it --
 // a CTA owns NT-4 columns plus a 2-cell halo, marches up a segment of rows,
@@ -92,42 +92,57 @@ __device__ __forceinline__ void hllc5_y(const double (&l)[5], const double (&r)[
 }
 
 // ------------------------------------------------------------ z faces
+// A thread owns column (i, j) and marches up a segment of zseg faces.  The
+// y-slope of cell (k, j) gives both its lower state (the right state of face
+// k-1|k) and its upper state (the left state of face k|k+1), so each plane's
+// three rows are converted and sloped once for two faces; the rows of the
+// next plane are in flight while a face is solved.  The expressions are
+// plm_up / plm_down's, so the fluxes are the same bits.
 template <bool PLM>
 __global__ void __launch_bounds__(128)
     k_zflux(const double* __restrict__ u, double* __restrict__ F3, Geom g, Phys ph,
-            const DevTime* __restrict__ tm, int rows) {
+            const DevTime* __restrict__ tm, int zseg) {
     if (!tm->active) return;
     const int i = g.ib + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.ie) return;
-    const int k = g.kb + blockIdx.z;  // face (k-1 | k), k = kb .. ke
-    const int y0 = g.jb + blockIdx.y * rows;
-    const int y1 = min(y0 + rows, g.je);
-    // rows j-1, j, j+1 of the planes below (L) and above (R) the face
-    W5 Lm = c2p_at(u, g, ph, sidx(g, k - 1, y0 - 1, i)), L0 = c2p_at(u, g, ph, sidx(g, k - 1, y0, i));
-    W5 Rm = c2p_at(u, g, ph, sidx(g, k, y0 - 1, i)), R0 = c2p_at(u, g, ph, sidx(g, k, y0, i));
-    Q5 qL = load5(u, g, sidx(g, k - 1, y0 + 1, i)), qR = load5(u, g, sidx(g, k, y0 + 1, i));
-    for (int j = y0; j < y1; ++j) {
-        // raw row j+2 in flight while row j+1 is converted and face j solved
-        Q5 nL = qL, nR = qR;
-        if (j + 2 <= y1) {
-            nL = load5(u, g, sidx(g, k - 1, j + 2, i));
-            nR = load5(u, g, sidx(g, k, j + 2, i));
-        }
-        const W5 Lp = c2p_q(qL, ph);
-        const W5 Rp = c2p_q(qR, ph);
-        qL = nL;
-        qR = nR;
-        double wl[5], wr[5];
+    const int j = g.jb + blockIdx.y;
+    const int k0 = g.kb + blockIdx.z * zseg;    // first face (k0-1 | k0)
+    const int k1 = min(k0 + zseg, g.ke + 1);    // one past the last face
+    // rows j-1, j, j+1 of plane k (ghost rows and planes included)
+    auto plane = [&](int k, Q5 (&q)[3]) {
+        const long long c = sidx(g, k, j, i);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            if (PLM) {
-                wl[v] = plm_up(Lm.v[v], L0.v[v], Lp.v[v]);
-                wr[v] = plm_down(Rm.v[v], R0.v[v], Rp.v[v]);
-            } else {
-                wl[v] = L0.v[v];
-                wr[v] = R0.v[v];
+        for (int r = 0; r < 3; ++r) q[r] = load5(u, g, c + (long long)(r - 1) * g.pitch);
+    };
+    // states of cell (k, j) from its plane's rows j-1, j, j+1
+    auto states = [&](const Q5 (&q)[3], double (&lo)[5], double (&up)[5]) {
+        const W5 b = c2p_q(q[1], ph);
+        if (PLM) {
+            const W5 a = c2p_q(q[0], ph), c = c2p_q(q[2], ph);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+#if GK_FASTMATH
+                const double h = vanleer_half(b.v[v] - a.v[v], c.v[v] - b.v[v]);
+#else
+                const double h = 0.5 * vanleer(b.v[v] - a.v[v], c.v[v] - b.v[v]);
+#endif
+                lo[v] = b.v[v] - h;
+                up[v] = b.v[v] + h;
             }
+        } else {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) lo[v] = up[v] = b.v[v];
         }
+    };
+    Q5 q[3];
+    double wl[5], wr[5], nu[5];
+    plane(k0 - 1, q);
+    states(q, wr, wl);  // the upper state of plane k0-1 is the first face's left state
+    plane(k0, q);
+    for (int k = k0; k < k1; ++k) {
+        const Q5 cur[3] = {q[0], q[1], q[2]};
+        if (k + 1 < k1) plane(k + 1, q);
+        states(cur, wr, nu);
         // z face: (vz | vx, vy)
         Flux5 f;
         hllc<true, kSel>(wl[gk::P_RHO], wl[gk::P_VZ], wl[gk::P_VX], wl[gk::P_VY], wl[gk::P_PRE],
@@ -138,8 +153,8 @@ __global__ void __launch_bounds__(128)
         F3[gk::S_MTX * g.fvstride + c] = f.t1;
         F3[gk::S_MTY * g.fvstride + c] = f.t2;
         F3[gk::S_ENG * g.fvstride + c] = f.e;
-        Lm = L0; L0 = Lp;
-        Rm = R0; R0 = Rp;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) wl[v] = nu[v];
     }
 }
 
