@@ -352,7 +352,10 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
     const double frac13 = 1.0 / 3.0;
     if (c.ph.has_grav || c.ph.npoint) GK_L(gk::K_KICK, k.kick(c, A, 0, s));
     if (h->path == 2) {
-        // z fluxes of the stage's state into F3, then the fused x-y stage
+        // z fluxes of the stage's state into F3, then the fused x-y stage;
+        // without a kick after it the last stage also reduces the CFL speed
+        const bool kicks = c.ph.has_grav || c.ph.npoint;
+        const int last = kicks ? 1 : 2;
         GK_L(gk::K_BC, k.bc(c, A, s));
         GK_L(gk::K_FLUX, k.zflux(c, A, h->F3, s));
         GK_L(gk::K_STAGE, k.stage3d(c, A, nullptr, B, h->F3, 0, 1.0, 1.0, 0.0, s));
@@ -362,12 +365,14 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
             GK_L(gk::K_STAGE, k.stage3d(c, B, A, Cb, h->F3, 1, 0.75, 0.25, 0.25, s));
             GK_L(gk::K_BC, k.bc(c, Cb, s));
             GK_L(gk::K_FLUX, k.zflux(c, Cb, h->F3, s));
-            GK_L(gk::K_STAGE, k.stage3d(c, Cb, A, A, h->F3, 1, frac13, 2 * frac13, 2 * frac13, s));
+            GK_L(gk::K_STAGE, k.stage3d(c, Cb, A, A, h->F3, last, frac13, 2 * frac13, 2 * frac13, s));
         } else {
-            GK_L(gk::K_STAGE, k.stage3d(c, B, A, A, h->F3, 1, 0.5, 0.5, 0.5, s));
+            GK_L(gk::K_STAGE, k.stage3d(c, B, A, A, h->F3, last, 0.5, 0.5, 0.5, s));
         }
-        if (c.ph.has_grav || c.ph.npoint) GK_L(gk::K_KICK, k.kick(c, A, 1, s));
-        GK_L(gk::K_CFL, k.cfl(c, A, 1, s));
+        if (kicks) {
+            GK_L(gk::K_KICK, k.kick(c, A, 1, s));
+            GK_L(gk::K_CFL, k.cfl(c, A, 1, s));
+        }
         return;
     }
     if (h->path == 1) {
@@ -883,11 +888,12 @@ int gk_graph_info(gk_handle* h, int* steps_per_graph, int* launches_per_step) {
     const gk::Ctx& c = h->ctx;
     const int stages = c.ph.integrator;  // 1, 2 or 3 stages
     int per;
-    const int inner = c.ph.fix_inner ? 1 : 0;  // inner reset after each ghost fill
+    // immersed body and inner reset after each ghost fill
+    const int inner = (c.ph.fix_inner ? 1 : 0) + (c.ph.nshell > 0 ? 1 : 0);
     if (h->path == 1) {
         per = (c.ph.has_grav ? 1 : 0) + (2 + inner) * stages;  // kick, (ghost fill + stage) per stage
     } else if (h->path == 2) {
-        per = (c.ph.has_grav || c.ph.npoint ? 2 : 0) + (3 + inner) * stages + 1;
+        per = (c.ph.has_grav || c.ph.npoint ? 3 : 0) + (3 + inner) * stages;
     } else {
         per = (c.ph.has_grav || c.ph.npoint ? 2 : 0) + stages * (3 + inner + c.g.ndim) + 1;
     }

@@ -1283,19 +1283,22 @@ void launch_zflux(const Ctx& c, const double* u, double* F3, cudaStream_t s) {
 
 template <int NT>
 static void launch_stage3d_nt(const Ctx& c, const double* uc, const double* u0, double* out,
-                              const double* F3, bool three, double c1, double c2, double c3,
+                              const double* F3, int three, double c1, double c2, double c3,
                               cudaStream_t s) {
     const Geom& g = c.g;
     const int rows = stage3d_rows(g);
     dim3 grid((g.nx + NT - 5) / (NT - 4), (g.ny + rows - 1) / rows, g.nz);
-#define GK_S3(TH, PL) \
-    k_stage3d<NT, TH, PL><<<grid, NT, 0, s>>>(uc, u0, out, F3, g, c.ph, c1, c2, c3, c.tm, rows)
-    if (three) {
-        if (c.ph.plm) GK_S3(true, true);
-        else GK_S3(true, false);
+#define GK_S3(TH, PL, LA) \
+    k_stage3d<NT, TH, PL, LA><<<grid, NT, 0, s>>>(uc, u0, out, F3, g, c.ph, c1, c2, c3, c.tm, rows)
+    if (three == 2) {
+        if (c.ph.plm) GK_S3(true, true, true);
+        else GK_S3(true, false, true);
+    } else if (three) {
+        if (c.ph.plm) GK_S3(true, true, false);
+        else GK_S3(true, false, false);
     } else {
-        if (c.ph.plm) GK_S3(false, true);
-        else GK_S3(false, false);
+        if (c.ph.plm) GK_S3(false, true, false);
+        else GK_S3(false, false, false);
     }
 #undef GK_S3
 }
@@ -1303,9 +1306,9 @@ static void launch_stage3d_nt(const Ctx& c, const double* uc, const double* u0, 
 void launch_stage3d(const Ctx& c, const double* uc, const double* u0, double* out, const double* F3,
                     int three, double c1, double c2, double c3, cudaStream_t s) {
     switch (stage3d_nt(c.g)) {
-        case 64: launch_stage3d_nt<64>(c, uc, u0, out, F3, three != 0, c1, c2, c3, s); break;
-        case 96: launch_stage3d_nt<96>(c, uc, u0, out, F3, three != 0, c1, c2, c3, s); break;
-        default: launch_stage3d_nt<128>(c, uc, u0, out, F3, three != 0, c1, c2, c3, s); break;
+        case 64: launch_stage3d_nt<64>(c, uc, u0, out, F3, three, c1, c2, c3, s); break;
+        case 96: launch_stage3d_nt<96>(c, uc, u0, out, F3, three, c1, c2, c3, s); break;
+        default: launch_stage3d_nt<128>(c, uc, u0, out, F3, three, c1, c2, c3, s); break;
     }
 }
 

@@ -161,13 +161,17 @@ __global__ void __launch_bounds__(128)
 // ------------------------------------------------------------ x-y plane stage
 // THREE = false: out = c1*uc - c2*dF (stage 1); true: out = c1*u0 + c2*uc -
 // c3*dF.  out never aliases uc (neighbours of uc are read while out is
-// written); u0 may alias out (read pointwise, before the write).
-template <int NT, bool THREE, bool PLM>
-__global__ void __launch_bounds__(NT, 2)
+// written); u0 may alias out (read pointwise, before the write).  LAST: the
+// step's last stage also reduces the CFL speed of the new state (CalCmax,
+// adiabatic.cpp:115-160, on the values it writes) and its last CTA runs the
+// step epilogue, as k_cfl would after it.
+template <int NT, bool THREE, bool PLM, bool LAST>
+__global__ void __launch_bounds__(NT, 384 / NT)
     k_stage3d(const double* __restrict__ uc, const double* u0, double* out,
               const double* __restrict__ F3, Geom g, Phys ph, double c1, double c2, double c3,
-              const DevTime* __restrict__ tm, int rows) {
+              DevTime* tm, int rows) {
     if (!tm->active) return;
+    unsigned long long cbest = 0ull;  // CFL speed of this thread's cells (bit pattern)
     __shared__ double sP[5][NT];
     __shared__ double sXL[5][NT];
     __shared__ double sF[5][NT];
@@ -253,6 +257,12 @@ __global__ void __launch_bounds__(NT, 2)
                 else r[v] = c1 * uc[v * g.vstride + c] - c2 * dF;
             }
             floors5(r, ph);
+            if (LAST) {
+                const double local = cell_cmax(r[gk::S_DEN], r[gk::S_MTX], r[gk::S_MTY],
+                                               r[gk::S_MTZ], r[gk::S_ENG], ph, true);
+                const unsigned long long b = (unsigned long long)__double_as_longlong(local);
+                cbest = b > cbest ? b : cbest;
+            }
 #pragma unroll
             for (int v = 0; v < 5; ++v) out[v * g.vstride + c] = r[v];
         }
@@ -263,5 +273,28 @@ __global__ void __launch_bounds__(NT, 2)
         }
         Pm1 = P0;
         P0 = P1;
+    }    if (LAST) {
+        __shared__ unsigned long long wmax[NT / 32];
+        __shared__ int last;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long x = __shfl_xor_sync(0xffffffffu, cbest, o);
+            cbest = x > cbest ? x : cbest;
+        }
+        if ((t & 31) == 0) wmax[t >> 5] = cbest;
+        __syncthreads();
+        if (t == 0) {
+            unsigned long long m = wmax[0];
+            for (int w = 1; w < NT / 32; ++w) m = wmax[w] > m ? wmax[w] : m;
+            atomicMax(&tm->cmax_acc, m);
+            __threadfence();
+            const unsigned total = gridDim.x * gridDim.y * gridDim.z;
+            last = atomicAdd(&tm->done_ctas, 1u) == total - 1;
+        }
+        __syncthreads();
+        if (last && t == 0) {
+            __threadfence();
+            step_epilogue(tm, g, ph, 1);
+        }
     }
 }
