@@ -89,3 +89,30 @@ def build_host(verbose: bool = False, force: bool = False) -> None:
         src = os.path.join(REFERENCE_SRC, "src", "setup", f"setup_{name}.cpp")
         if os.path.exists(src):
             build_hook(src, name="ref_" + name, verbose=verbose, force=force)
+
+
+SANITIZE = ["-O1", "-g", "-fno-omit-frame-pointer", "-fsanitize=address,undefined",
+            "-fno-sanitize-recover=undefined"]
+
+
+def build_sanitized(hooks: List[str], out_dir: str, verbose: bool = False) -> List[str]:
+    """The host layer under AddressSanitizer and UndefinedBehaviorSanitizer:
+    compiles its sources once into out_dir and links one driver per hook
+    (``<out_dir>/gaukuk_<name>.asan``) against lib/libgk_cuda.so.  Strict IEEE
+    flags are kept, so the drivers write the same frames as the plain ones."""
+    build_cuda(verbose=verbose)
+    os.makedirs(out_dir, exist_ok=True)
+    flags = [f for f in CXXFLAGS if f != "-O2"] + SANITIZE
+    objs = []
+    for rel in HOST_SRCS + ["main.cpp"]:
+        obj = os.path.join(out_dir, rel.replace("/", "_").replace(".cpp", ".o"))
+        _run([CXX] + flags + ["-c", os.path.join(SRC, rel), "-o", obj], verbose)
+        objs.append(obj)
+    exes = []
+    for hook in hooks:
+        name = os.path.basename(hook)[len("setup_"):-len(".cpp")]
+        exe = os.path.join(out_dir, f"gaukuk_{name}.asan")
+        _run([CXX] + flags + ["-I-", "-I" + SETUP, "-o", exe, hook] + objs +
+             ["-L" + LIB, "-lgk_cuda", "-Wl,-rpath," + LIB], verbose)
+        exes.append(exe)
+    return exes
