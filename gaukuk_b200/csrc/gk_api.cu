@@ -19,6 +19,7 @@
 #include <vector>
 
 #include <cudaTypedefs.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "gaukuk_cuda.h"
 #include "gk_internal.h"
@@ -135,6 +136,15 @@ struct gk_handle {
 };
 
 namespace {
+
+// An NVTX range over a public call (visible in Nsight timelines; free when
+// no tool is attached).
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
 
 int fail(gk_handle* h, int code, const std::string& msg) {
     if (h) h->err = msg;
@@ -585,6 +595,7 @@ long long gk_state_size(const gk_handle* h) {
 }
 
 int gk_upload_cons(gk_handle* h, const double* cons) {
+    Range range("gk_upload_cons");
     if (!h || !cons) return GK_ERR_INVALID;
     GK_CUDA(h, cudaSetDevice(h->device));
     const gk::Geom& g = h->ctx.g;
@@ -661,6 +672,7 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
 }
 
 static int download(gk_handle* h, double* cons, bool zero_other_planes) {
+    Range range("gk_download");
     int rc = check_ready(h);
     if (rc != GK_OK) return rc;
     if (!cons) return GK_ERR_INVALID;
@@ -786,6 +798,7 @@ static int run_loop(gk_handle* h, double dtoutput, int nsteps, bool wait) {
 }
 
 int gk_advance(gk_handle* h, double dtoutput, double* t, int* step, int* is_continue) {
+    Range range("gk_advance");
     int rc = check_ready(h);
     if (rc != GK_OK) return rc;
     rc = run_loop(h, dtoutput, 0, true);
@@ -798,6 +811,7 @@ int gk_advance(gk_handle* h, double dtoutput, double* t, int* step, int* is_cont
 }
 
 int gk_run_steps(gk_handle* h, int nsteps, int* done) {
+    Range range("gk_run_steps");
     int rc = check_ready(h);
     if (rc != GK_OK) return rc;
     if (nsteps <= 0) {
@@ -815,6 +829,7 @@ int gk_run_steps(gk_handle* h, int nsteps, int* done) {
 }
 
 int gk_enqueue_steps(gk_handle* h, int nsteps) {
+    Range range("gk_enqueue_steps");
     int rc = check_ready(h);
     if (rc != GK_OK) return rc;
     if (nsteps <= 0) return GK_OK;
@@ -1195,17 +1210,20 @@ int gk_ens_set_tiling(gk_ensemble* e, int threads, const int* rows) {
 }
 
 int gk_ens_advance(gk_ensemble* e, double dtoutput) {
+    Range range("gk_ens_advance");
     if (!e) return GK_ERR_INVALID;
     return ens_run(e, dtoutput, 0, true);
 }
 
 int gk_ens_run_steps(gk_ensemble* e, int nsteps) {
+    Range range("gk_ens_run_steps");
     if (!e) return GK_ERR_INVALID;
     if (nsteps <= 0) return GK_OK;
     return ens_run(e, 0.0, nsteps, true);
 }
 
 int gk_ens_enqueue_steps(gk_ensemble* e, int nsteps) {
+    Range range("gk_ens_enqueue_steps");
     if (!e) return GK_ERR_INVALID;
     if (nsteps <= 0) return GK_OK;
     return ens_run(e, 0.0, nsteps, false);
