@@ -44,6 +44,8 @@ SIGNATURES = {
     "gk_upload_cons": (ctypes.c_int, [_vp, _vp]),
     "gk_download_cons": (ctypes.c_int, [_vp, _vp]),
     "gk_download_planes": (ctypes.c_int, [_vp, _vp]),
+    "gk_floor_hits": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_ulonglong),
+                                     ctypes.POINTER(ctypes.c_ulonglong)]),
     "gk_io_bytes": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong),
                                    ctypes.POINTER(ctypes.c_longlong)]),
     "gk_advance": (ctypes.c_int, [_vp, ctypes.c_double, _dp, _ip, _ip]),

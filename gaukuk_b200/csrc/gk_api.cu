@@ -655,6 +655,8 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
     gk::DevTime t = *h->htm;
     double seed = 1e-16;
     std::memcpy(&t.cmax_acc, &seed, sizeof(double));
+    t.floor_den = 0;
+    t.floor_pre = 0;
     t.done_ctas = 0;
     t.status = 0;
     t.nlog = 0;
@@ -766,6 +768,15 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
 
 int gk_download_cons(gk_handle* h, double* cons) { return download(h, cons, true); }
 int gk_download_planes(gk_handle* h, double* cons) { return download(h, cons, false); }
+
+int gk_floor_hits(gk_handle* h, unsigned long long* density, unsigned long long* pressure) {
+    if (!h) return GK_ERR_INVALID;
+    int rc = pull_time(h);
+    if (rc != GK_OK) return rc;
+    if (density) *density = h->htm->floor_den;
+    if (pressure) *pressure = h->htm->floor_pre;
+    return GK_OK;
+}
 
 int gk_io_bytes(const gk_handle* h, long long* upload, long long* download) {
     if (!h) return GK_ERR_INVALID;

@@ -99,6 +99,9 @@ struct DevTime {
     int steps_left;                   // step budget (-1 = none)
     int nlog, log_cap;
     double* log;                      // dt of each step
+    // cells the floors repaired since the last upload (update_cons.cpp:55-68):
+    // density below the floor (vacuum reset), pressure below it (energy reset)
+    unsigned long long floor_den, floor_pre;
 };
 
 enum { STATUS_NONFINITE = 1, STATUS_TMA_TIMEOUT = 2 };

@@ -288,60 +288,72 @@ __global__ void k_flux(const double* __restrict__ w, double* __restrict__ F, Geo
 // ------------------------------------------------------------ UpdateCons
 // Sim::UpdateCons, both overloads (update_cons.cpp:11-133, 135-269).
 // update_cons.cpp:55-68, five slots (DEN, MTX, MTY, ENG, MTZ).
-__device__ __forceinline__ void floors5(double (&r)[5], const Phys& ph) {
+__device__ __forceinline__ void floors5(double (&r)[5], const Phys& ph, DevTime* tm) {
     if (r[gk::S_DEN] < ph.dmin) {
         r[gk::S_DEN] = ph.dmin;
         r[gk::S_MTX] = 0.0;
         r[gk::S_MTY] = 0.0;
         r[gk::S_MTZ] = 0.0;
         r[gk::S_ENG] = ph.pmin / ph.gm1 + 0.0;
+        atomicAdd(&tm->floor_den, 1ull);
     } else {
         double inv_den = GK_RCP(r[gk::S_DEN]);
         double ke = 0.5 * inv_den *
                     (r[gk::S_MTX] * r[gk::S_MTX] + r[gk::S_MTY] * r[gk::S_MTY] +
                      r[gk::S_MTZ] * r[gk::S_MTZ]);
         double press = ph.gm1 * (r[gk::S_ENG] - ke);
-        if (press < ph.pmin) r[gk::S_ENG] = ph.pmin / ph.gm1 + ke;
+        if (press < ph.pmin) {
+            r[gk::S_ENG] = ph.pmin / ph.gm1 + ke;
+            atomicAdd(&tm->floor_pre, 1ull);
+        }
     }
 }
 
 // The same with mz = 0 (four slots DEN, MTX, MTY, ENG): the mz terms are
 // exact zeros.
-__device__ __forceinline__ void floors4(double (&r)[4], const Phys& ph) {
+__device__ __forceinline__ void floors4(double (&r)[4], const Phys& ph, DevTime* tm) {
     if (r[0] < ph.dmin) {
         r[0] = ph.dmin;
         r[1] = 0.0;
         r[2] = 0.0;
         r[3] = ph.pmin / ph.gm1 + 0.0;
+        atomicAdd(&tm->floor_den, 1ull);
     } else {
         double inv_den = GK_RCP(r[0]);
         double ke = 0.5 * inv_den * (r[1] * r[1] + r[2] * r[2]);
         double press = ph.gm1 * (r[3] - ke);
-        if (press < ph.pmin) r[3] = ph.pmin / ph.gm1 + ke;
+        if (press < ph.pmin) {
+            r[3] = ph.pmin / ph.gm1 + ke;
+            atomicAdd(&tm->floor_pre, 1ull);
+        }
     }
 }
 
 // floors4 that also returns the reciprocal density of the result (for the
 // CFL speed of the same cell).
-__device__ __forceinline__ double floors4_inv(double (&r)[4], const Phys& ph) {
+__device__ __forceinline__ double floors4_inv(double (&r)[4], const Phys& ph, DevTime* tm) {
     if (r[0] < ph.dmin) {
         r[0] = ph.dmin;
         r[1] = 0.0;
         r[2] = 0.0;
         r[3] = ph.pmin / ph.gm1 + 0.0;
+        atomicAdd(&tm->floor_den, 1ull);
         return GK_RCP(ph.dmin);
     }
     double inv_den = GK_RCP(r[0]);
     double ke = 0.5 * inv_den * (r[1] * r[1] + r[2] * r[2]);
     double press = ph.gm1 * (r[3] - ke);
-    if (press < ph.pmin) r[3] = ph.pmin / ph.gm1 + ke;
+    if (press < ph.pmin) {
+        r[3] = ph.pmin / ph.gm1 + ke;
+        atomicAdd(&tm->floor_pre, 1ull);
+    }
     return inv_den;
 }
 
 __global__ void k_update(const double* u0, const double* uc, double* out,
                          const double* __restrict__ F1, const double* __restrict__ F2,
                          const double* __restrict__ F3, Geom g, Phys ph, int three, double c1,
-                         double c2, double c3, const DevTime* __restrict__ tm) {
+                         double c2, double c3, DevTime* tm) {
     if (!tm->active) return;
     const int i = g.ib + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = g.jb + blockIdx.y;
@@ -364,7 +376,7 @@ __global__ void k_update(const double* u0, const double* uc, double* out,
         if (three) r[v] = c1 * u0[v * g.vstride + c] + c2 * uc[v * g.vstride + c] - c3 * dF;
         else r[v] = c1 * uc[v * g.vstride + c] - c2 * dF;
     }
-    floors5(r, ph);
+    floors5(r, ph, tm);
 #pragma unroll
     for (int v = 0; v < 5; ++v) out[v * g.vstride + c] = r[v];
 }
@@ -784,7 +796,7 @@ __global__ void __launch_bounds__(kStageThreads, 3)
                 r[2] = c1 * Qm1.my - c2 * dF2;
                 r[3] = c1 * Qm1.e - c2 * dF3;
             }
-            floors4(r, ph);
+            floors4(r, ph, tm);
             if (LAST) {
                 if (ph.has_grav) {
                     // SourceTerm::ConstGravity with dt/2 (const_gravity.cpp:28-46)
@@ -1081,7 +1093,7 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
                 r[2] = c1 * Qm1.my - c2 * dF2;
                 r[3] = c1 * Qm1.e - c2 * dF3;
             }
-            const double invk = floors4_inv(r, ph);  // r[0] >= dmin after it
+            const double invk = floors4_inv(r, ph, tm);  // r[0] >= dmin after it
             if (LAST) {
                 if (ph.has_grav) {
                     const double hdt = 0.5 * dt;

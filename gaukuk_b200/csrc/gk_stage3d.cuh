@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(NT, 384 / NT)
                 if (THREE) r[v] = c1 * u0[v * g.vstride + c] + c2 * uc[v * g.vstride + c] - c3 * dF;
                 else r[v] = c1 * uc[v * g.vstride + c] - c2 * dF;
             }
-            floors5(r, ph);
+            floors5(r, ph, tm);
             if (LAST) {
                 const double local = cell_cmax(r[gk::S_DEN], r[gk::S_MTX], r[gk::S_MTY],
                                                r[gk::S_MTZ], r[gk::S_ENG], ph, true);

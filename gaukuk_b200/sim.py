@@ -88,6 +88,12 @@ class Sim:
         _lib.check(fn(self.h, out.ctypes.data_as(ctypes.c_void_p)), self.h)
         return out
 
+    def floor_hits(self) -> Tuple[int, int]:
+        """Cells whose density / pressure the floors repaired since the last upload."""
+        d, p = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        _lib.check(self._L.gk_floor_hits(self.h, ctypes.byref(d), ctypes.byref(p)), self.h)
+        return d.value, p.value
+
     def io_bytes(self) -> Tuple[int, int]:
         """Bytes the last upload and the last download moved across the bus."""
         up, down = ctypes.c_longlong(), ctypes.c_longlong()

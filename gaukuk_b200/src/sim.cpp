@@ -11,6 +11,7 @@
 // (sim.cpp:100-103) are printed afterwards from the device's dt log, with
 // t accumulated in the same order, so they read the same.
 #include <algorithm>
+#include <chrono>
 #include <iostream>
 #include <stdexcept>
 #include <string>
@@ -157,6 +158,7 @@ void Sim::Advance(Real dtoutput) {
     EnsureDevice();
     const int step0 = step;
     const Real t0 = t;
+    const auto wall0 = std::chrono::steady_clock::now();
     Check(dev_, gk_set_time(dev_, t, step), "gk_set_time");
     Check(dev_, gk_upload_cons(dev_, cons.data()), "gk_upload_cons");
     double tt = t;
@@ -174,6 +176,14 @@ void Sim::Advance(Real dtoutput) {
     }
     Check(dev_, rc, "gk_advance");
     Check(dev_, gk_download_cons(dev_, cons.data()), "gk_download_cons");
+    last_ = AdvanceStats{};
+    last_.steps = st - step0;
+    last_.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
+    if (!dts.empty()) {
+        last_.dt_min = *std::min_element(dts.begin(), dts.end());
+        last_.dt_max = *std::max_element(dts.begin(), dts.end());
+    }
+    Check(dev_, gk_floor_hits(dev_, &last_.floor_density, &last_.floor_pressure), "gk_floor_hits");
     if ((st - step0) % 2 != 0) SwapUnwritten();
     double tdev = 0, dtdev = 0;
     int sdev = 0, cdev = 1;

@@ -7,9 +7,10 @@
 // goes to the device at the start of the call and comes back at the end, so
 // cons always holds the current state between calls.
 //
-// Two .in keys beyond the reference's select the device: gpuMode (0 =
-// bit-identical to the reference built with strict IEEE flags, the default;
-// 1 = fast mode, within 1e-12) and gpuDevice (CUDA ordinal, default 0).
+// Keys beyond the reference's: gpuMode (0 = bit-identical to the reference
+// built with strict IEEE flags, the default; 1 = fast mode, within 1e-12),
+// gpuDevice (CUDA ordinal, default 0) and metrics (1: main appends one JSON
+// line per output interval to metrics.jsonl, from LastAdvance()).
 #pragma once
 
 #include <cstddef>
@@ -63,12 +64,23 @@ public:
     Real Getdt() { return dt; }
     int GetStep() { return step; }
 
+    // What the last Advance did: steps, host wall time around the device
+    // call (upload, steps, download), the smallest and largest dt, and the
+    // cells the floors repaired (density, pressure).
+    struct AdvanceStats {
+        int steps = 0;
+        double seconds = 0, dt_min = 0, dt_max = 0;
+        unsigned long long floor_density = 0, floor_pressure = 0;
+    };
+    const AdvanceStats& LastAdvance() const { return last_; }
+
 private:
     int step, stepMax;
     Real t, dt, dtUntilOutput, cmax, CFL;
     int rcOrder, integratorType;
     int gpuMode_, gpuDevice_;
     gk_handle* dev_ = nullptr;
+    AdvanceStats last_;
     void EnsureDevice();
     // Cells that no ghost fill or update writes (corner and edge ghosts,
     // ghost rows of unused directions) and consTemp's values of them.

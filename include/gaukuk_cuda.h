@@ -148,6 +148,13 @@ int gk_download_cons(gk_handle* h, double* cons);
  * has the same bits there. */
 int gk_download_planes(gk_handle* h, double* cons);
 
+/* Cells the floors repaired since the last upload (Sim::UpdateCons,
+ * update_cons.cpp:55-68): density below the floor (the cell is reset to
+ * vacuum) and pressure below it (the energy is reset).  The reference
+ * repairs silently; these count every stage's repairs.  Either pointer may
+ * be NULL. */
+int gk_floor_hits(gk_handle* h, unsigned long long* density, unsigned long long* pressure);
+
 /* Bytes the last gk_upload_cons and the last download moved across the bus
  * (either pointer may be NULL). */
 int gk_io_bytes(const gk_handle* h, long long* upload, long long* download);

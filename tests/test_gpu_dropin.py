@@ -157,3 +157,24 @@ def test_zero_z_momentum_plane_stays_on_the_host():
         out = np.full(p.shape, 7.0)
         s.download(out, planes_only=True)
         assert out[3, k, 0, 0] == 1.0 and out[3, k, p.ng, p.ng] == 0.0
+
+
+def test_metrics_log_matches_the_run(tmp_path):
+    """With metrics = 1 the driver appends one JSON line per output interval:
+    the steps add up to the run's, t is the frame time, the dt range brackets
+    the printed steps' dt, and a smooth KH run repairs no cell."""
+    import json
+    p, extra = CASES["kh_baseline"]
+    (tmp_path / "run.in").write_text(p.to_in_text(dict(extra, metrics=1)))
+    out = _run(os.path.join(BIN, "gaukuk_kh_baseline.sim"), ["-i", "run.in"], tmp_path)
+    recs = [json.loads(l) for l in (tmp_path / "metrics.jsonl").read_text().splitlines()]
+    steps = _steps(out)
+    dts = [float(l.split("dt =")[1]) for l in steps]
+    assert [r["output"] for r in recs] == list(range(1, len(recs) + 1)) and len(recs) >= 3
+    assert sum(r["steps"] for r in recs) == len(steps) == recs[-1]["step"]
+    assert abs(recs[-1]["t"] - p.tmax) < 1e-12
+    for r in recs:
+        assert r["zone_updates_per_s"] > 0 and r["floor_density"] == r["floor_pressure"] == 0
+        assert r["dt_min"] <= r["dt_max"]
+    assert min(r["dt_min"] for r in recs) <= min(dts) * (1 + 1e-5)
+    assert max(r["dt_max"] for r in recs) >= max(dts) * (1 - 1e-5)

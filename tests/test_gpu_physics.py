@@ -75,3 +75,30 @@ def test_kh256_to_t2_conserves():
         assert abs(a[v].sum() - a0[v].sum()) / a0[v].sum() < 1e-12, v
     for v in (1, 2):
         assert abs(a[v].sum() - a0[v].sum()) / a0[0].sum() < 1e-12, v
+
+
+@pytest.mark.parametrize("mode", ["parity", "fast"])
+def test_floor_repairs_are_counted(mode):
+    """Two streams rushing apart with a pressure (1e-20) below the floor
+    (1e-16): every stage repairs the cells whose pressure stays below it (the
+    reference does so silently) and gk_floor_hits counts them; the parity run
+    still equals the oracle bit for bit.  A smooth KH run repairs nothing."""
+    from gaukuk_b200.sim import Sim
+    p, _ = problems.sod(128)
+    x = (np.arange(p.nx) + 0.5) / p.nx
+    z = np.zeros(p.nx)
+    c = problems.prim_to_cons(p, np.ones(p.nx), np.where(x < 0.5, -3.0, 3.0), z, z,
+                              np.full(p.nx, 1e-20))
+    with Sim(p, c, mode=mode) as s:
+        s.run(0.02, 0.02)
+        den, pre = s.floor_hits()
+        got = s.download()
+    assert den + pre > 0 and np.isfinite(got).all()
+    if mode == "parity":
+        o = gk_oracle.OracleSim(p, c)
+        o.run(0.02, 0.02)
+        assert np.array_equal(active(p, got), active(p, o.get_cons()))
+    pk, ck = problems.kh(64)
+    with Sim(pk, ck, mode=mode) as s:
+        s.run_steps(20)
+        assert s.floor_hits() == (0, 0)
