@@ -527,6 +527,16 @@ int physics_changed(gk_handle* h) {
     return GK_OK;
 }
 
+// The device status word after a run: a TMA row wait that gave up (the
+// stage kernel's waits are bounded), or a non-finite CFL reduction.
+int status_error(gk_handle* h) {
+    const int st = h->htm->status;
+    if (st & gk::STATUS_TMA_TIMEOUT)
+        return fail(h, GK_ERR_CUDA, "a TMA row load did not complete within the stage kernel's wait limit");
+    if (st) return fail(h, GK_ERR_NONFINITE, "CFL reduction met a non-finite state");
+    return GK_OK;
+}
+
 int check_ready(gk_handle* h) {
     if (!h) return GK_ERR_INVALID;
     if (!h->uploaded) return fail(h, GK_ERR_STATE, "no state uploaded");
@@ -817,7 +827,7 @@ int gk_advance(gk_handle* h, double dtoutput, double* t, int* step, int* is_cont
     if (t) *t = h->htm->t;
     if (step) *step = h->htm->step;
     if (is_continue) *is_continue = h->htm->is_continue;
-    if (h->htm->status) return fail(h, GK_ERR_NONFINITE, "CFL reduction met a non-finite state");
+    if (h->htm->status) return status_error(h);
     return GK_OK;
 }
 
@@ -835,7 +845,7 @@ int gk_run_steps(gk_handle* h, int nsteps, int* done) {
     rc = run_loop(h, 0.0, nsteps, true);
     if (rc != GK_OK) return rc;
     if (done) *done = h->htm->step - before;
-    if (h->htm->status) return fail(h, GK_ERR_NONFINITE, "CFL reduction met a non-finite state");
+    if (h->htm->status) return status_error(h);
     return GK_OK;
 }
 
