@@ -94,15 +94,25 @@ def test_paths_selected():
     assert _sim(dataclasses.replace(p, integrator=1), c).path == "generic"  # Euler: in place
 
 
-def test_stage3d_equals_generic_path_bitwise(monkeypatch):
+@pytest.mark.parametrize("source", ["none", "gravity", "point"])
+def test_stage3d_equals_generic_path_bitwise(monkeypatch, source):
     """The 3D stage (z fluxes + fused x-y stage per plane) uses the generic
-    path's expressions: both give the same bits in parity mode."""
-    p = Params(nx=40, ny=36, nz=32, bc=(1, 3, 1, 1, 2, 1), integrator=3, tmax=1.0, dtoutput=1.0,
-               stepmax=6)
+    path's expressions: both give the same bits in parity mode.  Without a
+    source the last stage also reduces the CFL speed; with constant gravity
+    (RK2) or a point mass (RK3) the kick and a separate CFL pass follow it."""
+    integ = {"none": 3, "gravity": 2, "point": 3}[source]
+    grav = (0.05, -0.1, 0.08) if source == "gravity" else (0.0, 0.0, 0.0)
+    p = Params(nx=40, ny=36, nz=32, bc=(1, 3, 1, 1, 2, 1), integrator=integ, grav=grav,
+               tmax=1.0, dtoutput=1.0, stepmax=6)
     c = problems.random_smooth(p, seed=8, with_vz=True)
+    mass = [(0.5, 0.45, 0.5, 0.55, 0.1)]
     a = _sim(p, c)
-    monkeypatch.setenv("GK_STAGE3D", "0")
+    if source == "point":
+        a.set_point_gravity(mass)
+    monkeypatch.setenv("GK_STAGE3D", "0")  # read whenever the path is chosen
     b = _sim(p, c)
+    if source == "point":
+        b.set_point_gravity(mass)
     monkeypatch.delenv("GK_STAGE3D")
     assert a.path == "stage3d" and b.path == "generic"
     a.run(p.tmax, p.dtoutput)
