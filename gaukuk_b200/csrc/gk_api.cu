@@ -295,17 +295,36 @@ int env_int(const char* name, int dflt) {
     return v && *v ? std::atoi(v) : dflt;
 }
 
-// Threads per CTA of the TMA stage kernel: 128 unless GK_STAGE_THREADS says
-// 64 or 256 (tuning).
-int stage_threads_default() {
-    const int v = env_int("GK_STAGE_THREADS", 128);
-    return (v == 64 || v == 256) ? v : 128;
+// Tile shape of the fused 2D stage (threads per CTA, rows per tile), from the
+// grid: enough tiles for every resident CTA slot (148 SMs x 512/threads), at
+// most 24 rows.  Each tile repeats a 4-row prologue, so longer tiles do less
+// work; but few waves of tiles leave a tail, and a small grid needs short
+// tiles and narrow CTAs for every SM to get work.  Measured:
+//   KH 4096^2, 128 threads, G zone-updates/s at 16 / 24 / 32 rows: fast
+//   17.6 / 17.8 / 17.8, parity 7.37 / 7.40 / 7.31;
+//   RT 1024x3072 (9 strips), same: fast 9.10 / 9.10 / 9.04, parity 4.09 /
+//   4.01 / 3.45 (1.5 waves at 32 rows);
+//   KH 256^2, us per step, 128 threads x 4 rows -> 64 x 2: fast 24.2 -> 20.7,
+//   parity 52.8 -> 38.3; KH 512^2, 128 x 4 -> 64 x 4: fast 37.9 -> 33.4,
+//   parity 92.7 -> 63.4.
+// GK_STAGE_THREADS / GK_STAGE_ROWS override (tuning).
+int stage_threads_for(const gk::Geom& g) {
+    const int v = env_int("GK_STAGE_THREADS", 0);
+    if (v == 64 || v == 128 || v == 256) return v;
+    const long long strips = (g.nx + 123) / 124;
+    return (long long)g.ny * strips / (148 * 4) < 8 ? 64 : 128;
 }
 
-// Rows per CTA segment of the fused kernel.  Short segments (16 rows) give
-// many waves of CTAs, so no partial last wave dominates (measured on 4096^2:
-// 16-32 rows beat one wave of long segments by 1.5x); small grids use down
-// to 4 rows so that every SM gets work.  GK_STAGE_ROWS overrides (tuning).
+int stage_rows(const gk::Geom& g, int threads) {
+    const int forced = env_int("GK_STAGE_ROWS", 0);
+    if (forced > 0) return forced;
+    const long long cols = threads - 4;
+    const long long strips = (g.nx + cols - 1) / cols;
+    const long long slots = 148LL * (512 / threads);
+    const long long per_slot = ((long long)g.ny * strips + slots - 1) / slots;
+    return (int)std::max(2LL, std::min(24LL, per_slot));
+}
+
 // Path 1, the fused 2D stage, applies to 2D RK2/RK3 runs with MTZ
 // identically zero, no z gravity (it would make MTZ non-zero), no point
 // masses (their kicks run between the fused stages' CFL reduction and the
@@ -317,20 +336,6 @@ int choose_path(const gk_handle* h) {
     if (c.g.ndim == 3 && c.ph.integrator != 1 && env_int("GK_STAGE3D", 1) != 0) return 2;
     return (c.g.ndim == 2 && !c.has_vz && c.ph.integrator != 1 && c.ph.grav[2] == 0 &&
             c.ph.npoint == 0 && !h->model) ? 1 : 0;
-}
-
-// Rows per tile of the fused 2D stage: enough tiles for every resident CTA
-// slot (148 SMs x 4), at most 24 rows.  Each tile repeats a 4-row prologue,
-// so longer tiles do less work; but few waves of tiles leave a tail.
-// Measured (G zone-updates/s, 16 / 24 / 32 rows): KH 4096^2 fast 17.6 /
-// 17.8 / 17.8, parity 7.37 / 7.40 / 7.31; RT 1024x3072 (9 strips) fast
-// 9.10 / 9.10 / 9.04, parity 4.09 / 4.01 / 3.45 (1.5 waves at 32 rows).
-int stage_rows(const gk::Geom& g) {
-    int forced = env_int("GK_STAGE_ROWS", 0);
-    if (forced > 0) return forced;
-    long long strips = (g.nx + 123) / 124;
-    long long per_slot = (long long)g.ny * strips / (148 * 4);
-    return (int)std::max(4LL, std::min(24LL, per_slot));
 }
 
 // One time step.  Kernel order per RK stage follows Sim::RK2_/RK3_/
@@ -651,10 +656,13 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
     // immersed body writes MTZ (signed zeros in 2D) into its shell cells
     if (h->ctx.ph.npoint || h->ctx.ph.nshell) h->ctx.has_vz = 1;
     h->path = choose_path(h);
-    h->ctx.h2d_rows = stage_rows(g);
     h->ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
-    if (!h->tiling_set) h->ctx.stage_threads = stage_threads_default();
-    else h->ctx.h2d_rows = h->tiling_rows;
+    if (!h->tiling_set) {
+        h->ctx.stage_threads = stage_threads_for(g);
+        h->ctx.h2d_rows = stage_rows(g, h->ctx.stage_threads);
+    } else {
+        h->ctx.h2d_rows = h->tiling_rows;
+    }
     if (h->path != 1) {
         int rc = alloc_generic(h);
         if (rc != GK_OK) return rc;
@@ -1009,9 +1017,9 @@ int gk_internal_build_ctx(const gk_grid_desc* gd, const gk_phys_desc* pd, gk::Ct
         if (err) *err = tmp.err;
         return rc;
     }
-    tmp.ctx.h2d_rows = stage_rows(tmp.ctx.g);
     tmp.ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
-    tmp.ctx.stage_threads = stage_threads_default();
+    tmp.ctx.stage_threads = stage_threads_for(tmp.ctx.g);
+    tmp.ctx.h2d_rows = stage_rows(tmp.ctx.g, tmp.ctx.stage_threads);
     *ctx = tmp.ctx;
     return GK_OK;
 }
