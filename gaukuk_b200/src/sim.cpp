@@ -175,7 +175,10 @@ void Sim::Advance(Real dtoutput) {
                   << std::endl;
     }
     Check(dev_, rc, "gk_advance");
-    Check(dev_, gk_download_cons(dev_, cons.data()), "gk_download_cons");
+    // The planes the device does not hold (1D/2D: the unused z-planes) and an
+    // all-zero z-momentum plane on the fused 2D path are never written during
+    // Advance, here or by the reference, so cons keeps its own values there.
+    Check(dev_, gk_download_planes(dev_, cons.data()), "gk_download_planes");
     last_ = AdvanceStats{};
     last_.steps = st - step0;
     last_.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
