@@ -110,7 +110,11 @@ int main(int argc, char** argv) {
     int outputStep = 0;
     Real tnow = sim.GetTime();
     sim.boundary.UpdateBD(sim.cons, sim.grid, sim.domain, sim.eos);
-    if (frames) sim.WriteData(outputStep, DataType::Cons);
+    // the frame type of main.cpp:32-38 (dataType 1: primitives)
+    const DataType outputType = static_cast<int>(Config::getInstance().get("dataType", 0)) == 1
+                                    ? DataType::Prim
+                                    : DataType::Cons;
+    if (frames) sim.WriteData(outputStep, outputType);
 
     double seconds = 0.0;
     while (std::abs(tmax - tnow) > 1e-12 && sim.isContinue) {
@@ -121,7 +125,7 @@ int main(int argc, char** argv) {
         seconds += std::chrono::duration<double>(t1 - t0).count();
         tnow = sim.GetTime();
         outputStep++;
-        if (frames) sim.WriteData(outputStep, DataType::Cons);
+        if (frames) sim.WriteData(outputStep, outputType);
     }
     std::cout.clear();
     std::cout.flush();

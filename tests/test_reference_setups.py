@@ -147,3 +147,41 @@ def test_self_defined_sides_run_on_the_device_only_when_stationary(copies, tmp_p
         # past the probe: it runs on a GPU, or fails later for want of one
         assert not refused, r.stderr[-2000:]
         assert (tmp_path / "cons_00000").exists()
+
+
+PRIM_CASES = ["kh", "disk", "blast", "solid_body"]
+
+
+@pytest.mark.parametrize("name", PRIM_CASES)
+def test_first_prim_frame_matches_the_reference(name, tmp_path):
+    """dataType = 1 (main.cpp:32-38): frames hold the primitives from the
+    host ConsToPrim (adiabatic.cpp:18-61, floors included, every cell)."""
+    ref, ours = _exes(name)
+    p, extra = CASES[name]
+    import dataclasses
+    text = dataclasses.replace(p, tmax=0.0).to_in_text(dict(extra, dataType=1))
+    a, b = tmp_path / "ref", tmp_path / "ours"
+    a.mkdir(); b.mkdir()
+    (a / "run.in").write_text(text)
+    (b / "run.in").write_text(text)
+    _run(ref, ["-i", "run.in", "--frames", "--quiet"], a)
+    _run(ours, ["-i", "run.in"], b)
+    assert (a / "prim_00000").read_bytes() == (b / "prim_00000").read_bytes()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["kh", "blast", "solid_body"])
+def test_prim_runs_match_the_reference(name, tmp_path):
+    ref, ours = _exes(name)
+    p, extra = CASES[name]
+    text = p.to_in_text(dict(extra, dataType=1))
+    a, b = tmp_path / "ref", tmp_path / "gpu"
+    a.mkdir(); b.mkdir()
+    (a / "run.in").write_text(text)
+    (b / "run.in").write_text(text)
+    _run(ref, ["-i", "run.in", "--frames", "--quiet"], a)
+    _run(ours, ["-i", "run.in"], b)
+    names = sorted(f for f in os.listdir(a) if f.startswith("prim_"))
+    assert len(names) >= 3 and names == sorted(f for f in os.listdir(b) if f.startswith("prim_"))
+    for f in names:
+        assert (a / f).read_bytes() == (b / f).read_bytes(), f
