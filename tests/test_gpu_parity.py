@@ -214,37 +214,40 @@ def test_fastmath_refinements_within_error_bound():
     assert w[0] <= 2.0 and w[1] <= 2.0 and w[2] <= 2.0, list(w)
 
 
-def _extreme_state(n, with_vz, seed=0):
-    """A random 2D state at the edges of the scheme: densities log-uniform
-    in [1e-12, 1e2] with 2 % negative (the floor resets them), velocities up
-    to 10, pressures log-uniform in [1e-14, 10], and 5 % of the cells with
-    negative internal energy (the pressure floor), under mixed sides."""
-    p = Params(nx=n, ny=n, bc=(1, 3, 2, 0, 1, 1), integrator=2, tmax=1.0, dtoutput=1.0,
-               stepmax=3)
+def _extreme_state(n, with_vz, seed=0, nz=1):
+    """A random 2D or 3D state at the edges of the scheme: densities
+    log-uniform in [1e-12, 1e2] with 2 % negative (the floor resets them),
+    velocities up to 10, pressures log-uniform in [1e-14, 10], and 5 % of the
+    cells with negative internal energy (the pressure floor), under mixed
+    sides."""
+    p = Params(nx=n, ny=n, nz=nz, bc=(1, 3, 2, 0, 3, 1) if nz > 1 else (1, 3, 2, 0, 1, 1),
+               integrator=2, tmax=1.0, dtoutput=1.0, stepmax=3)
     rng = np.random.default_rng(seed)
-    sh = (n, n)
+    sh = (nz, n, n) if nz > 1 else (n, n)
     rho = 10 ** rng.uniform(-12, 2, sh)
     rho[rng.random(sh) < 0.02] = -1e-3
     vx, vy = rng.uniform(-10, 10, sh), rng.uniform(-10, 10, sh)
     vz = rng.uniform(-10, 10, sh) if with_vz else np.zeros(sh)
     c = problems.prim_to_cons(p, rho, vx, vy, vz, 10 ** rng.uniform(-14, 1, sh))
-    a = c[:, p.ng, p.ng:p.ng + n, p.ng:p.ng + n]
+    g = p.ng
+    a = c[:, g:g + nz, g:g + n, g:g + n] if nz > 1 else c[:, g, g:g + n, g:g + n]
     neg = rng.random(sh) < 0.05
     a[4][neg] = 0.25 * (a[1][neg] ** 2 + a[2][neg] ** 2 + a[3][neg] ** 2) / np.abs(a[0][neg])
     return p, c
 
 
-@pytest.mark.parametrize("with_vz", [False, True], ids=["fused2d", "generic"])
-def test_extreme_states_bitwise(with_vz):
+@pytest.mark.parametrize("path", ["fused2d", "generic", "stage3d"])
+def test_extreme_states_bitwise(path):
     """Every face's reconstruction and Riemann solve, and the floors, on a
     state full of near-vacuum, negative-density and negative-energy cells:
     three steps equal the oracle's bit for bit, dt sequence included, and
     the floors fired.  (At 96^2 the same recipe goes non-finite in the
     oracle too; the device then stops with GK_ERR_NONFINITE.)"""
-    p, c = _extreme_state(64, with_vz)
+    p, c = (_extreme_state(16, True, nz=16) if path == "stage3d"
+            else _extreme_state(64, path == "generic"))
     ref, ref_dts, _ = _oracle_run(p, c)
     s = _sim(p, c)
-    assert s.path == ("generic" if with_vz else "fused2d")
+    assert s.path == path
     s.run(p.tmax, p.dtoutput)
     assert s.dt_log() == ref_dts and len(ref_dts) == 3
     got = active(p, s.download())
