@@ -47,15 +47,23 @@ class Replicas:
         if self._sync is not None:
             self._sync()
 
-    def max(self, x: float) -> float:
-        """The maximum of x over the ranks (x itself with one rank)."""
+    def _reduce(self, x: float, op: str) -> float:
         if self._dist is None:
             return float(x)
         import torch
         dev = "cuda" if self.backend == "nccl" else "cpu"
         t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
-        self._dist.all_reduce(t, op=self._dist.ReduceOp.MAX)
+        self._dist.all_reduce(t, op=getattr(self._dist.ReduceOp, op))
         return float(t.item())
+
+    def max(self, x: float) -> float:
+        """The maximum of x over the ranks (x itself with one rank)."""
+        return self._reduce(x, "MAX")
+
+    def sum(self, x: float) -> float:
+        """The sum of x over the ranks (x itself with one rank), e.g. the
+        units the ranks processed when they differ per rank."""
+        return self._reduce(x, "SUM")
 
     def rate(self, units_per_rank: float, seconds_this_rank: float) -> float:
         """Whole-job rate: every rank's units over the slowest rank's time

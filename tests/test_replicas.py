@@ -34,7 +34,8 @@ def _worker(rank, world, port, mode, q):
         secs = time.perf_counter() - t0
         worst = reps.max(secs)
         rate = reps.rate(1000.0, secs)
-        q.put((rank, (secs, worst, rate, reps.is_root)))
+        total = reps.sum(10.0 * (rank + 1))  # per-rank units that differ
+        q.put((rank, (secs, worst, rate, reps.is_root, total)))
         reps.close()
     except Exception as e:  # reported to the test
         q.put((rank, "error: " + type(e).__name__))
@@ -65,7 +66,8 @@ def _run(mode, world=2, timeout=60):
 def test_two_replicas_time_the_slowest_rank():
     out = _run("ok")
     assert set(out) == {0, 1}, out
-    (s0, w0, r0, root0), (s1, w1, r1, root1) = out[0], out[1]
+    (s0, w0, r0, root0, n0), (s1, w1, r1, root1, n1) = out[0], out[1]
+    assert n0 == n1 == 30.0
     # the barrier after the work makes both ranks wait for the slower one
     assert w0 == w1 == pytest.approx(max(s0, s1))
     assert w0 >= 0.1 - 1e-3
