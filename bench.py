@@ -54,6 +54,12 @@ METRIC = "zone-updates/s"
 UNIT = "zone-updates/s"
 BYTES_PER_ZU_RK2 = 160  # 5 * V * 8 B with V = 4 (2D): algorithmic HBM bytes per zone-update
 STAGE_BYTES_PER_CELL = 80  # per stage launch, averaged over the two RK2 stages
+# FP64 add/mul/fma thread-instructions per zone-update of the fast-mode fused
+# RK2 step (stage 1 + last stage), from the ncu capture in
+# profiles/stage2d_tma_kh2048_ncu_full.md; the FP64 pipe issues 64 lanes per
+# SM per clock on B200 (148 SMs)
+FP64_OPS_PER_ZU_FAST = 308 + 336
+FP64_LANES = 64 * 148
 
 
 def _env_int(k, d):
@@ -315,6 +321,21 @@ def main_ours(args, rank, world, local_rank):
                 "avg_launch_ms": avg_stage_s * 1000.0,
                 "traffic": ncu_traffic(),
                 "step_frac_of_hbm_roofline": (BYTES_PER_ZU_RK2 * value / world / 1e9) / peak}
+    roof64 = None
+    if args.mode == "fast":
+        # the bound that binds: FP64 issue of the stage kernel (add/mul/fma only;
+        # compares and min/max also use the pipe)
+        mhz = (clocks or {}).get("sm_mhz")
+        src = "the median SM clock sampled in the timed region"
+        if not mhz:
+            mhz, src = 1965.0, "the B200's maximum SM clock (no clock sample in the timed region)"
+        ach = FP64_OPS_PER_ZU_FAST * value / world / 1e12
+        pk = FP64_LANES * mhz * 1e6 / 1e12
+        roof64 = {"bound": "fp64 issue", "achieved": ach, "peak": pk,
+                  "unit": "T FP64 thread-instructions/s", "frac": ach / pk,
+                  "ops_per_zone_update": FP64_OPS_PER_ZU_FAST,
+                  "peak_source": "64 FP64 lanes x 148 SMs x " + src,
+                  "ops_source": "ncu, profiles/stage2d_tma_kh2048_ncu_full.md"}
 
     # end to end through the C ABI with pinned host buffers
     e2e_steps = max(1, args.e2e_steps)
@@ -395,7 +416,7 @@ def main_ours(args, rank, world, local_rank):
                    "d2h_bytes_per_step": d2h, "steps": e2e_steps,
                    "cadence": "the state in and out around every single step (PCIe-bound)",
                    "timing": "host wall clock around the C-ABI calls, max over ranks"},
-               "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+               "roofline": roof, "roofline_fp64": roof64, "cpu_baseline": cpu, "clocks": clocks,
                "gpu_launches": launches, "kernel_shares": shares, "other_mode": other}
         print(json.dumps(out))
     sim.close()
