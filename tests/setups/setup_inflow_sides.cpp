@@ -3,8 +3,10 @@
 // A uniform flow; the x-left ghosts come from the hook's own routine.  With
 // the input key inflowCopies = 1 the routine copies the first active column
 // (the copy template of the reference's setup files), so its writes depend
-// on the state; otherwise it writes a constant inflow state, as the
-// reference's solid-body hook does (src/setup/setup_solid_body.cpp:62-96).
+// on the state; with inflowWide = 1 it writes the constant state into the
+// corner ghosts as well, outside the side's strip; otherwise it writes a
+// constant inflow state into the strip, as the reference's solid-body hook
+// does (src/setup/setup_solid_body.cpp:62-96).
 #include "gaukuk.hpp"
 #include "sim.hpp"
 
@@ -26,10 +28,11 @@ void Sim::Setup() {
 
 void Boundary::SelfDefineBDXL(TArray<Real>& cons, const Grid& grid, const EquationOfState& eos) {
     const bool copies = Config::getInstance().get("inflowCopies", 0) != 0;
+    const bool wide = Config::getInstance().get("inflowWide", 0) != 0;
     const Real q[NVar] = {2.0, 2.0, 0.0, 0.0, 1.0 + eos.EGas(2.0, 1.0)};
     for (int v = DEN; v <= ENG; ++v)
         for (int k = grid.kb; k < grid.ke; ++k)
-            for (int j = grid.jb; j < grid.je; ++j)
+            for (int j = wide ? grid.jgb : grid.jb; j < (wide ? grid.jge : grid.je); ++j)
                 for (int i = grid.igb; i < grid.ib; ++i) {
                     cons(v, k, j, i) = copies ? cons(v, k, j, grid.ib) : q[v];
                 }

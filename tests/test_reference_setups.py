@@ -126,22 +126,24 @@ def test_runs_match_the_reference(name, tmp_path):
                 assert err <= 1e-12, (f, v, err)
 
 
-@pytest.mark.parametrize("copies", [1, 0])
-def test_self_defined_sides_run_on_the_device_only_when_stationary(copies, tmp_path):
+@pytest.mark.parametrize("variant", ["copies", "wide", "constant"])
+def test_self_defined_sides_run_on_the_device_only_when_stationary(variant, tmp_path):
     """A setup's own boundary routine cannot run on the device.  One that
-    writes a constant inflow (tests/setups/setup_inflow_sides.cpp) is captured
-    as a fixed side; one that copies the state (inflowCopies = 1) is refused
+    writes a constant inflow into its ghost strip
+    (tests/setups/setup_inflow_sides.cpp) is captured as a fixed side; one
+    that copies the state, or that also writes the corner ghosts, is refused
     with a message, before any device work, so this runs on the CPU too."""
     from gaukuk_b200 import _build_host
     src = os.path.join(ROOT, "tests", "setups", "setup_inflow_sides.cpp")
     exe = _build_host.build_hook(src, name="inflow_sides", out_dir=str(tmp_path))
     p = Params(nx=16, ny=12, cfl=0.4, integrator=2, rc_order=2, bc=(3, 3, 3, 3, 1, 1),
                tmax=0.02, dtoutput=0.01, **P3)
-    (tmp_path / "run.in").write_text(p.to_in_text({"inflowCopies": copies}))
+    keys = {"inflowCopies": int(variant == "copies"), "inflowWide": int(variant == "wide")}
+    (tmp_path / "run.in").write_text(p.to_in_text(keys))
     r = subprocess.run([exe, "-i", "run.in"], cwd=tmp_path, capture_output=True, text=True,
                        timeout=300)
-    refused = "depends on the state" in r.stderr
-    if copies:
+    refused = "depends on the state or writes outside its ghost strip" in r.stderr
+    if variant != "constant":
         assert r.returncode != 0 and refused, r.stderr[-2000:]
     else:
         # past the probe: it runs on a GPU, or fails later for want of one
