@@ -79,6 +79,43 @@ def test_hllc_batch_symmetry():
     np.testing.assert_allclose(f[4], (e + p) * vx, rtol=1e-12, atol=1e-15)
 
 
+def _random_faces(n, seed):
+    rng = np.random.default_rng(seed)
+    def one():
+        return np.stack([rng.uniform(0.2, 3, n), rng.uniform(-2, 2, n), rng.uniform(-1, 1, n),
+                         rng.uniform(-1, 1, n), rng.uniform(0.2, 3, n)])
+    return one(), one()
+
+
+def test_hllc_mirror_symmetry():
+    """Reflecting a face (sides swapped, normal velocity negated) negates the
+    mass, tangential-momentum and energy fluxes and keeps the normal-momentum
+    flux (hllc.cpp:22-101 is symmetric up to rounding)."""
+    wl, wr = _random_faces(2000, 1)
+    f = gk_oracle.hllc_batch(wl, wr, 1, 1.4)
+    ml, mr = wr.copy(), wl.copy()
+    ml[1] *= -1
+    mr[1] *= -1
+    g = gk_oracle.hllc_batch(ml, mr, 1, 1.4)
+    scale = np.abs(f).max(axis=1, keepdims=True)
+    for v, sign in ((0, -1), (1, 1), (2, -1), (3, -1), (4, -1)):
+        assert np.max(np.abs(g[v] - sign * f[v]) / scale[v]) < 1e-13, v
+
+
+def test_hllc_resolves_an_isolated_contact():
+    """Equal pressure and normal velocity, different density and tangential
+    velocity: HLLC (unlike HLL) returns the upwind side's physical flux."""
+    wl, wr = _random_faces(2000, 2)
+    wr[1], wr[4] = wl[1], wl[4]
+    f = gk_oracle.hllc_batch(wl, wr, 1, 1.4)
+    up = np.where(wl[1] >= 0, wl, wr)
+    rho, vx, vy, vz, p = up
+    e = p / 0.4 + 0.5 * rho * (vx * vx + vy * vy + vz * vz)
+    exact = np.stack([rho * vx, rho * vx * vx + p, rho * vx * vy, rho * vx * vz, (e + p) * vx])
+    scale = np.abs(exact).max(axis=1, keepdims=True)
+    assert np.max(np.abs(f - exact) / scale) < 1e-12
+
+
 def test_vanleer_limiter():
     a = np.array([1.0, -1.0, 2.0, 0.0, -3.0])
     b = np.array([1.0, 2.0, 2.0, 5.0, -1.0])
