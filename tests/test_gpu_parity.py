@@ -254,3 +254,32 @@ def test_extreme_states_bitwise(path):
     assert np.isfinite(got).all() and np.array_equal(got, ref)
     den, pre = s.floor_hits()
     assert den > 0 and pre > 0
+
+
+@pytest.mark.parametrize("state", ["kh", "smooth", "rt"])
+def test_fast_face_fluxes_close_to_parity(state):
+    """Face by face, the fast mode's reconstruction and HLLC (FMA
+    contraction, refined reciprocals and roots, only the selected side, half
+    slopes) stay within 1e-13 of parity mode, whose fluxes are the
+    reference's bits (scale: the largest |flux| of each component).  The
+    extreme states above are left out on purpose: there floored cells carry
+    velocities near 1e13, S - v cancels to rounding noise in both modes, and
+    the two roundings differ."""
+    from gaukuk_b200.learned import face_fluxes
+    if state == "kh":
+        p, c = problems.kh(192, seed=3)
+    elif state == "rt":
+        p, c = problems.rt(64, 192)
+    else:
+        p = Params(nx=160, ny=128, bc=(1,) * 6, integrator=2, tmax=1.0, dtoutput=1.0)
+        c = problems.random_smooth(p, seed=5)
+    out = {}
+    for mode in ("parity", "fast"):
+        s = _sim(p, c, mode=mode)
+        out[mode] = face_fluxes(s)
+        s.close()
+    for a, b in zip(out["parity"], out["fast"]):
+        assert np.isfinite(a).all() and np.isfinite(b).all()
+        for v in range(4):
+            scale = np.abs(a[v]).max()
+            assert np.abs(b[v] - a[v]).max() <= 1e-13 * scale, (v, np.abs(b[v] - a[v]).max() / scale)
