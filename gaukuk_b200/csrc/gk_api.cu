@@ -307,6 +307,13 @@ int env_int(const char* name, int dflt) {
 //   KH 256^2, us per step, 128 threads x 4 rows -> 64 x 2: fast 24.2 -> 20.7,
 //   parity 52.8 -> 38.3; KH 512^2, 128 x 4 -> 64 x 4: fast 37.9 -> 33.4,
 //   parity 92.7 -> 63.4.
+// Parity mode's heavier cells want more waves of long tiles where a grid has
+// more than one wave at 24 rows: it then aims at 4 waves with at least 12
+// rows.  Parity, us per step at the rows chosen (12 / 16 / 24 rows):
+// RT 1024x3072 761 (761 / 772 / 788), KH 2048^2 621 at 15 (625 / 631 / 666),
+// KH 4096^2 2267 at 24.  Smaller grids keep the one-wave rule, which a tail
+// wave would cost more than short tiles save: KH 1024^2 at 16 rows is one
+// wave of 576 tiles, 189 us (12 rows: 234).
 // GK_STAGE_THREADS / GK_STAGE_ROWS override (tuning).
 int stage_threads_for(const gk::Geom& g) {
     const int v = env_int("GK_STAGE_THREADS", 0);
@@ -315,14 +322,15 @@ int stage_threads_for(const gk::Geom& g) {
     return (long long)g.ny * strips / (148 * 4) < 8 ? 64 : 128;
 }
 
-int stage_rows(const gk::Geom& g, int threads) {
+int stage_rows(const gk::Geom& g, int threads, bool parity) {
     const int forced = env_int("GK_STAGE_ROWS", 0);
     if (forced > 0) return forced;
     const long long cols = threads - 4;
     const long long strips = (g.nx + cols - 1) / cols;
-    const long long slots = 148LL * (512 / threads);
-    const long long per_slot = ((long long)g.ny * strips + slots - 1) / slots;
-    return (int)std::max(2LL, std::min(24LL, per_slot));
+    const long long tiles = (long long)g.ny * strips, slots = 148LL * (512 / threads);
+    const long long per_slot = (tiles + slots - 1) / slots;
+    if (!parity || per_slot <= 24) return (int)std::max(2LL, std::min(24LL, per_slot));
+    return (int)std::max(12LL, std::min(24LL, (tiles + 4 * slots - 1) / (4 * slots)));
 }
 
 // Path 1, the fused 2D stage, applies to 2D RK2/RK3 runs with MTZ
@@ -659,7 +667,7 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
     h->ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
     if (!h->tiling_set) {
         h->ctx.stage_threads = stage_threads_for(g);
-        h->ctx.h2d_rows = stage_rows(g, h->ctx.stage_threads);
+        h->ctx.h2d_rows = stage_rows(g, h->ctx.stage_threads, h->ks == &kParity);
     } else {
         h->ctx.h2d_rows = h->tiling_rows;
     }
@@ -1019,7 +1027,7 @@ int gk_internal_build_ctx(const gk_grid_desc* gd, const gk_phys_desc* pd, gk::Ct
     }
     tmp.ctx.use_tma = env_int("GK_STAGE_TMA", 1) != 0;
     tmp.ctx.stage_threads = stage_threads_for(tmp.ctx.g);
-    tmp.ctx.h2d_rows = stage_rows(tmp.ctx.g, tmp.ctx.stage_threads);
+    tmp.ctx.h2d_rows = stage_rows(tmp.ctx.g, tmp.ctx.stage_threads, pd->mode != GK_MODE_FAST);
     *ctx = tmp.ctx;
     return GK_OK;
 }
