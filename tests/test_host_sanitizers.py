@@ -1,7 +1,8 @@
 """The C++ host layer under AddressSanitizer and UndefinedBehaviorSanitizer
-(errors abort the run).  Setup hooks run through their first frame: the
-setup, the host ghost fill with fixed sides, an immersed body's table and
-its fill, and the frame writer.  The frames must equal the plain build's.
+(errors abort the run).  All nine of the reference's setup hooks run
+through their first frame: the setup, the host ghost fill with fixed sides,
+an immersed body's table and its fill, point and binary gravity enrollment,
+and the frame writer.  The frames must equal the plain build's.
 A hook whose own boundary routine depends on the state is refused at the
 first Advance; that path (the three probes of the routine) runs under the
 sanitizers too, before any device work, so all of this runs on the CPU."""
@@ -18,7 +19,8 @@ from test_reference_setups import CASES, P3, ROOT
 ENV = dict(os.environ, ASAN_OPTIONS="halt_on_error=1:detect_leaks=1",
            UBSAN_OPTIONS="halt_on_error=1:print_stacktrace=1")
 REF_SETUP = os.path.join(_build_host.REFERENCE_SRC, "src", "setup")
-NAMES = ["solid_body", "disk_planet", "blast", "kh"]
+NAMES = ["blast", "disk", "disk_planet", "example", "kh", "rt", "shock_tube", "solid_body",
+         "wave_test"]
 
 
 @pytest.fixture(scope="module")
