@@ -11,10 +11,11 @@ computes the same initial state bits as the reference built with strict IEEE
 flags.  ``build_hook(path)`` builds a driver for any hook file written for
 the reference -- the hook's own ``#include "../sim.hpp"`` resolves to this
 layer's headers (``-I-`` stops the compiler from looking next to the hook).
-Where the reference's sources are present (``GK_REFERENCE_SRC``, default the
-reference checkout the oracle recipe also reads), its own setup files that
-run on the device path are built as well, unchanged, as
-``bin/gaukuk_ref_<name>.sim``.
+Where the reference's sources are given (``GK_REFERENCE_SRC``, else the
+checkout the oracle recipe last built from, recorded in oracle/_ref/SOURCE),
+its own setup files that run on the device path are built as well,
+unchanged, as ``bin/gaukuk_ref_<name>.sim``.  With neither, they are
+skipped.
 """
 from __future__ import annotations
 
@@ -76,7 +77,20 @@ def build_hook(hook_src: str, name: Optional[str] = None, verbose: bool = False,
     return exe
 
 
-REFERENCE_SRC = os.environ.get("GK_REFERENCE_SRC", "/root/reference")
+def reference_src() -> str:
+    """The reference checkout: GK_REFERENCE_SRC, else the path the oracle
+    recipe recorded when it built from it, else '' (none given)."""
+    env = os.environ.get("GK_REFERENCE_SRC", "")
+    if env:
+        return env
+    rec = os.path.join(os.path.dirname(PKG), "oracle", "_ref", "SOURCE")
+    if os.path.exists(rec):
+        with open(rec) as f:
+            return f.read().strip()
+    return ""
+
+
+REFERENCE_SRC = reference_src()
 REFERENCE_HOOKS = ("blast", "disk", "disk_planet", "example", "kh", "rt", "shock_tube", "solid_body",
                    "wave_test")
 
@@ -85,9 +99,10 @@ def build_host(verbose: bool = False, force: bool = False) -> None:
     build_host_lib(verbose=verbose, force=force)
     for hook in sorted(glob.glob(os.path.join(SETUP, "setup_*.cpp"))):
         build_hook(hook, verbose=verbose, force=force)
+    ref = reference_src()
     for name in REFERENCE_HOOKS:
-        src = os.path.join(REFERENCE_SRC, "src", "setup", f"setup_{name}.cpp")
-        if os.path.exists(src):
+        src = os.path.join(ref, "src", "setup", f"setup_{name}.cpp")
+        if ref and os.path.exists(src):
             build_hook(src, name="ref_" + name, verbose=verbose, force=force)
 
 

@@ -316,16 +316,23 @@ int gk_fastmath_check(int n, unsigned long long seed, double* worst3);
  * device state, for callers that cannot allocate device memory while they
  * run: their memory comes from their own pool or arena, or their budget is
  * fixed at start-up.  No counterpart in the reference; the arithmetic is
- * that of gk_run_steps with one step.  Nothing is allocated: the
- * intermediate stage state and the device clock live in one fixed 64 MiB
- * array inside the library, held by every GPU that loads it until the
- * process exits, so grids whose stage state exceeds it (more than about
- * 1440 x 1440 cells) are rejected with GK_ERR_INVALID.
+ * that of gk_run_steps with one step (constant gravity included: both half
+ * kicks).  Nothing is allocated: the intermediate stage state (all five
+ * planes, since the ghost fill writes every plane's ghosts) and the device
+ * clock live in one fixed 64 MiB array inside the library, held by every GPU
+ * that loads it until the process exits, so grids whose stage state exceeds
+ * it (5 * leny * pitch > 2^23 doubles: more than about 1290 x 1290 cells)
+ * are rejected with GK_ERR_INVALID.  Fixed (type 4) sides need the state at
+ * enrollment that only a handle holds: GK_ERR_UNSUPPORTED.
  *
  * state: the device layout of the library -- five planes DEN, MTX, MTY, ENG,
  * MTZ, each leny rows of `pitch` doubles (lenx rounded up to a multiple of
  * 16), ghost columns and rows included; MTZ must be zero.  It is updated in
- * place; its ghost cells are overwritten by the boundary fill.
+ * place; its ghost cells are overwritten by the boundary fill.  A state
+ * aligned to 16 bytes (any cudaMalloc'd or pool block) is staged into the
+ * stage kernel by TMA; the tensor map cannot describe a less aligned one, and
+ * the call then runs the register-staged form of the stage (same results)
+ * after a line on stderr.
  * dt = min(CFL*drmin/cmax(state), dtmax) as in Sim::Advance (sim.cpp:77-81);
  * *dt_used (host, may be NULL) receives it.  stream: a cudaStream_t or NULL;
  * the call returns after that stream synchronises.
