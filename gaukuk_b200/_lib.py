@@ -61,6 +61,8 @@ SIGNATURES = {
     "gk_profile_steps": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _dp,
                                         _ip, ctypes.c_int, _ip]),
     "gk_fastmath_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_ulonglong, _dp]),
+    "gk_paritymath_check": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_ulonglong,
+                                           ctypes.POINTER(ctypes.c_ulonglong)]),
     "gk_rk2_step_noalloc": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(PhysDesc),
                                            _vp, ctypes.c_double, _dp, _vp]),
     "gk_set_tiling": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
@@ -91,6 +93,22 @@ SIGNATURES = {
     "gk_flux_model_fired": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint)]),
     "gk_face_fluxes": (ctypes.c_int, [_vp, _vp, _vp]),
     "gk_tap_substeps": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _vp]),
+    "gk_slab_layout": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      _ip, _ip, _ip, _ip]),
+    "gk_slabs_create": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(PhysDesc),
+                                       ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "gk_slabs_nccl_id": (ctypes.c_int, [_vp]),
+    "gk_slabs_create_nccl": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(PhysDesc),
+                                            ctypes.c_int, ctypes.c_int, _vp,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "gk_slabs_destroy": (None, [_vp]),
+    "gk_slabs_upload_cons": (ctypes.c_int, [_vp, _vp]),
+    "gk_slabs_download_cons": (ctypes.c_int, [_vp, _vp]),
+    "gk_slabs_advance": (ctypes.c_int, [_vp, ctypes.c_double, _dp, _ip, _ip]),
+    "gk_slabs_run_steps": (ctypes.c_int, [_vp, ctypes.c_int, _ip]),
+    "gk_slabs_dt_log": (ctypes.c_int, [_vp, _dp, ctypes.c_int, _ip]),
+    "gk_slabs_info": (ctypes.c_int, [_vp, _ip, _ip, _ip, _ip]),
+    "gk_slabs_last_error": (ctypes.c_char_p, [_vp]),
     "gk_strerror": (ctypes.c_char_p, [ctypes.c_int]),
     "gk_last_error": (ctypes.c_char_p, [_vp]),
 }

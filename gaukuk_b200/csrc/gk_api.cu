@@ -27,6 +27,9 @@
 namespace gk_fast {
 int fastmath_check(int n, unsigned long long seed, double* host_worst3);
 }
+namespace gk_parity {
+int paritymath_check(long long n, unsigned long long seed, unsigned long long* host_out5);
+}
 
 namespace gk {
 
@@ -73,6 +76,7 @@ struct KernelSet {
     decltype(&gk_parity::launch_ens_begin) ens_begin;
     decltype(&gk_parity::launch_zflux) zflux;
     decltype(&gk_parity::launch_stage3d) stage3d;
+    decltype(&gk_parity::launch_epilogue) epilogue;
 };
 
 const KernelSet kParity = {gk_parity::launch_bc,     gk_parity::launch_c2p,
@@ -81,12 +85,13 @@ const KernelSet kParity = {gk_parity::launch_bc,     gk_parity::launch_c2p,
                            gk_parity::launch_stage2d, gk_parity::launch_begin,
                            gk_parity::launch_mtz_check, gk_parity::launch_ens_stage,
                            gk_parity::launch_ens_bc,  gk_parity::launch_ens_begin,
-                           gk_parity::launch_zflux,   gk_parity::launch_stage3d};
+                           gk_parity::launch_zflux,   gk_parity::launch_stage3d,
+                           gk_parity::launch_epilogue};
 const KernelSet kFast = {gk_fast::launch_bc,     gk_fast::launch_c2p,     gk_fast::launch_flux,
                          gk_fast::launch_update, gk_fast::launch_kick,    gk_fast::launch_cfl,
                          gk_fast::launch_stage2d, gk_fast::launch_begin,  gk_fast::launch_mtz_check,
                          gk_fast::launch_ens_stage, gk_fast::launch_ens_bc, gk_fast::launch_ens_begin,
-                         gk_fast::launch_zflux, gk_fast::launch_stage3d};
+                         gk_fast::launch_zflux, gk_fast::launch_stage3d, gk_fast::launch_epilogue};
 
 constexpr int kLogCap = 1 << 20;
 
@@ -178,6 +183,8 @@ int build_ctx(gk_handle* h) {
     if (!(pd.cfl > 0.0)) return fail(h, GK_ERR_INVALID, "CFL must be positive");
     if (pd.mode != GK_MODE_PARITY && pd.mode != GK_MODE_FAST)
         return fail(h, GK_ERR_INVALID, "unknown arithmetic mode");
+    if (pd.mode == GK_MODE_FAST && !(pd.dfloor > 0.0 && pd.pfloor > 0.0))
+        return fail(h, GK_ERR_UNSUPPORTED, "fast mode needs positive density and pressure floors");
     g.nx = gd.nx; g.ny = gd.ny; g.nz = gd.nz; g.ng = gd.nghost;
     g.lenx = g.nx + 2 * g.ng; g.leny = g.ny + 2 * g.ng; g.lenz = g.nz + 2 * g.ng;
     g.ib = g.ng; g.ie = g.ib + g.nx;
@@ -231,6 +238,7 @@ int build_ctx(gk_handle* h) {
     ph.npoint = 0;
     ph.shells = nullptr;
     ph.nshell = 0;
+    ph.defer_epilogue = 0;
     ph.fill_z = 0;
     if (g.ndim == 3) {
         // z sides of type 0 run OutflowCopyYL/YR after the y fill
@@ -996,6 +1004,11 @@ int gk_fastmath_check(int n, unsigned long long seed, double* worst3) {
     return gk_fast::fastmath_check(n, seed, worst3) == 0 ? GK_OK : GK_ERR_CUDA;
 }
 
+int gk_paritymath_check(long long n, unsigned long long seed, unsigned long long* counts5) {
+    if (n <= 0 || !counts5) return GK_ERR_INVALID;
+    return gk_parity::paritymath_check(n, seed, counts5) == 0 ? GK_OK : GK_ERR_CUDA;
+}
+
 const char* gk_strerror(int status) {
     switch (status) {
         case GK_OK: return "ok";
@@ -1541,3 +1554,507 @@ extern "C" int gk_flux_model_fired(gk_handle* h, unsigned* fired) {
     GK_CUDA(h, cudaMemcpy(fired, h->fired, sizeof(unsigned), cudaMemcpyDeviceToHost));
     return GK_OK;
 }
+
+// ------------------------------------------------------------ y-slabs
+// One 2D grid split into y-slabs (a scale-out form of Sim::Advance for a grid
+// larger than one GPU's share).  Each slab is a fused-2D handle over rows
+// [j0, j0 + ny) of the global grid, with the global dx, dy and drmin.  Per RK
+// stage, after the ghost fill of the x sides and of any physical y side, the
+// two ghost rows on either side of a slab come from its neighbours' active
+// rows; with periodic y the slabs form a ring.  The last stage defers the
+// step epilogue: the CFL maximum is taken over all slabs first, so every slab
+// takes the dt of the whole grid (sim.cpp:77-81) and the results are the
+// undivided grid's bit for bit.  Slabs in one process share one device and
+// one stream and exchange through a copy kernel; one slab per process
+// exchanges through NCCL (send/recv of the packed rows, all-reduce(max) of
+// the CFL speed and the status word), loaded at run time so the library does
+// not depend on NCCL otherwise.
+#include <dlfcn.h>
+#include <nccl.h>
+
+namespace {
+
+struct NcclApi {
+    ncclResult_t (*GetUniqueId)(ncclUniqueId*);
+    ncclResult_t (*CommInitRank)(ncclComm_t*, int, ncclUniqueId, int);
+    ncclResult_t (*CommDestroy)(ncclComm_t);
+    ncclResult_t (*GroupStart)();
+    ncclResult_t (*GroupEnd)();
+    ncclResult_t (*Send)(const void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t);
+    ncclResult_t (*Recv)(void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t);
+    ncclResult_t (*AllReduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t,
+                              cudaStream_t);
+    const char* (*GetErrorString)(ncclResult_t);
+};
+
+// NCCL, resolved once from the process's libnccl.so.2 (the one a framework in
+// the same process already loaded, else the system's).
+const NcclApi* nccl_api(std::string* err) {
+    static NcclApi api{};
+    static bool tried = false, ok = false;
+    static std::string why;
+    if (!tried) {
+        tried = true;
+        void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+        if (!h) {
+            why = std::string("cannot load libnccl.so.2: ") + dlerror();
+        } else {
+            auto sym = [&](const char* name) { return dlsym(h, name); };
+            api.GetUniqueId = (decltype(api.GetUniqueId))sym("ncclGetUniqueId");
+            api.CommInitRank = (decltype(api.CommInitRank))sym("ncclCommInitRank");
+            api.CommDestroy = (decltype(api.CommDestroy))sym("ncclCommDestroy");
+            api.GroupStart = (decltype(api.GroupStart))sym("ncclGroupStart");
+            api.GroupEnd = (decltype(api.GroupEnd))sym("ncclGroupEnd");
+            api.Send = (decltype(api.Send))sym("ncclSend");
+            api.Recv = (decltype(api.Recv))sym("ncclRecv");
+            api.AllReduce = (decltype(api.AllReduce))sym("ncclAllReduce");
+            api.GetErrorString = (decltype(api.GetErrorString))sym("ncclGetErrorString");
+            ok = api.GetUniqueId && api.CommInitRank && api.CommDestroy && api.GroupStart &&
+                 api.GroupEnd && api.Send && api.Recv && api.AllReduce && api.GetErrorString;
+            if (!ok) why = "libnccl.so.2 lacks a needed symbol";
+        }
+    }
+    if (!ok && err) *err = why;
+    return ok ? &api : nullptr;
+}
+
+// Rows of slab k of n over ny active rows: the first ny % n slabs take one
+// row more.
+void slab_rows(int ny, int n, int k, int* j0, int* cnt) {
+    const int base = ny / n, rem = ny % n;
+    *cnt = base + (k < rem ? 1 : 0);
+    *j0 = k * base + (k < rem ? k : rem);
+}
+
+// Neighbours of slab k of n: -1 where the y side is the grid's own boundary
+// (filled by the ghost fill); with periodic y the first and last slabs are
+// each other's neighbours (a single slab is its own).
+void slab_neighbors(int n, int k, bool periodic, int* lower, int* upper) {
+    *lower = k > 0 ? k - 1 : (periodic ? n - 1 : -1);
+    *upper = k < n - 1 ? k + 1 : (periodic ? 0 : -1);
+}
+
+}  // namespace
+
+struct gk_slabs {
+    gk_grid_desc gd{};        // the whole grid
+    gk_phys_desc pd{};
+    int nslab = 1;            // slabs of the whole grid
+    int first = 0;            // index of this process's first slab
+    std::vector<gk_handle*> s;  // this process's slabs
+    std::vector<int> j0, ny;  // their first active row (global, 0-based) and row count
+    cudaStream_t stream = nullptr;  // the first slab's: every launch of the group
+    gk::SlabDev* dsd = nullptr;     // device table of the local slabs
+    const NcclApi* nccl = nullptr;
+    ncclComm_t comm = nullptr;
+    int lower = -1, upper = -1;     // NCCL: neighbour ranks
+    double* xbuf = nullptr;         // NCCL: send lo, send hi, recv lo, recv hi
+    unsigned long long* red = nullptr;
+    std::string err;
+};
+
+namespace {
+
+int sfail(gk_slabs* G, int code, const std::string& msg) {
+    if (G) G->err = msg;
+    return code;
+}
+
+#define GK_SCUDA(G, call)                                                                       \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return sfail((G), GK_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define GK_SNCCL(G, call)                                                                      \
+    do {                                                                                       \
+        ncclResult_t r_ = (call);                                                              \
+        if (r_ != ncclSuccess)                                                                 \
+            return sfail((G), GK_ERR_CUDA, std::string(#call) + ": " + (G)->nccl->GetErrorString(r_)); \
+    } while (0)
+
+// Creates this process's slabs (global indices first .. first + count - 1).
+int slabs_build(gk_slabs* G, int first, int count) {
+    const gk_grid_desc& gd = G->gd;
+    const gk_phys_desc& pd = G->pd;
+    if (gd.nz != 1 || gd.ny < 2 || gd.nx < 2)
+        return sfail(G, GK_ERR_UNSUPPORTED, "y-slabs split 2D grids");
+    if (pd.integrator != 2 && pd.integrator != 3)
+        return sfail(G, GK_ERR_UNSUPPORTED, "y-slabs run RK2 or RK3 (the fused 2D stage)");
+    if (pd.grav[2] != 0)
+        return sfail(G, GK_ERR_UNSUPPORTED, "y-slabs need gz = 0 (the fused 2D stage)");
+    if (pd.bc[2] == 4 || pd.bc[3] == 4 || pd.bc[0] == 4 || pd.bc[1] == 4)
+        return sfail(G, GK_ERR_UNSUPPORTED, "fixed (type 4) sides are not split");
+    if (G->nslab < 1 || gd.ny / G->nslab < gd.nghost)
+        return sfail(G, GK_ERR_INVALID, "every slab needs at least NGhost rows");
+    // the whole grid's spacings (sim.cpp:16-36), which every slab keeps
+    gk_handle whole;
+    whole.gd = gd;
+    whole.pd = pd;
+    int rc = build_ctx(&whole);
+    if (rc != GK_OK) return sfail(G, rc, whole.err);
+    const bool periodic = whole.ctx.ph.bc[2] == 1;
+    if (periodic != (whole.ctx.ph.bc[3] == 1))
+        return sfail(G, GK_ERR_UNSUPPORTED, "a periodic y side needs a periodic partner");
+    for (int k = first; k < first + count; ++k) {
+        int j0, cnt, lo, up;
+        slab_rows(gd.ny, G->nslab, k, &j0, &cnt);
+        slab_neighbors(G->nslab, k, periodic, &lo, &up);
+        gk_grid_desc sg = gd;
+        sg.ny = cnt;
+        gk_handle* h = nullptr;
+        rc = gk_create(&sg, &pd, &h);
+        if (rc != GK_OK) return sfail(G, rc, "slab creation failed");
+        G->s.push_back(h);
+        G->j0.push_back(j0);
+        G->ny.push_back(cnt);
+        gk::Geom& g = h->ctx.g;
+        g.dy = whole.ctx.g.dy;
+        g.dyRec = whole.ctx.g.dyRec;
+        g.drmin = whole.ctx.g.drmin;
+        g.ymin = whole.ctx.g.ymin + j0 * whole.ctx.g.dy;  // cell centres, not used by the fused stage
+        // sides between slabs (all y sides under periodic y) come from the exchange
+        if (lo >= 0) h->ctx.ph.bc[2] = 5;
+        if (up >= 0) h->ctx.ph.bc[3] = 5;
+        h->ctx.ph.defer_epilogue = 1;
+    }
+    G->stream = G->s[0]->stream;
+    return GK_OK;
+}
+
+int slabs_device_table(gk_slabs* G) {
+    const int n = (int)G->s.size();
+    std::vector<gk::SlabDev> t(n);
+    const bool periodic = G->pd.bc[2] == 1;
+    for (int k = 0; k < n; ++k) {
+        gk_handle* h = G->s[k];
+        t[k].buf[0] = h->A;
+        t[k].buf[1] = h->B;
+        t[k].buf[2] = h->C;
+        t[k].tm = h->tm;
+        t[k].vstride = h->ctx.g.vstride;
+        t[k].jb = h->ctx.g.jb;
+        t[k].je = h->ctx.g.je;
+        int lo, up;
+        slab_neighbors(G->nslab, G->first + k, periodic, &lo, &up);
+        // in-process exchange only: neighbours are local slabs
+        t[k].lower = lo >= 0 ? lo - G->first : -1;
+        t[k].upper = up >= 0 ? up - G->first : -1;
+    }
+    GK_SCUDA(G, cudaMalloc(&G->dsd, sizeof(gk::SlabDev) * n));
+    GK_SCUDA(G, cudaMemcpy(G->dsd, t.data(), sizeof(gk::SlabDev) * n, cudaMemcpyHostToDevice));
+    return GK_OK;
+}
+
+double* slab_buf(gk_handle* h, int role) { return role == 0 ? h->A : (role == 1 ? h->B : h->C); }
+
+// The two ghost rows on each side of every local slab, in buffer `role`.
+int slabs_halo(gk_slabs* G, int role) {
+    if (!G->comm) {
+        gk::launch_slab_halo(G->dsd, (int)G->s.size(), role, G->s[0]->ctx.g, G->stream);
+        return GK_OK;
+    }
+    gk_handle* h = G->s[0];
+    const gk::Geom& g = h->ctx.g;
+    const size_t cnt = 10 * (size_t)g.nx;
+    double *slo = G->xbuf, *shi = G->xbuf + cnt, *rlo = G->xbuf + 2 * cnt, *rhi = G->xbuf + 3 * cnt;
+    double* u = slab_buf(h, role);
+    gk::launch_slab_pack(u, slo, shi, g, h->ctx.tm, G->stream);
+    // rows going up first, then rows going down: between any two ranks the
+    // k-th send matches the k-th receive, self-exchange of a single ring
+    // slab included
+    GK_SNCCL(G, G->nccl->GroupStart());
+    if (G->upper >= 0) GK_SNCCL(G, G->nccl->Send(shi, cnt, ncclDouble, G->upper, G->comm, G->stream));
+    if (G->lower >= 0) GK_SNCCL(G, G->nccl->Recv(rlo, cnt, ncclDouble, G->lower, G->comm, G->stream));
+    if (G->lower >= 0) GK_SNCCL(G, G->nccl->Send(slo, cnt, ncclDouble, G->lower, G->comm, G->stream));
+    if (G->upper >= 0) GK_SNCCL(G, G->nccl->Recv(rhi, cnt, ncclDouble, G->upper, G->comm, G->stream));
+    GK_SNCCL(G, G->nccl->GroupEnd());
+    gk::launch_slab_unpack(u, G->lower >= 0 ? rlo : nullptr, G->upper >= 0 ? rhi : nullptr, g,
+                           h->ctx.tm, G->stream);
+    return GK_OK;
+}
+
+// The CFL maximum (and status) over all slabs into every slab's clock.
+int slabs_reduce(gk_slabs* G, int which) {
+    if (!G->comm) {
+        gk::launch_slab_reduce(G->dsd, (int)G->s.size(), which, G->stream);
+        return GK_OK;
+    }
+    gk_handle* h = G->s[0];
+    gk::launch_slab_red_pack(h->tm, G->red, which, G->stream);
+    GK_SNCCL(G, G->nccl->AllReduce(G->red, G->red, 2, ncclUint64, ncclMax, G->comm, G->stream));
+    gk::launch_slab_red_unpack(h->tm, G->red, which, G->stream);
+    return GK_OK;
+}
+
+// One time step of the whole grid (Sim::RK2_/RK3_ with the Strang half kicks
+// of sim.cpp:85-91), every phase over all local slabs before the next.
+int slabs_enqueue_step(gk_slabs* G) {
+    const KernelSet& k = *G->s[0]->ks;
+    cudaStream_t st = G->stream;
+    const bool rk3 = G->s[0]->ctx.ph.integrator == 3;
+    const double frac13 = 1.0 / 3.0;
+    int rc;
+    for (gk_handle* h : G->s)
+        if (h->ctx.ph.has_grav) k.kick(h->ctx, h->A, 0, st);
+    for (gk_handle* h : G->s) k.bc(h->ctx, h->A, st);
+    if ((rc = slabs_halo(G, 0)) != GK_OK) return rc;
+    for (gk_handle* h : G->s) k.stage2d(h->ctx, h->A, nullptr, h->B, 0, 1.0, 1.0, 0.0, st);
+    for (gk_handle* h : G->s) k.bc(h->ctx, h->B, st);
+    if ((rc = slabs_halo(G, 1)) != GK_OK) return rc;
+    if (rk3) {
+        for (gk_handle* h : G->s) k.stage2d(h->ctx, h->B, h->A, h->C, 1, 0.75, 0.25, 0.25, st);
+        for (gk_handle* h : G->s) k.bc(h->ctx, h->C, st);
+        if ((rc = slabs_halo(G, 2)) != GK_OK) return rc;
+        for (gk_handle* h : G->s)
+            k.stage2d(h->ctx, h->C, h->A, h->A, 2, frac13, 2 * frac13, 2 * frac13, st);
+    } else {
+        for (gk_handle* h : G->s) k.stage2d(h->ctx, h->B, h->A, h->A, 2, 0.5, 0.5, 0.5, st);
+    }
+    if ((rc = slabs_reduce(G, 0)) != GK_OK) return rc;
+    for (gk_handle* h : G->s) k.epilogue(h->ctx, st);
+    return GK_OK;
+}
+
+int slabs_check_ready(gk_slabs* G) {
+    if (!G) return GK_ERR_INVALID;
+    for (gk_handle* h : G->s) {
+        if (!h->uploaded) return sfail(G, GK_ERR_STATE, "no state uploaded");
+        if (h->path != 1)
+            return sfail(G, GK_ERR_UNSUPPORTED,
+                         "y-slabs run the fused 2D stage (vz = 0, no point masses or immersed body)");
+    }
+    GK_SCUDA(G, cudaSetDevice(G->s[0]->device));
+    return GK_OK;
+}
+
+// Sim::Advance over the whole grid (nsteps = 0) or a fixed step count.
+int slabs_run(gk_slabs* G, double dtoutput, int nsteps) {
+    int rc = slabs_reduce(G, 1);
+    if (rc != GK_OK) return rc;
+    const KernelSet& k = *G->s[0]->ks;
+    for (gk_handle* h : G->s) k.begin(h->ctx, dtoutput, nsteps, G->stream);
+    gk_handle* h0 = G->s[0];
+    if (nsteps > 0) {
+        for (int i = 0; i < nsteps; ++i)
+            if ((rc = slabs_enqueue_step(G)) != GK_OK) return rc;
+    } else {
+        // every process sees the same clock (one dt for the whole grid), so
+        // all of them enqueue the same batches and stop together
+        int batch = 1;
+        for (;;) {
+            for (int i = 0; i < batch; ++i)
+                if ((rc = slabs_enqueue_step(G)) != GK_OK) return rc;
+            GK_SCUDA(G, cudaMemcpyAsync(&h0->htm->active, &h0->tm->active, sizeof(int),
+                                        cudaMemcpyDeviceToHost, G->stream));
+            GK_SCUDA(G, cudaStreamSynchronize(G->stream));
+            if (!h0->htm->active) break;
+            batch = std::min(batch * 2, 64);
+        }
+    }
+    GK_SCUDA(G, cudaGetLastError());
+    GK_SCUDA(G, cudaStreamSynchronize(G->stream));
+    for (gk_handle* s : G->s)
+        if ((rc = pull_time(s)) != GK_OK) return sfail(G, rc, s->err);
+    if (h0->htm->status) {
+        rc = status_error(h0);
+        return sfail(G, rc, h0->err);
+    }
+    return GK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gk_slab_layout(int ny, int nslab, int k, int periodic, int* j0, int* rows, int* lower,
+                   int* upper) {
+    if (nslab < 1 || k < 0 || k >= nslab || ny < nslab) return GK_ERR_INVALID;
+    int a, b, c, d;
+    slab_rows(ny, nslab, k, &a, &b);
+    slab_neighbors(nslab, k, periodic != 0, &c, &d);
+    if (j0) *j0 = a;
+    if (rows) *rows = b;
+    if (lower) *lower = c;
+    if (upper) *upper = d;
+    return GK_OK;
+}
+
+int gk_slabs_create(const gk_grid_desc* grid, const gk_phys_desc* phys, int nslab, gk_slabs** out) {
+    if (!grid || !phys || !out || nslab < 1) return GK_ERR_INVALID;
+    *out = nullptr;
+    gk_slabs* G = new gk_slabs();
+    G->gd = *grid;
+    G->pd = *phys;
+    G->nslab = nslab;
+    G->first = 0;
+    int rc = slabs_build(G, 0, nslab);
+    if (rc == GK_OK) rc = slabs_device_table(G);
+    if (rc != GK_OK) {
+        std::fprintf(stderr, "gk_slabs_create: %s\n", G->err.c_str());
+        gk_slabs_destroy(G);
+        return rc;
+    }
+    *out = G;
+    return GK_OK;
+}
+
+int gk_slabs_nccl_id(void* id128) {
+    if (!id128) return GK_ERR_INVALID;
+    std::string err;
+    const NcclApi* api = nccl_api(&err);
+    if (!api) {
+        std::fprintf(stderr, "gk_slabs_nccl_id: %s\n", err.c_str());
+        return GK_ERR_UNSUPPORTED;
+    }
+    ncclUniqueId id;
+    if (api->GetUniqueId(&id) != ncclSuccess) return GK_ERR_CUDA;
+    std::memcpy(id128, &id, sizeof(id));
+    return GK_OK;
+}
+
+int gk_slabs_create_nccl(const gk_grid_desc* grid, const gk_phys_desc* phys, int nranks, int rank,
+                         const void* id128, gk_slabs** out) {
+    if (!grid || !phys || !out || !id128 || nranks < 1 || rank < 0 || rank >= nranks)
+        return GK_ERR_INVALID;
+    *out = nullptr;
+    gk_slabs* G = new gk_slabs();
+    G->gd = *grid;
+    G->pd = *phys;
+    G->nslab = nranks;
+    G->first = rank;
+    std::string err;
+    G->nccl = nccl_api(&err);
+    int rc = G->nccl ? GK_OK : sfail(G, GK_ERR_UNSUPPORTED, err);
+    if (rc == GK_OK) rc = slabs_build(G, rank, 1);
+    if (rc == GK_OK) {
+        gk_handle* h = G->s[0];
+        slab_neighbors(nranks, rank, G->pd.bc[2] == 1, &G->lower, &G->upper);
+        const size_t cnt = 10 * (size_t)h->ctx.g.nx;
+        cudaError_t e = cudaSetDevice(h->device);
+        if (e == cudaSuccess) e = cudaMalloc(&G->xbuf, 4 * cnt * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemset(G->xbuf, 0, 4 * cnt * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&G->red, 2 * sizeof(unsigned long long));
+        if (e != cudaSuccess) rc = sfail(G, GK_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (rc == GK_OK) {
+        ncclUniqueId id;
+        std::memcpy(&id, id128, sizeof(id));
+        ncclComm_t comm = nullptr;
+        const ncclResult_t r = G->nccl->CommInitRank(&comm, nranks, id, rank);
+        if (r != ncclSuccess) rc = sfail(G, GK_ERR_CUDA, std::string("ncclCommInitRank: ") +
+                                                           G->nccl->GetErrorString(r));
+        else G->comm = comm;
+    }
+    if (rc != GK_OK) {
+        std::fprintf(stderr, "gk_slabs_create_nccl: %s\n", G->err.c_str());
+        gk_slabs_destroy(G);
+        return rc;
+    }
+    *out = G;
+    return GK_OK;
+}
+
+void gk_slabs_destroy(gk_slabs* G) {
+    if (!G) return;
+    if (!G->s.empty()) {
+        cudaSetDevice(G->s[0]->device);
+        if (G->stream) cudaStreamSynchronize(G->stream);
+    }
+    if (G->comm && G->nccl) G->nccl->CommDestroy(G->comm);
+    cudaFree(G->dsd);
+    cudaFree(G->xbuf);
+    cudaFree(G->red);
+    for (gk_handle* h : G->s) gk_destroy(h);
+    delete G;
+}
+
+int gk_slabs_upload_cons(gk_slabs* G, const double* cons) {
+    Range range("gk_slabs_upload_cons");
+    if (!G || !cons) return GK_ERR_INVALID;
+    const gk::Geom& g0 = G->s[0]->ctx.g;
+    const size_t lenx = g0.lenx, lenz = g0.lenz, leny_all = (size_t)G->gd.ny + 2 * g0.ng;
+    for (size_t k = 0; k < G->s.size(); ++k) {
+        gk_handle* h = G->s[k];
+        const size_t leny = h->ctx.g.leny;
+        // the slab's rows j0 .. j0 + leny - 1 of the whole grid, ghosts included
+        std::vector<double> part(5 * lenz * leny * lenx);
+        for (size_t v = 0; v < 5 * lenz; ++v)
+            std::memcpy(part.data() + v * leny * lenx,
+                        cons + (v * leny_all + (size_t)G->j0[k]) * lenx,
+                        sizeof(double) * leny * lenx);
+        int rc = gk_upload_cons(h, part.data());
+        if (rc != GK_OK) return sfail(G, rc, h->err);
+    }
+    return slabs_check_ready(G);
+}
+
+int gk_slabs_download_cons(gk_slabs* G, double* cons) {
+    Range range("gk_slabs_download_cons");
+    int rc = slabs_check_ready(G);
+    if (rc != GK_OK) return rc;
+    if (!cons) return GK_ERR_INVALID;
+    GK_SCUDA(G, cudaStreamSynchronize(G->stream));
+    const gk::Geom& g0 = G->s[0]->ctx.g;
+    const size_t lenx = g0.lenx, lenz = g0.lenz, ng = g0.ng;
+    const size_t leny_all = (size_t)G->gd.ny + 2 * ng;
+    for (size_t k = 0; k < G->s.size(); ++k) {
+        gk_handle* h = G->s[k];
+        const size_t leny = h->ctx.g.leny;
+        std::vector<double> part(5 * lenz * leny * lenx);
+        rc = gk_download_cons(h, part.data());
+        if (rc != GK_OK) return sfail(G, rc, h->err);
+        // active rows; the ghost rows too where the slab ends the grid
+        const int gk_ = G->first + (int)k;
+        const size_t r0 = gk_ == 0 ? 0 : ng;
+        const size_t r1 = gk_ == G->nslab - 1 ? leny : leny - ng;
+        for (size_t v = 0; v < 5 * lenz; ++v)
+            std::memcpy(cons + (v * leny_all + (size_t)G->j0[k] + r0) * lenx,
+                        part.data() + (v * leny + r0) * lenx, sizeof(double) * (r1 - r0) * lenx);
+    }
+    return GK_OK;
+}
+
+int gk_slabs_run_steps(gk_slabs* G, int nsteps, int* done) {
+    Range range("gk_slabs_run_steps");
+    int rc = slabs_check_ready(G);
+    if (rc != GK_OK) return rc;
+    if (done) *done = 0;
+    if (nsteps <= 0) return GK_OK;
+    const int before = G->s[0]->htm->step;
+    rc = slabs_run(G, 0.0, nsteps);
+    if (done) *done = G->s[0]->htm->step - before;
+    return rc;
+}
+
+int gk_slabs_advance(gk_slabs* G, double dtoutput, double* t, int* step, int* is_continue) {
+    Range range("gk_slabs_advance");
+    int rc = slabs_check_ready(G);
+    if (rc != GK_OK) return rc;
+    rc = slabs_run(G, dtoutput, 0);
+    const gk::DevTime& c = *G->s[0]->htm;
+    if (t) *t = c.t;
+    if (step) *step = c.step;
+    if (is_continue) *is_continue = c.is_continue;
+    return rc;
+}
+
+int gk_slabs_dt_log(gk_slabs* G, double* buf, int cap, int* n) {
+    if (!G || G->s.empty()) return GK_ERR_INVALID;
+    GK_SCUDA(G, cudaStreamSynchronize(G->stream));
+    return gk_dt_log(G->s[0], buf, cap, n);
+}
+
+int gk_slabs_info(gk_slabs* G, int* nslab_local, int* first, int* j0, int* rows) {
+    if (!G || G->s.empty()) return GK_ERR_INVALID;
+    if (nslab_local) *nslab_local = (int)G->s.size();
+    if (first) *first = G->first;
+    if (j0) *j0 = G->j0[0];
+    if (rows) *rows = G->ny[0];
+    return GK_OK;
+}
+
+const char* gk_slabs_last_error(const gk_slabs* G) { return G ? G->err.c_str() : ""; }
+
+}  // extern "C"

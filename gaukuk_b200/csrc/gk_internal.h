@@ -83,6 +83,9 @@ struct Phys {
     // Immersed body (immersed.cpp): nshell shell cells (0 = none).
     const Shell* shells;
     int nshell;
+    // A slab of a grid split in y: the last stage leaves the step epilogue
+    // to launch_epilogue, which runs after the CFL maximum over all slabs.
+    int defer_epilogue;
 };
 
 // Device-resident clock of Sim::Advance (sim.cpp:69-117).  Written by the
@@ -157,6 +160,38 @@ void launch_flux_correct(const float* model, const double* W, double* F, const G
                          const Phys& ph, const DevTime* tm, int dir, const FluxGate& gate,
                          unsigned* fired, cudaStream_t s);
 
+// One slab of a grid split into y-slabs, as the halo and reduction kernels
+// of gk_slab.cu read it: its three state buffers (A, B, C; C null without
+// RK3), its clock, its row range and its neighbours (slab indices, -1 where
+// the side is a physical boundary filled by the ghost fill).
+struct SlabDev {
+    double* buf[3];
+    DevTime* tm;
+    long long vstride;
+    int jb, je;          // active rows [jb, je) in the slab's own indices
+    int lower, upper;
+};
+
+// Halo exchange between the slabs of one process (same device): the two
+// ghost rows below and above every slab, all five planes, active columns,
+// copied from its neighbours' active rows in buffer `role` (0 A, 1 B, 2 C).
+void launch_slab_halo(const SlabDev* sd, int n, int role, const Geom& g, cudaStream_t s);
+// The CFL maximum over slabs: which = 0 the running maximum of a step
+// (cmax_acc, before the deferred epilogue), 1 the maximum of the uploaded
+// states (cmax_last, before a run begins); status words are combined.
+void launch_slab_reduce(const SlabDev* sd, int n, int which, cudaStream_t s);
+// Across processes: the rows a slab sends down (its first two active rows)
+// and up (its last two) packed into two buffers of 5 x 2 x nx doubles, the
+// rows it receives unpacked into its ghost rows (null: a physical side).
+void launch_slab_pack(const double* u, double* send_lo, double* send_hi, const Geom& g,
+                      const DevTime* tm, cudaStream_t s);
+void launch_slab_unpack(double* u, const double* recv_lo, const double* recv_hi, const Geom& g,
+                        const DevTime* tm, cudaStream_t s);
+// {CFL maximum bits, status} of one slab to and from the all-reduce buffer.
+void launch_slab_red_pack(const DevTime* tm, unsigned long long* red, int which, cudaStream_t s);
+void launch_slab_red_unpack(DevTime* tm, const unsigned long long* red, int which,
+                            cudaStream_t s);
+
 // Kernel classes, for per-kernel profiling.
 enum KClass { K_BC = 0, K_C2P, K_FLUX, K_UPDATE, K_KICK, K_CFL, K_STAGE, K_BEGIN, K_NCLASS };
 static const char* const kClassNames[K_NCLASS] = {
@@ -184,6 +219,7 @@ static const char* const kClassNames[K_NCLASS] = {
     void launch_stage2d(const gk::Ctx& c, const double* uc, const double* u0, double* out,     \
                         int kind, double c1, double c2, double c3, cudaStream_t s);            \
     void launch_begin(const gk::Ctx& c, double dtoutput, int steps, cudaStream_t s);           \
+    void launch_epilogue(const gk::Ctx& c, cudaStream_t s);                                    \
     void launch_mtz_check(const gk::Ctx& c, const double* u, int* flag, cudaStream_t s);       \
     void launch_ens_stage(int threads, int kind, int plm, const gk::EnsInst* inst,             \
                           const int2* tiles, int ntiles, unsigned* counter, double c1,          \

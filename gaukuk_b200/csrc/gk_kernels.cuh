@@ -1,8 +1,9 @@
 // gk_kernels.cuh -- the device kernels of one arithmetic mode.
 //
-// Included by gk_kernels_parity.cu (GK_NS = gk_parity, GK_SEL = false,
+// Included by gk_kernels_parity.cu (GK_NS = gk_parity, GK_SEL = 2,
 // compiled with -fmad=false) and gk_kernels_fast.cu (GK_NS = gk_fast,
-// GK_SEL = true, FMA contraction allowed).
+// GK_SEL = 1, FMA contraction allowed); GK_SEL is the HLLC side selection
+// of gk_physics.cuh.
 //
 // Two implementations of one RK stage share the pointwise physics:
 //   * the generic path, one kernel per reference phase (ghost fill,
@@ -39,7 +40,7 @@ using gk::DevTime;
 using gk::Geom;
 using gk::Phys;
 
-constexpr bool kSel = GK_SEL;
+constexpr int kSel = GK_SEL;
 
 __device__ __forceinline__ long long sidx(const Geom& g, int k, int j, int i) {
     return (long long)(k - g.kofs) * g.kstride + (long long)j * g.pitch + i;
@@ -75,6 +76,7 @@ __device__ __forceinline__ void bc_fill_one(double* __restrict__ u, const Geom& 
     else if (dir == 1) { cj = gc; sj = sc; ci = si = g.ib + a; ck = sk = g.kb + b; }
     else { ck = gc; sk = sc; ci = si = g.ib + a; cj = sj = g.jb + b; }
     const long long dst = sidx(g, ck, cj, ci), src = sidx(g, sk, sj, si);
+    if (type == 5) return;  // a slab's side filled by the halo exchange (gk_slab.cu)
     if (type == 4) {
         // FixedBD* (fixed.cpp:16-176): the ghost keeps its value at enrollment
         // (the host refuses to run a type-4 side without data; never read null)
@@ -332,7 +334,7 @@ __device__ __forceinline__ void floors4(double (&r)[4], const Phys& ph, DevTime*
 // floors4 that also returns the reciprocal density of the result (for the
 // CFL speed of the same cell).
 __device__ __forceinline__ double floors4_inv(double (&r)[4], const Phys& ph, DevTime* tm) {
-    if (r[0] < ph.dmin) {
+    if (GK_BELOW(r[0], ph.dmin)) {
         r[0] = ph.dmin;
         r[1] = 0.0;
         r[2] = 0.0;
@@ -343,7 +345,7 @@ __device__ __forceinline__ double floors4_inv(double (&r)[4], const Phys& ph, De
     double inv_den = GK_RCP(r[0]);
     double ke = 0.5 * inv_den * (r[1] * r[1] + r[2] * r[2]);
     double press = ph.gm1 * (r[3] - ke);
-    if (press < ph.pmin) {
+    if (GK_BELOW(press, ph.pmin)) {
         r[3] = ph.pmin / ph.gm1 + ke;
         atomicAdd(&tm->floor_pre, 1ull);
     }
@@ -478,10 +480,16 @@ __device__ __forceinline__ double cell_cmax_inv(double mx, double my, double e, 
     double vx = mx * denInv, vy = my * denInv;
     double engKin = 0.5 * (vx * mx + vy * my);
     double pres = ph.gm1 * (e - engKin);
-    pres = (pres > ph.pmin) ? pres : ph.pmin;
+    pres = GK_BELOW(ph.pmin, pres) ? pres : ph.pmin;
     double cs = GK_SQRT(ph.gamma * pres * denInv);
     double local = fabs(vx) + cs;
+#if GK_FASTMATH
+    // both non-negative: their bit patterns order like the values
+    const double other = fabs(vy) + cs;
+    local = __double_as_longlong(local) < __double_as_longlong(other) ? other : local;
+#else
     local = smax(local, fabs(vy) + cs);
+#endif
     return local;
 }
 
@@ -579,6 +587,13 @@ __global__ void k_begin(DevTime* tm, Geom g, Phys ph, double dtoutput, int steps
     begin_one(tm, g, ph, dtoutput, steps);
 }
 
+// The step epilogue of a slab whose last stage deferred it: cmax_acc holds
+// the maximum over every slab of the grid by now.
+__global__ void k_epilogue(DevTime* tm, Geom g, Phys ph) {
+    if (!tm->active) return;
+    step_epilogue(tm, g, ph, 1);
+}
+
 __global__ void k_mtz_check(const double* __restrict__ u, Geom g, int* flag) {
     const long long ncell = (long long)g.nx * g.ny * g.nz;
     for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < ncell;
@@ -619,14 +634,14 @@ struct Q4 {
 
 __device__ __forceinline__ W4 c2p4(const Q4& q, const Phys& ph) {
     W4 w;
-    double d = smax(q.d, ph.dmin);
+    double d = GK_FLOOR(q.d, ph.dmin);
     w.r = d;
     double denInv = GK_RCP(d);
     w.vx = q.mx * denInv;
     w.vy = q.my * denInv;
     double engKin = 0.5 * denInv * (q.mx * q.mx + q.my * q.my);
     double pre = ph.gm1 * (q.e - engKin);
-    w.p = (pre > ph.pmin) ? pre : ph.pmin;
+    w.p = GK_BELOW(ph.pmin, pre) ? pre : ph.pmin;
     return w;
 }
 
@@ -1133,9 +1148,14 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
             unsigned long long m = sm.wmax[0];
             for (int w = 1; w < NT / 32; ++w) m = sm.wmax[w] > m ? sm.wmax[w] : m;
             atomicMax(&tm->cmax_acc, m);
-            __threadfence();
-            const unsigned int prev = atomicAdd(&tm->done_ctas, 1u);
-            sm.last = (prev == tiles_total - 1);
+            sm.last = false;
+            if (!ph.defer_epilogue) {
+                // a slab of a split grid runs its epilogue after the max over
+                // all slabs (launch_epilogue)
+                __threadfence();
+                const unsigned int prev = atomicAdd(&tm->done_ctas, 1u);
+                sm.last = (prev == tiles_total - 1);
+            }
         }
         __syncthreads();
         if (sm.last && t == 0) {
@@ -1438,6 +1458,8 @@ void launch_ens_bc(const gk::EnsInst* inst, int n, int which, int max_count, cud
 void launch_ens_begin(const gk::EnsInst* inst, int n, double dtoutput, int steps, cudaStream_t s) {
     k_ens_begin<<<(n + 63) / 64, 64, 0, s>>>(inst, n, dtoutput, steps);
 }
+
+void launch_epilogue(const Ctx& c, cudaStream_t s) { k_epilogue<<<1, 1, 0, s>>>(c.tm, c.g, c.ph); }
 
 void launch_begin(const Ctx& c, double dtoutput, int steps, cudaStream_t s) {
     k_begin<<<1, 1, 0, s>>>(c.tm, c.g, c.ph, dtoutput, steps);

@@ -1,7 +1,7 @@
 // Kernels in fast mode: FMA contraction allowed, only the selected HLLC side
 // evaluated, branch-free refined reciprocal / square root (gk_physics.cuh).
 #define GK_NS gk_fast
-#define GK_SEL true
+#define GK_SEL 1
 #define GK_FASTMATH 1
 #include "gk_kernels.cuh"
 

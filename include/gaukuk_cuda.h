@@ -312,6 +312,16 @@ int gk_tap_substeps(gk_handle* h, int nsub, double dt_sub, int ratio, double* fx
  * device. */
 int gk_fastmath_check(int n, unsigned long long seed, double* worst3);
 
+/* Diagnostic of the PARITY mode arithmetic (no counterpart in the reference):
+ * its inline correctly rounded quotient and square root against CUDA's IEEE
+ * `/` and sqrt() over n random argument pairs (every exponent, zeros,
+ * subnormals, infinities, NaNs and powers of two included, half of them
+ * quotients near 1).  counts5 = {division results whose bits differ,
+ * divisions sent to the IEEE operation, roots whose bits differ, roots sent
+ * to the IEEE operation, pairs tried}; the differing counts must be 0.  Runs
+ * on the current device. */
+int gk_paritymath_check(long long n, unsigned long long seed, unsigned long long* counts5);
+
 /* One RK2 time step of a 2D problem (vz = 0, gz = 0) on a caller-owned
  * device state, for callers that cannot allocate device memory while they
  * run: their memory comes from their own pool or arena, or their budget is
@@ -343,6 +353,53 @@ int gk_fastmath_check(int n, unsigned long long seed, double* worst3);
  * overlaps on one GPU race on it. */
 int gk_rk2_step_noalloc(const gk_grid_desc* grid, const gk_phys_desc* phys, double* state,
                         double dtmax, double* dt_used, void* stream);
+
+/* ---- One 2D grid split into y-slabs (scale-out of Sim::Advance) ----
+ * No counterpart in the reference, which runs one grid in one process
+ * (sim.cpp:69-117); the arithmetic is Sim::Advance's over the whole grid.
+ * The ny active rows are split into nslab slabs of ny/nslab rows (the first
+ * ny % nslab take one more).  Per RK stage every slab's two ghost rows on
+ * each side come from its neighbours' active rows (a ring under periodic y);
+ * per step the CFL maximum is taken over all slabs, so every slab takes the
+ * whole grid's dt.  Results (state and dt sequence) equal the undivided
+ * grid's bit for bit.  Needs the fused 2D path: 2D, RK2 or RK3, vz = 0,
+ * gz = 0, no point masses, immersed body, fixed sides or flux model; a
+ * periodic y side needs a periodic partner; every slab needs >= 2 rows. */
+typedef struct gk_slabs gk_slabs;
+
+/* Rows and neighbours of slab k of nslab over ny active rows: first active
+ * row j0 (0-based), row count, lower and upper neighbour slab (-1: a side of
+ * the grid, filled by the ghost fill).  Host only. */
+int gk_slab_layout(int ny, int nslab, int k, int periodic, int* j0, int* rows, int* lower,
+                   int* upper);
+/* nslab slabs in this process, on phys->device, exchanging through device
+ * copies on one stream (a grid emulated as slabs on one GPU, or slabs that
+ * share a GPU). */
+int gk_slabs_create(const gk_grid_desc* grid, const gk_phys_desc* phys, int nslab, gk_slabs** out);
+/* One slab per process (rank of nranks, slab index = rank) on phys->device,
+ * exchanging through NCCL (libnccl.so.2, loaded at the first call): the
+ * rows are sent and received once per stage, the CFL speed is all-reduced
+ * (max) once per step.  id128: a 128-byte NCCL unique id made by one process
+ * with gk_slabs_nccl_id and passed to all.  Every process must make the same
+ * calls in the same order (they take part in the same collectives). */
+int gk_slabs_nccl_id(void* id128);
+int gk_slabs_create_nccl(const gk_grid_desc* grid, const gk_phys_desc* phys, int nranks, int rank,
+                         const void* id128, gk_slabs** out);
+void gk_slabs_destroy(gk_slabs* s);
+/* The whole grid's state in the reference layout (NVar x lenz x (ny+4) x
+ * lenx): each slab of this process takes its rows.  Download writes this
+ * process's active rows (and the grid's own ghost rows where its slabs end
+ * the grid) and leaves the other rows of `cons` as they are. */
+int gk_slabs_upload_cons(gk_slabs* s, const double* cons);
+int gk_slabs_download_cons(gk_slabs* s, double* cons);
+/* Sim::Advance(dtoutput) of the whole grid, and a fixed step count. */
+int gk_slabs_advance(gk_slabs* s, double dtoutput, double* t, int* step, int* is_continue);
+int gk_slabs_run_steps(gk_slabs* s, int nsteps, int* done);
+/* The whole grid's dt sequence (every slab takes the same steps). */
+int gk_slabs_dt_log(gk_slabs* s, double* buf, int cap, int* n);
+/* This process's slabs: count, index of the first, its first row and rows. */
+int gk_slabs_info(gk_slabs* s, int* nslab_local, int* first, int* j0, int* rows);
+const char* gk_slabs_last_error(const gk_slabs* s);
 
 /* Text for a status code, and the last failure message on a handle. */
 const char* gk_strerror(int status);

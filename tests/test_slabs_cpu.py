@@ -1,0 +1,90 @@
+"""Host logic of the y-slab split, on CPU (no device needed).
+
+* The partition: every active row belongs to exactly one slab, the first
+  ny % n slabs take one row more, neighbours form a chain (a ring under
+  periodic y; a single periodic slab is its own neighbour).
+* Two gloo ranks as separate processes (127.0.0.1): rank 0 makes the
+  128-byte NCCL id, both ranks end up with the same bytes, and both compute
+  the same layout of the whole grid, each knowing its own slab's rows and
+  its neighbour ranks -- the information every rank needs before the first
+  NCCL exchange, which must pair sends and receives between the right ranks.
+"""
+import multiprocessing as mp
+import os
+import socket
+import time
+
+import pytest
+
+
+def test_partition_covers_every_row_once():
+    from gaukuk_b200.slabs import layout
+    for ny in (2, 7, 100, 4096, 3072):
+        for n in (1, 2, 3, 5, 8):
+            if ny // n < 2:
+                continue
+            for periodic in (False, True):
+                rows = []
+                for k in range(n):
+                    j0, cnt, lo, up = layout(ny, n, k, periodic)
+                    assert cnt in (ny // n, ny // n + 1) and cnt >= 2
+                    rows.extend(range(j0, j0 + cnt))
+                    assert lo == (k - 1 if k > 0 else (n - 1 if periodic else -1))
+                    assert up == (k + 1 if k < n - 1 else (0 if periodic else -1))
+                assert rows == list(range(ny))
+                firsts = [layout(ny, n, k, periodic)[1] for k in range(n)]
+                assert firsts == sorted(firsts, reverse=True)  # the extra rows go first
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    try:
+        import datetime
+
+        import torch.distributed as dist
+
+        from gaukuk_b200.slabs import layout, nccl_id_broadcast
+        dist.init_process_group("gloo", rank=rank, world_size=world,
+                                timeout=datetime.timedelta(seconds=10))
+        nid = nccl_id_broadcast(dist, make_id=lambda: bytes(range(128)))
+        mine = layout(1030, world, rank, True)
+        q.put((rank, (nid, mine)))
+        dist.destroy_process_group()
+    except Exception as e:  # reported to the test
+        q.put((rank, "error: " + type(e).__name__ + ": " + str(e)))
+
+
+def test_two_ranks_agree_on_id_and_layout():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = {}
+    deadline = time.time() + 60
+    while len(out) < world and time.time() < deadline:
+        try:
+            r, v = q.get(timeout=max(0.1, deadline - time.time()))
+            out[r] = v
+        except Exception:
+            break
+    for p in procs:
+        p.join(timeout=10)
+        if p.is_alive():
+            p.kill()
+    assert sorted(out) == [0, 1], out
+    for r in range(world):
+        assert not isinstance(out[r], str), out[r]
+    assert out[0][0] == out[1][0] == bytes(range(128))
+    # rank 0 owns rows 0..514, rank 1 rows 515..1029; under periodic y each
+    # is the other's lower and upper neighbour
+    assert out[0][1] == (0, 515, 1, 1)
+    assert out[1][1] == (515, 515, 0, 0)
