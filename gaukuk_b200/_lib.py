@@ -88,6 +88,7 @@ SIGNATURES = {
     "gk_set_fixed_boundary": (ctypes.c_int, [_vp, _vp, ctypes.c_int]),
     "gk_set_immersed": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp]),
     "gk_set_point_gravity": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "gk_set_host_fill": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "gk_set_flux_model": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                          ctypes.c_float, ctypes.c_float]),
     "gk_flux_model_fired": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint)]),

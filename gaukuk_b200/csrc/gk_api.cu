@@ -137,6 +137,15 @@ struct gk_handle {
     cudaGraphExec_t gexec = nullptr;
     int graph_steps = 0;
     int graph_path = -1;
+    // sides whose ghost fill is a host routine (gk_set_host_fill)
+    struct HostFill {
+        int side, depth;
+        gk_host_fill_fn fn;
+        void* user;
+        double* cons;
+    };
+    std::vector<HostFill> host_fills;
+    int host_fill_rc = GK_OK;  // first failure inside a host fill, reported by the run
     std::string err;
 };
 
@@ -354,6 +363,66 @@ int choose_path(const gk_handle* h) {
             c.ph.npoint == 0 && !h->model) ? 1 : 0;
 }
 
+// Sides filled by host routines (gk_set_host_fill), after the device ghost
+// fill of buffer u: the stream is synchronised, the cells each routine may
+// read (its ghost strip and `depth` layers next to it, every transverse
+// index, every variable) are copied into its host array, the routines run in
+// UpdateBD's side order (boundary.cpp:127-142), and each side's ghost strip
+// (active transverse cells, as the routine writes it) goes back.  Skipped
+// once the run has stopped, like the kernels.
+int run_host_fills(gk_handle* h, double* u) {
+    const gk::Geom& g = h->ctx.g;
+    cudaStream_t s = h->stream;
+    GK_CUDA(h, cudaMemcpyAsync(&h->htm->active, &h->tm->active, sizeof(int),
+                               cudaMemcpyDeviceToHost, s));
+    GK_CUDA(h, cudaStreamSynchronize(s));
+    if (!h->htm->active) return GK_OK;
+    const int n3[3] = {g.nx, g.ny, g.nz};
+    const size_t db = sizeof(double);
+    // ranges along each direction: [lo, hi)
+    auto region = [&](int side, int depth, bool strip_only, int lo[3], int hi[3]) {
+        const int dir = side / 2, sd = side % 2;
+        const int len[3] = {g.lenx, g.leny, g.lenz};
+        const int beg[3] = {g.ib, g.jb, g.kb}, end[3] = {g.ie, g.je, g.ke};
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = strip_only ? beg[d] : 0;
+            hi[d] = strip_only ? end[d] : len[d];
+        }
+        // depth >= n + nghost: the whole extent along dir
+        const int reach = strip_only ? 0 : std::min(depth, n3[dir] + g.ng);
+        lo[dir] = sd == 0 ? 0 : std::max(0, end[dir] - reach);
+        hi[dir] = sd == 0 ? std::min(len[dir], g.ng + reach) : len[dir];
+    };
+    auto copy = [&](const gk_handle::HostFill& f, bool to_host) -> int {
+        int lo[3], hi[3];
+        region(f.side, f.depth, !to_host, lo, hi);
+        for (int n = 0; n < 5; ++n)
+            for (int k = std::max(lo[2], g.kofs); k < std::min(hi[2], g.kofs + g.nzs); ++k) {
+                double* ref = f.cons + ((size_t)(n * g.lenz + k) * g.leny + lo[1]) * g.lenx + lo[0];
+                double* dev = u + (size_t)kSlotOf[n] * g.vstride + (size_t)(k - g.kofs) * g.kstride +
+                              (size_t)lo[1] * g.pitch + lo[0];
+                const size_t w = db * (hi[0] - lo[0]);
+                if (to_host)
+                    GK_CUDA(h, cudaMemcpy2DAsync(ref, db * g.lenx, dev, db * g.pitch, w, hi[1] - lo[1],
+                                                 cudaMemcpyDeviceToHost, s));
+                else
+                    GK_CUDA(h, cudaMemcpy2DAsync(dev, db * g.pitch, ref, db * g.lenx, w, hi[1] - lo[1],
+                                                 cudaMemcpyHostToDevice, s));
+            }
+        return GK_OK;
+    };
+    int rc;
+    for (const auto& f : h->host_fills)
+        if ((rc = copy(f, true)) != GK_OK) return rc;
+    GK_CUDA(h, cudaStreamSynchronize(s));
+    for (const auto& f : h->host_fills) f.fn(f.user, f.cons);
+    for (const auto& f : h->host_fills)
+        if ((rc = copy(f, false)) != GK_OK) return rc;
+    // the host arrays are read again by the next fill: let the copies finish
+    GK_CUDA(h, cudaStreamSynchronize(s));
+    return GK_OK;
+}
+
 // One time step.  Kernel order per RK stage follows Sim::RK2_/RK3_/
 // ForwardEuler_ (rk2.cpp:11-23, rk3.cpp:11-29, forward_euler.cpp:11-18),
 // wrapped in the Strang half kicks of sim.cpp:85-91; the step ends with the
@@ -376,6 +445,11 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
         stmt;           \
         mark(-1);       \
     } while (0)
+    // ghost fill of a buffer: the device sides, then any host-routine sides
+    auto fill = [&](double* u) {
+        k.bc(c, u, s);
+        if (!h->host_fills.empty() && h->host_fill_rc == GK_OK) h->host_fill_rc = run_host_fills(h, u);
+    };
     double* A = h->A;
     double* B = h->B;
     double* Cb = h->C;
@@ -387,14 +461,14 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
         // without a kick after it the last stage also reduces the CFL speed
         const bool kicks = c.ph.has_grav || c.ph.npoint;
         const int last = kicks ? 1 : 2;
-        GK_L(gk::K_BC, k.bc(c, A, s));
+        GK_L(gk::K_BC, fill(A));
         GK_L(gk::K_FLUX, k.zflux(c, A, h->F3, s));
         GK_L(gk::K_STAGE, k.stage3d(c, A, nullptr, B, h->F3, 0, 1.0, 1.0, 0.0, s));
-        GK_L(gk::K_BC, k.bc(c, B, s));
+        GK_L(gk::K_BC, fill(B));
         GK_L(gk::K_FLUX, k.zflux(c, B, h->F3, s));
         if (integ == 3) {
             GK_L(gk::K_STAGE, k.stage3d(c, B, A, Cb, h->F3, 1, 0.75, 0.25, 0.25, s));
-            GK_L(gk::K_BC, k.bc(c, Cb, s));
+            GK_L(gk::K_BC, fill(Cb));
             GK_L(gk::K_FLUX, k.zflux(c, Cb, h->F3, s));
             GK_L(gk::K_STAGE, k.stage3d(c, Cb, A, A, h->F3, last, frac13, 2 * frac13, 2 * frac13, s));
         } else {
@@ -409,12 +483,12 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
     if (h->path == 1) {
         // the last stage also applies the second half kick, the CFL
         // reduction and the step epilogue
-        GK_L(gk::K_BC, k.bc(c, A, s));
+        GK_L(gk::K_BC, fill(A));
         GK_L(gk::K_STAGE, k.stage2d(c, A, nullptr, B, 0, 1.0, 1.0, 0.0, s));
-        GK_L(gk::K_BC, k.bc(c, B, s));
+        GK_L(gk::K_BC, fill(B));
         if (integ == 3) {
             GK_L(gk::K_STAGE, k.stage2d(c, B, A, Cb, 1, 0.75, 0.25, 0.25, s));
-            GK_L(gk::K_BC, k.bc(c, Cb, s));
+            GK_L(gk::K_BC, fill(Cb));
             GK_L(gk::K_STAGE, k.stage2d(c, Cb, A, A, 2, frac13, 2 * frac13, 2 * frac13, s));
         } else {
             GK_L(gk::K_STAGE, k.stage2d(c, B, A, A, 2, 0.5, 0.5, 0.5, s));
@@ -434,17 +508,17 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
                                                      h->gate, h->fired, s));
         }
     };
-    GK_L(gk::K_BC, k.bc(c, A, s));
+    GK_L(gk::K_BC, fill(A));
     fluxes(A);
     if (integ == 1) {
         GK_L(gk::K_UPDATE, k.update(c, nullptr, A, A, h->F1, h->F2, h->F3, 0, 1.0, 1.0, 0.0, s));
     } else {
         GK_L(gk::K_UPDATE, k.update(c, nullptr, A, B, h->F1, h->F2, h->F3, 0, 1.0, 1.0, 0.0, s));
-        GK_L(gk::K_BC, k.bc(c, B, s));
+        GK_L(gk::K_BC, fill(B));
         fluxes(B);
         if (integ == 3) {
             GK_L(gk::K_UPDATE, k.update(c, A, B, B, h->F1, h->F2, h->F3, 1, 0.75, 0.25, 0.25, s));
-            GK_L(gk::K_BC, k.bc(c, B, s));
+            GK_L(gk::K_BC, fill(B));
             fluxes(B);
             GK_L(gk::K_UPDATE, k.update(c, A, B, A, h->F1, h->F2, h->F3, 1, frac13, 2 * frac13,
                                         2 * frac13, s));
@@ -819,7 +893,26 @@ int gk_io_bytes(const gk_handle* h, long long* upload, long long* download) {
     return GK_OK;
 }
 
+// Runs with host-routine sides: no graph (each ghost fill returns to the
+// host), every step enqueued and finished in turn.
+static int run_loop_host(gk_handle* h, double dtoutput, int nsteps) {
+    h->host_fill_rc = GK_OK;
+    h->ks->begin(h->ctx, dtoutput, nsteps, h->stream);
+    GK_CUDA(h, cudaGetLastError());
+    for (int i = 0; nsteps <= 0 || i < nsteps; ++i) {
+        enqueue_step(h, nullptr);
+        if (h->host_fill_rc != GK_OK) return h->host_fill_rc;
+        GK_CUDA(h, cudaMemcpyAsync(&h->htm->active, &h->tm->active, sizeof(int),
+                                   cudaMemcpyDeviceToHost, h->stream));
+        GK_CUDA(h, cudaStreamSynchronize(h->stream));
+        if (!h->htm->active) break;
+    }
+    GK_CUDA(h, cudaGetLastError());
+    return pull_time(h);
+}
+
 static int run_loop(gk_handle* h, double dtoutput, int nsteps, bool wait) {
+    if (!h->host_fills.empty()) return run_loop_host(h, dtoutput, nsteps);
     int rc = ensure_graph(h);
     if (rc != GK_OK) return rc;
     h->ks->begin(h->ctx, dtoutput, nsteps, h->stream);
@@ -1205,7 +1298,9 @@ int gk_ens_create(gk_handle* const* handles, int n, gk_ensemble** out) {
     for (int i = 0; i < n; ++i) {
         gk_handle* h = handles[i];
         if (!h || !h->uploaded) return GK_ERR_STATE;
-        if (h->path != 1 || h->ctx.ph.integrator != 2 || h->ctx.ph.fix_inner) return GK_ERR_UNSUPPORTED;
+        if (h->path != 1 || h->ctx.ph.integrator != 2 || h->ctx.ph.fix_inner ||
+            !h->host_fills.empty())
+            return GK_ERR_UNSUPPORTED;
         // an instance's physics is copied here: fixed data must already be set
         for (int s = 0; s < 6; ++s)
             if (h->ctx.ph.bc[s] == 4 && !h->ctx.ph.fixed_bd) return GK_ERR_STATE;
@@ -1444,6 +1539,35 @@ extern "C" int gk_set_fixed_boundary(gk_handle* h, const double* snapshot, int f
     ph.inner[1] = static_cast<int>(g.ib + 0.75 * (g.ie - g.ib));
     ph.inner[2] = static_cast<int>(g.jb + 0.25 * (g.je - g.jb));
     ph.inner[3] = static_cast<int>(g.jb + 0.75 * (g.je - g.jb));
+    return physics_changed(h);
+}
+
+extern "C" int gk_set_host_fill(gk_handle* h, int side, int depth, gk_host_fill_fn fn, void* user,
+                                double* cons) {
+    if (!h || side < 0 || side > 5) return GK_ERR_INVALID;
+    gk::Phys& ph = h->ctx.ph;
+    const int n3[3] = {h->ctx.g.nx, h->ctx.g.ny, h->ctx.g.nz};
+    auto& v = h->host_fills;
+    for (size_t i = 0; i < v.size(); ++i)
+        if (v[i].side == side) {
+            v.erase(v.begin() + i);
+            break;
+        }
+    if (!fn) {
+        // back to the side's own ghost fill
+        gk_handle fresh;
+        fresh.gd = h->gd;
+        fresh.pd = h->pd;
+        if (build_ctx(&fresh) == GK_OK) ph.bc[side] = fresh.ctx.ph.bc[side];
+        return physics_changed(h);
+    }
+    if (!cons || depth < 1) return fail(h, GK_ERR_INVALID, "a host fill needs its array and depth >= 1");
+    if (n3[side / 2] <= 1) return fail(h, GK_ERR_INVALID, "that direction has one cell");
+    v.push_back({side, depth, fn, user, cons});
+    std::sort(v.begin(), v.end(), [](const gk_handle::HostFill& a, const gk_handle::HostFill& b) {
+        return a.side < b.side;
+    });
+    ph.bc[side] = 5;  // the device ghost fill leaves the side alone
     return physics_changed(h);
 }
 

@@ -351,14 +351,36 @@ bool SameBits(Real a, Real b) {
 // run and NaN in the other, so partial fills are caught; so are routines
 // that copy or scale state values.  A routine that throws, or anything else,
 // keeps the run on the host.
+void Boundary::RunSide(int s, TArray<Real>& cons, const Grid& grid,
+                       const EquationOfState& eos) const {
+    const BoundaryFunc* fn[6] = {&Bdxl, &Bdxr, &Bdyl, &Bdyr, &Bdzl, &Bdzr};
+    (*fn[s])(cons, grid, eos);
+}
+
+// How the device runs each self-defined side, from probes of its routine on
+// copies of the state:
+// * the routine must write only its side's ghost strip (ghost layers, active
+//   transverse cells): on arrays filled with -1e300 and with NaN, every other
+//   cell keeps the fill -- otherwise the run is refused;
+// * if its writes are the same bits on the state and on both fills, they do
+//   not depend on the state: the side becomes a fixed side with those values;
+// * else it runs on the host at every ghost fill.  Its read depth is the
+//   smallest D in 1, 2, 4, ... such that the routine writes the same bits
+//   when every cell farther than D layers from the strip (across the whole
+//   transverse extent) is replaced by -1e300 or by NaN; the library copies
+//   the strip and those D layers to the host before each call.
 bool Boundary::PrepareDevice(const TArray<Real>& cons, const Grid& grid,
                              const EquationOfState& eos, std::string* why) {
     static const char* names[6] = {"x left", "x right", "y left", "y right", "z left", "z right"};
     const BoundaryFunc* fn[6] = {&Bdxl, &Bdxr, &Bdyl, &Bdyr, &Bdzl, &Bdzr};
-    for (int s = 0; s < 6; ++s) deviceTypes_[s] = types_[s];
+    for (int s = 0; s < 6; ++s) {
+        deviceTypes_[s] = types_[s];
+        hostDepth_[s] = 0;
+    }
     deviceFixedSet_ = fixedEnrolled_;
     if (fixedEnrolled_) deviceFixed_ = fixedData_;
     const int sides = grid.nz > 1 ? 6 : 4;  // UpdateBD fills z sides in 3D only
+    const Real fill[2] = {-1e300, std::numeric_limits<Real>::quiet_NaN()};
     for (int s = 0; s < sides; ++s) {
         if (!((custom_ >> s) & 1)) continue;
         const int dir = s / 2, side = s % 2;
@@ -370,8 +392,12 @@ bool Boundary::PrepareDevice(const TArray<Real>& cons, const Grid& grid,
         auto inside = [&](int k, int j, int i) {
             return i >= lo[0] && i < hi[0] && j >= lo[1] && j < hi[1] && k >= lo[2] && k < hi[2];
         };
+        // distance (in layers) of coordinate c along dir from the strip
+        auto layers = [&](int c) {
+            return side == 0 ? c - grid.nGhost + 1 : grid.nGhost + n[dir] - c;
+        };
+        auto coord = [&](int k, int j, int i) { return dir == 0 ? i : (dir == 1 ? j : k); };
         TArray<Real> probe[3] = {cons, cons, cons};
-        const Real fill[2] = {-1e300, std::numeric_limits<Real>::quiet_NaN()};
         for (int p = 1; p < 3; ++p) {
             Real* d = probe[p].data();
             for (size_t q = 0; q < probe[p].GetSize(); ++q) d[q] = fill[p - 1];
@@ -383,25 +409,50 @@ bool Boundary::PrepareDevice(const TArray<Real>& cons, const Grid& grid,
                    " boundary cannot be probed for the device (" + e.what() + ")";
             return false;
         }
-        bool ok = true;
-        for (int v = 0; v < NVar && ok; ++v)
-            for (int k = 0; k < grid.lenz && ok; ++k)
-                for (int j = 0; j < grid.leny && ok; ++j)
-                    for (int i = 0; i < grid.lenx && ok; ++i) {
+        bool local = true, stationary = true;
+        for (int v = 0; v < NVar; ++v)
+            for (int k = 0; k < grid.lenz; ++k)
+                for (int j = 0; j < grid.leny; ++j)
+                    for (int i = 0; i < grid.lenx; ++i) {
                         const Real a = probe[0](v, k, j, i), b = probe[1](v, k, j, i),
                                    c = probe[2](v, k, j, i);
                         if (inside(k, j, i)) {
-                            ok = SameBits(a, b) && SameBits(a, c);
+                            stationary = stationary && SameBits(a, b) && SameBits(a, c);
                         } else {
-                            ok = SameBits(a, cons(v, k, j, i)) && SameBits(b, fill[0]) &&
-                                 SameBits(c, fill[1]);
+                            local = local && SameBits(a, cons(v, k, j, i)) && SameBits(b, fill[0]) &&
+                                    SameBits(c, fill[1]);
                         }
                     }
-        if (!ok) {
+        if (!local) {
             *why = std::string("the self-defined ") + names[s] +
-                   " boundary depends on the state or writes outside its ghost strip; it runs "
-                   "on the host only";
+                   " boundary writes outside its ghost strip; it runs on the host only";
             return false;
+        }
+        if (!stationary) {
+            // the routine reads the state: find how far from its strip
+            int depth = 0;
+            for (int d = 1; depth == 0; d *= 2) {
+                const int D = std::min(d, n[dir]);
+                bool same = true;
+                for (int f = 0; f < 2 && same; ++f) {
+                    TArray<Real> q = cons;
+                    for (int v = 0; v < NVar; ++v)
+                        for (int k = 0; k < grid.lenz; ++k)
+                            for (int j = 0; j < grid.leny; ++j)
+                                for (int i = 0; i < grid.lenx; ++i)
+                                    if (layers(coord(k, j, i)) > D) q(v, k, j, i) = fill[f];
+                    (*fn[s])(q, grid, eos);
+                    for (int v = 0; v < NVar && same; ++v)
+                        for (int k = lo[2]; k < hi[2] && same; ++k)
+                            for (int j = lo[1]; j < hi[1] && same; ++j)
+                                for (int i = lo[0]; i < hi[0] && same; ++i)
+                                    same = SameBits(q(v, k, j, i), probe[0](v, k, j, i));
+                }
+                if (same) depth = D;
+                else if (D == n[dir]) depth = n[dir] + grid.nGhost;  // reads the far ghosts: all of it
+            }
+            hostDepth_[s] = depth;
+            continue;
         }
         if (!deviceFixedSet_) {
             deviceFixed_.NewArray(NVar, grid.lenz, grid.leny, grid.lenx);

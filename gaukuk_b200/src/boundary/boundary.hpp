@@ -9,7 +9,9 @@
 // output; during Sim::Advance the device fills ghosts with the same rules:
 // fixed sides, the immersed body and the inner reset included.  The device
 // cannot call a hook's own routine: PrepareDevice turns one whose writes do
-// not depend on the state into a fixed side, and rejects the others.
+// not depend on the state into a fixed side; one that reads the state runs
+// on the host at every ghost fill, on the cells it was found to read.  A
+// routine that writes outside its side's ghost strip is rejected.
 #pragma once
 
 #include <functional>
@@ -59,6 +61,12 @@ public:
     // the fixed-side data (the enrolled snapshot with captured sides written
     // in; empty when no side is fixed).
     int DeviceType(int s) const { return deviceTypes_[s]; }
+    // After PrepareDevice: 0, or for a self-defined side that reads the state
+    // the number of cell layers next to its ghost strip that it reads (the
+    // library copies strip + layers to the host before each call).
+    int HostDepth(int s) const { return hostDepth_[s]; }
+    // Runs the routine installed for side s on cons.
+    void RunSide(int s, TArray<Real>& cons, const Grid& grid, const EquationOfState& eos) const;
     const TArray<Real>& DeviceFixedData() const { return deviceFixed_; }
     bool HasDeviceFixedData() const { return deviceFixedSet_; }
 
@@ -92,6 +100,7 @@ private:
     void ImmersedReflective(TArray<Real>& cons, const EquationOfState& eos) const;
 
     int deviceTypes_[6] = {0, 0, 0, 0, 0, 0};
+    int hostDepth_[6] = {0, 0, 0, 0, 0, 0};
     bool deviceFixedSet_ = false;
     TArray<Real> deviceFixed_;
 };

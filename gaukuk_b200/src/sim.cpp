@@ -110,6 +110,21 @@ void Sim::EnsureDevice() {
     double pm[11];
     const int npoint = srcTerm.PointParams(pm);
     if (npoint > 0) Check(dev_, gk_set_point_gravity(dev_, npoint, pm), "gk_set_point_gravity");
+    for (int s = 0; s < 6; ++s) {
+        if (boundary.HostDepth(s) <= 0) continue;
+        hostSides_[s] = HostSide{this, s};
+        Check(dev_, gk_set_host_fill(dev_, s, boundary.HostDepth(s), &Sim::HostFill, &hostSides_[s],
+                                     cons.data()),
+              "gk_set_host_fill");
+    }
+}
+
+// A self-defined side run by the library at a ghost fill: the library has
+// copied the cells the routine reads into cons and copies its ghost strip
+// back afterwards.
+void Sim::HostFill(void* user, double* /*cons*/) {
+    HostSide* h = static_cast<HostSide*>(user);
+    h->sim->boundary.RunSide(h->side, h->sim->cons, h->sim->grid, h->sim->eos);
 }
 
 // The reference's integrators end with cons.Swap(consTemp) (rk2.cpp:21,

@@ -87,6 +87,15 @@ private:
     std::vector<size_t> unwritten_;
     std::vector<Real> spare_;
     void SwapUnwritten();
+    // Self-defined sides that depend on the state run on the host at every
+    // ghost fill (gk_set_host_fill): the library calls HostFill with one of
+    // these, on cons.
+    struct HostSide {
+        Sim* sim;
+        int side;
+    };
+    HostSide hostSides_[6];
+    static void HostFill(void* user, double* cons);
 };
 
 }  // namespace Gaukuk

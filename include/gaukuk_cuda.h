@@ -93,6 +93,23 @@ void gk_destroy(gk_handle* h);
  * advance until the data are set. */
 int gk_set_fixed_boundary(gk_handle* h, const double* snapshot, int fix_inner);
 
+/* A self-defined side whose ghost values depend on the state
+ * (Boundary::EnrollSelfDefineBD*, boundary.hpp:28-45; the copy template of
+ * setup_example.cpp:120-140): a host routine fills it at every ghost fill.
+ * side 0..5 = x left, x right, y left, y right, z left, z right.  cons: the
+ * caller's reference-layout array the routine works on (NVar x lenz x leny x
+ * lenx, host).  Before each call the library copies into `cons` the side's
+ * ghost strip and the `depth` cell layers next to it (depth >= n + nghost:
+ * the whole extent), across the whole transverse extent and every variable;
+ * fn(user, cons) then fills the strip (ghost layers, active transverse
+ * cells), which is copied back.  The device fills the other sides first.  A
+ * handle with host sides runs its steps without a CUDA graph, returning to
+ * the host at every ghost fill.  fn = NULL removes the side's routine.  Not
+ * for ensembles. */
+typedef void (*gk_host_fill_fn)(void* user, double* cons);
+int gk_set_host_fill(gk_handle* h, int side, int depth, gk_host_fill_fn fn, void* user,
+                     double* cons);
+
 /* Point masses: SourceTerm::EnrollPointGravity (source.cpp:33-68) as the
  * Strang half kicks of PointGravity (point_gravity.cpp:11-92, n = 1) or
  * BinaryGravity (binary_gravity.cpp, n = 2), after the constant gravity.

@@ -54,10 +54,18 @@ def test_first_frame_is_clean_and_unchanged(name, drivers, tmp_path):
     assert (tmp_path / "cons_00000").read_bytes() == (plain / "cons_00000").read_bytes()
 
 
-def test_refused_side_probe_is_clean(drivers, tmp_path):
+@pytest.mark.parametrize("variant", ["inflowWide", "inflowCopies"])
+def test_side_probes_are_clean(variant, drivers, tmp_path):
+    """The probes of a self-defined side: the refused one (it writes corner
+    ghosts) and the depth search of one that reads the state."""
     p = Params(nx=16, ny=12, cfl=0.4, integrator=2, rc_order=2, bc=(3, 3, 3, 3, 1, 1),
                tmax=0.02, dtoutput=0.01, **P3)
-    (tmp_path / "run.in").write_text(p.to_in_text({"inflowCopies": 1}))
+    (tmp_path / "run.in").write_text(p.to_in_text({variant: 1}))
     r = _run(drivers["inflow_sides"], tmp_path)
-    assert "depends on the state" in r.stderr, r.stderr[-3000:]
-    assert "AddressSanitizer" not in r.stderr and "runtime error" not in r.stderr, r.stderr[-3000:]
+    if variant == "inflowWide":
+        assert "writes outside its ghost strip" in r.stderr, r.stderr[-3000:]
+    else:
+        assert "ghost strip" not in r.stderr, r.stderr[-3000:]
+    # UBSan reports read "<file>:<line>:<col>: runtime error: ..." (a CUDA
+    # error without a device only reads "CUDA runtime error")
+    assert "AddressSanitizer" not in r.stderr and ": runtime error:" not in r.stderr, r.stderr[-3000:]

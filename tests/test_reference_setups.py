@@ -126,29 +126,58 @@ def test_runs_match_the_reference(name, tmp_path):
                 assert err <= 1e-12, (f, v, err)
 
 
+INFLOW = Params(nx=32, ny=24, cfl=0.4, integrator=2, rc_order=2, bc=(3, 3, 3, 3, 1, 1),
+                tmax=0.02, dtoutput=0.01, **P3)
+
+
 @pytest.mark.parametrize("variant", ["copies", "wide", "constant"])
-def test_self_defined_sides_run_on_the_device_only_when_stationary(variant, tmp_path):
+def test_self_defined_sides_are_probed(variant, tmp_path):
     """A setup's own boundary routine cannot run on the device.  One that
     writes a constant inflow into its ghost strip
     (tests/setups/setup_inflow_sides.cpp) is captured as a fixed side; one
-    that copies the state, or that also writes the corner ghosts, is refused
-    with a message, before any device work, so this runs on the CPU too."""
+    that copies the state (the copy template of the reference's setup
+    files) passes the probe and runs on the host at every ghost fill; one
+    that also writes the corner ghosts is refused with a message, before any
+    device work, so this runs on the CPU too."""
     from gaukuk_b200 import _build_host
     src = os.path.join(ROOT, "tests", "setups", "setup_inflow_sides.cpp")
     exe = _build_host.build_hook(src, name="inflow_sides", out_dir=str(tmp_path))
-    p = Params(nx=16, ny=12, cfl=0.4, integrator=2, rc_order=2, bc=(3, 3, 3, 3, 1, 1),
-               tmax=0.02, dtoutput=0.01, **P3)
     keys = {"inflowCopies": int(variant == "copies"), "inflowWide": int(variant == "wide")}
-    (tmp_path / "run.in").write_text(p.to_in_text(keys))
+    (tmp_path / "run.in").write_text(INFLOW.to_in_text(keys))
     r = subprocess.run([exe, "-i", "run.in"], cwd=tmp_path, capture_output=True, text=True,
                        timeout=300)
-    refused = "depends on the state or writes outside its ghost strip" in r.stderr
-    if variant != "constant":
+    refused = "writes outside its ghost strip" in r.stderr
+    if variant == "wide":
         assert r.returncode != 0 and refused, r.stderr[-2000:]
     else:
         # past the probe: it runs on a GPU, or fails later for want of one
         assert not refused, r.stderr[-2000:]
         assert (tmp_path / "cons_00000").exists()
+
+
+@pytest.mark.gpu
+def test_state_dependent_side_matches_the_reference(tmp_path):
+    """The copy template (the x-left ghosts copy the first active column,
+    every variable), enrolled by a setup file: the host fill runs it between
+    device stages and every frame is byte-identical to the reference
+    build's, which runs the same file."""
+    from gaukuk_b200 import _build_host
+    ref = os.path.join(REF, "ref_strict_test_inflow_sides")
+    if not os.path.exists(ref):
+        pytest.skip("the reference build of the test hook is not here")
+    src = os.path.join(ROOT, "tests", "setups", "setup_inflow_sides.cpp")
+    ours = _build_host.build_hook(src, name="inflow_sides", out_dir=str(tmp_path))
+    text = INFLOW.to_in_text({"inflowCopies": 1})
+    a, b = tmp_path / "ref", tmp_path / "gpu"
+    a.mkdir(); b.mkdir()
+    (a / "run.in").write_text(text)
+    (b / "run.in").write_text(text)
+    _run(ref, ["-i", "run.in", "--frames", "--quiet"], a)
+    _run(ours, ["-i", "run.in"], b)
+    names = sorted(f for f in os.listdir(a) if f.startswith("cons_"))
+    assert len(names) >= 3 and names == sorted(f for f in os.listdir(b) if f.startswith("cons_"))
+    for f in names:
+        assert (a / f).read_bytes() == (b / f).read_bytes(), f
 
 
 PRIM_CASES = ["kh", "disk", "blast", "solid_body"]
