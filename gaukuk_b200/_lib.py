@@ -61,8 +61,6 @@ SIGNATURES = {
     "gk_profile_steps": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _dp,
                                         _ip, ctypes.c_int, _ip]),
     "gk_fastmath_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_ulonglong, _dp]),
-    "gk_paritymath_check": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_ulonglong,
-                                           ctypes.POINTER(ctypes.c_ulonglong)]),
     "gk_rk2_step_noalloc": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(PhysDesc),
                                            _vp, ctypes.c_double, _dp, _vp]),
     "gk_set_tiling": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),

@@ -27,9 +27,6 @@
 namespace gk_fast {
 int fastmath_check(int n, unsigned long long seed, double* host_worst3);
 }
-namespace gk_parity {
-int paritymath_check(long long n, unsigned long long seed, unsigned long long* host_out5);
-}
 
 namespace gk {
 
@@ -1097,10 +1094,6 @@ int gk_fastmath_check(int n, unsigned long long seed, double* worst3) {
     return gk_fast::fastmath_check(n, seed, worst3) == 0 ? GK_OK : GK_ERR_CUDA;
 }
 
-int gk_paritymath_check(long long n, unsigned long long seed, unsigned long long* counts5) {
-    if (n <= 0 || !counts5) return GK_ERR_INVALID;
-    return gk_parity::paritymath_check(n, seed, counts5) == 0 ? GK_OK : GK_ERR_CUDA;
-}
 
 const char* gk_strerror(int status) {
     switch (status) {

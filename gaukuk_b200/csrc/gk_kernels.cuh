@@ -1,6 +1,6 @@
 // gk_kernels.cuh -- the device kernels of one arithmetic mode.
 //
-// Included by gk_kernels_parity.cu (GK_NS = gk_parity, GK_SEL = 2,
+// Included by gk_kernels_parity.cu (GK_NS = gk_parity, GK_SEL = 0,
 // compiled with -fmad=false) and gk_kernels_fast.cu (GK_NS = gk_fast,
 // GK_SEL = 1, FMA contraction allowed); GK_SEL is the HLLC side selection
 // of gk_physics.cuh.

@@ -2,9 +2,9 @@
 //
 // Included inside the mode namespace (gk_parity / gk_fast).  Every
 // expression keeps the reference's association order.  The parity unit is
-// compiled with -fmad=false and uses correctly rounded division and square
-// root (IEEE on the GPU as on the host): results are bit-identical to the
-// reference built without -ffast-math.  The fast unit (GK_FASTMATH) lets the
+// compiled with -fmad=false and uses IEEE division and square root, which
+// are correctly rounded on the GPU as on the host: results are bit-identical
+// to the reference built without -ffast-math.  The fast unit (GK_FASTMATH) lets the
 // compiler contract to FMA and replaces division, reciprocal and square root
 // by the branch-free refinements below.
 #pragma once
@@ -73,94 +73,11 @@ __device__ __forceinline__ double floor_at(double x, double f) {
 #define GK_FLOOR(x, f) floor_at((x), (f))
 #define GK_BELOW(x, f) (__double_as_longlong(x) < __double_as_longlong(f))
 #else
-// Parity mode: correctly rounded quotient and square root (IEEE 754
-// round-to-nearest-even), so every result equals CUDA's `/` and sqrt() --
-// and the reference's -- bit for bit.  Each is inline straight-line code
-// with a verified result: a refined hardware approximation, one Markstein
-// correction with the exact residual (Markstein, IBM J. Res. Dev. 34(1),
-// 1990), then an exact acceptance test on a second residual; an input the
-// test cannot vouch for (zero, subnormal, infinite or NaN arguments,
-// results near the ends of the exponent range, an approximation that missed)
-// takes the compiler's IEEE operation instead, so the result is IEEE in
-// every case.
-//
-// Acceptance, quotient q of a/b: r = fma(-b, q, a) is exact when q is
-// within an ulp of a/b and nothing underflows (the residual of a faithful
-// quotient is representable), and q = RN(a/b) iff |r| < |b| ulp(q)/2: a
-// quotient of two doubles is never a midpoint, so there is no tie.  When q
-// is a power of two the spacing below it is half: the bound is then
-// |b| ulp(q)/4, a subset of the exact region.  If q missed by an ulp or
-// more, |r| >= |b| ulp(q) and the test fails however r rounds.
-//
-// Acceptance, root s of x: r = fma(-s, s, x) = x - s^2 is exact for a
-// faithful s (Boldo and Daumas, ARITH 2003), and RN(sqrt x) = s iff
-// -s u (1/2 when s is a power of two) < r <= s u with u = ulp(s): no
-// double lies strictly between s u and s u + u^2/4, which is where the
-// exact bound (s + u/2)^2 - s^2 falls, and likewise below.
-//
-// The bounds are products of a double and a power of two, formed on the
-// bit patterns (exponent field plus k); non-negative doubles compare like
-// their bit patterns as unsigned integers, so the tests run on the integer
-// pipes, not the FP64 pipe.
-__device__ __forceinline__ unsigned long long dbits(double x) {
-    return (unsigned long long)__double_as_longlong(x);
-}
-
-// The candidate quotient and whether the acceptance test vouches for it.
-__device__ __forceinline__ double div_rn_candidate(double a, double b, bool& ok) {
-    double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
-    const double e = fma(-b, y, 1.0);
-    y = fma(y, fma(e, e, e), y);
-    const double q0 = __dmul_rn(a, y);
-    const double q = fma(fma(-b, q0, a), y, q0);
-    const double r = fma(-b, q, a);
-    const unsigned long long qb = dbits(q), bb = dbits(b) & 0x7fffffffffffffffull;
-    const int eq = (int)(qb >> 52) & 0x7ff, eb = (int)(bb >> 52);
-    // exponent field of |b| ulp(q)/2 (power of two q: ulp(q)/4)
-    const int et = eb + eq - 1076 - ((qb & 0x000fffffffffffffull) == 0);
-    ok = eb >= 1 && eb <= 2046 && eq >= 1 && eq <= 2046 && et >= 1 && et <= 2046 &&
-         (dbits(r) & 0x7fffffffffffffffull) < bb + ((unsigned long long)(long long)(et - eb) << 52);
-    return q;
-}
-
-__device__ __forceinline__ double div_rn(double a, double b) {
-    bool ok;
-    const double q = div_rn_candidate(a, b, ok);
-    if (__builtin_expect(!ok, 0)) return a / b;
-    return q;
-}
-
-// The candidate root and whether the acceptance test vouches for it.
-__device__ __forceinline__ double sqrt_rn_candidate(double x, bool& ok) {
-    double y;
-    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    const double d = fma(-__dmul_rn(x, y), y, 1.0);
-    y = fma(y, __dmul_rn(d, fma(0.375, d, 0.5)), y);
-    const double s0 = __dmul_rn(x, y);
-    const double s = fma(fma(-s0, s0, x), __dmul_rn(0.5, y), s0);
-    const double r = fma(-s, s, x);
-    const unsigned long long sb = dbits(s), rb = dbits(r);
-    const int es = (int)(sb >> 52) & 0x7ff;  // s >= 0 or NaN here
-    const int et = 2 * es - 1075;             // exponent field of s ulp(s)
-    const bool pow2 = (sb & 0x000fffffffffffffull) == 0;
-    const unsigned long long up = sb + ((unsigned long long)(long long)(et - es) << 52);
-    const unsigned long long lo = up - ((unsigned long long)pow2 << 52);
-    const bool neg = (rb >> 63) != 0;
-    const unsigned long long ra = rb & 0x7fffffffffffffffull;
-    ok = es >= 1 && es <= 2046 && et >= 2 && et <= 2046 && (neg ? ra < lo : ra <= up);
-    return s;
-}
-
-__device__ __forceinline__ double sqrt_rn(double x) {
-    bool ok;
-    const double s = sqrt_rn_candidate(x, ok);
-    if (__builtin_expect(!ok, 0)) return sqrt(x);
-    return s;
-}
-#define GK_DIV(a, b) div_rn((a), (b))
-#define GK_RCP(b) div_rn(1.0, (b))
-#define GK_SQRT(x) sqrt_rn(x)
+// Parity mode: IEEE division and square root (correctly rounded on the GPU
+// as on the host).
+#define GK_DIV(a, b) ((a) / (b))
+#define GK_RCP(b) (1.0 / (b))
+#define GK_SQRT(x) sqrt(x)
 // the reference's compares and std::max/min
 #define GK_MAX0(x) smax((x), 0.0)
 #define GK_MIN0(x) smin(0.0, (x))
@@ -195,18 +112,6 @@ struct Flux5 {
     double d, n, t1, t2, e;  // density, normal momentum, tangential 1/2, energy
 };
 
-#if !GK_FASTMATH
-// |x| as the high word's magnitude bits: for finite and infinite x these
-// order like |x|, and NaN sorts above infinity.
-__device__ __forceinline__ unsigned hmag(double x) {
-    return (unsigned)__double2hiint(x) & 0x7fffffffu;
-}
-// x != +-0 (NaN counts as non-zero), on the integer pipe.
-__device__ __forceinline__ bool nonzero(double x) {
-    return (((unsigned)__double2hiint(x) & 0x7fffffffu) | (unsigned)__double2loint(x)) != 0u;
-}
-#endif
-
 // Flux::RiemannSolver for one face (hllc.cpp:22-101), HLLC after Toro
 // ch. 10 with the PVRS pressure estimate.  Velocities come as (normal,
 // tangential 1, tangential 2) in the reference's rotation
@@ -215,19 +120,10 @@ __device__ __forceinline__ bool nonzero(double x) {
 // runs with vz = 0): every term it contributes is then an exact zero.
 //
 // SEL picks how the two star sides are combined, f = selectl*fl + selectr*fr
-// with selectl = (ss >= 0) ? 1 : 0 (hllc.cpp:75-94):
-//   0  both sides, as the reference writes it;
-//   1  only the selected side (fast mode): differs only where the unused
-//      side is not finite, or in the sign of a zero;
-//   2  only the selected side when that provably gives the reference's bits,
-//      else both (parity mode).  1.0*fs + 0.0*fu equals fs whenever fs is
-//      non-zero and fu is finite (0.0*fu is then a signed zero, and adding
-//      a zero to a non-zero double is exact).  fu is certainly finite when
-//      every input of the unused side, ss and 1/(gamma-1) are below 2^51 in
-//      magnitude and |su - ss| >= 2^-50: its quotient stays below 2^154 and
-//      its largest product below 2^311.  Faces that fail either test
-//      (exactly zero flux components, as on a wall or across a state at
-//      rest, and extreme states) take the two-sided form.
+// with selectl = (ss >= 0) ? 1 : 0 (hllc.cpp:75-94): 0 both sides, as the
+// reference writes it (parity mode); 1 only the selected side (fast mode),
+// which differs only where the unused side is not finite, or in the sign of
+// a zero.
 template <bool T2, int SEL>
 __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double vzl, double prel,
                                      double denr, double vxr, double vyr, double vzr, double prer,
@@ -322,17 +218,4 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
     f.t1 = f1 * v1;
     f.t2 = T2 ? f1 * v2 : 0.0;
     f.e = (e + p) * (vn + c) + d * c * ss * (s - vn);
-#if !GK_FASTMATH
-    if (SEL == 2) {
-        const double du = left ? denr : denl, vnu = left ? vxr : vxl, v1u = left ? vyr : vyl;
-        const double v2u = left ? vzr : vzl, pu = left ? prer : prel, su = left ? sr : sl;
-        unsigned m = max(max(hmag(du), hmag(vnu)), max(hmag(v1u), hmag(pu)));
-        m = max(m, max(max(hmag(su), hmag(ss)), hmag(ph.gm1Rec)));
-        if (T2) m = max(m, hmag(v2u));
-        const bool exact = m < (1074u << 20) && hmag(su - ss) >= (973u << 20) && nonzero(f.d) &&
-                           nonzero(f.n) && nonzero(f.t1) && nonzero(f.e) &&
-                           (!T2 || nonzero(f.t2));
-        if (__builtin_expect(!exact, 0)) both_sides();
-    }
-#endif
 }

@@ -329,15 +329,6 @@ int gk_tap_substeps(gk_handle* h, int nsub, double dt_sub, int ratio, double* fx
  * device. */
 int gk_fastmath_check(int n, unsigned long long seed, double* worst3);
 
-/* Diagnostic of the PARITY mode arithmetic (no counterpart in the reference):
- * its inline correctly rounded quotient and square root against CUDA's IEEE
- * `/` and sqrt() over n random argument pairs (every exponent, zeros,
- * subnormals, infinities, NaNs and powers of two included, half of them
- * quotients near 1).  counts5 = {division results whose bits differ,
- * divisions sent to the IEEE operation, roots whose bits differ, roots sent
- * to the IEEE operation, pairs tried}; the differing counts must be 0.  Runs
- * on the current device. */
-int gk_paritymath_check(long long n, unsigned long long seed, unsigned long long* counts5);
 
 /* One RK2 time step of a 2D problem (vz = 0, gz = 0) on a caller-owned
  * device state, for callers that cannot allocate device memory while they

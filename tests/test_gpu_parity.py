@@ -214,26 +214,6 @@ def test_fastmath_refinements_within_error_bound():
     assert w[0] <= 2.0 and w[1] <= 2.0 and w[2] <= 2.0, list(w)
 
 
-def test_parity_quotient_and_root_equal_ieee():
-    """Parity mode's inline correctly rounded quotient and square root give
-    CUDA's IEEE `/` and sqrt() bits on 2^26 random argument pairs (every
-    exponent, zeros, subnormals, infinities, NaNs, powers of two, quotients
-    near 1); the acceptance test sends only the odd cases to the IEEE
-    operation."""
-    import ctypes
-    from gaukuk_b200 import _lib
-    L = _lib.load()
-    c = (ctypes.c_ulonglong * 5)()
-    _lib.check(L.gk_paritymath_check(1 << 26, 2024, c))
-    div_mis, div_fb, sqrt_mis, sqrt_fb, n = list(c)
-    print(f"\nparity math: {n} pairs, division fallbacks {div_fb / n:.4f}, "
-          f"root fallbacks {sqrt_fb / n:.4f}")
-    assert n == 1 << 26
-    assert div_mis == 0 and sqrt_mis == 0, list(c)
-    # zeros, subnormals, infinities and NaNs are 1/8 of each operand's draws
-    assert div_fb < 0.35 * n and sqrt_fb < 0.35 * n, list(c)
-
-
 def _extreme_state(n, with_vz, seed=0, nz=1):
     """A random 2D or 3D state at the edges of the scheme: densities
     log-uniform in [1e-12, 1e2] with 2 % negative (the floor resets them),

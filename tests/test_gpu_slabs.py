@@ -7,7 +7,10 @@ job (gk_slabs_create_nccl: the exchange is NCCL send/recv to itself around
 the periodic ring, the maximum an NCCL all-reduce).  Compared with the same
 problem run as one handle: the whole state (ghost rows included) and the dt
 sequence, in parity mode and in fast mode (the slabs run the same kernels
-as the undivided grid).
+as the undivided grid) -- bit for bit in parity mode; in fast mode within the
+fast-mode tolerance, since the compiler may contract a tile's first row
+(its prologue) differently from the rows after it, and the slabs' tiles
+start at other rows than the whole grid's.
 """
 import dataclasses
 
@@ -16,6 +19,7 @@ import pytest
 
 from gaukuk_b200 import problems
 from gaukuk_b200.config import BC_COPY, BC_OUTFLOW, BC_PERIODIC, BC_REFLECTIVE
+from helpers import active, rel_linf
 
 pytestmark = pytest.mark.gpu
 
@@ -57,8 +61,13 @@ def test_slabs_equal_the_whole_grid(case, nslab, mode):
         got = s.download()
         dts = s.dt_log()
     assert len(dts) == len(want_dts) > 0
-    assert dts == want_dts
-    assert np.array_equal(got, want)
+    if mode == "parity":
+        assert dts == want_dts
+        assert np.array_equal(got, want)
+    else:
+        np.testing.assert_allclose(dts, want_dts, rtol=1e-12)
+        errs = rel_linf(active(p, got), active(p, want))
+        assert max(errs[v] for v in (0, 1, 2, 4)) <= 1e-12, errs
 
 
 def test_slabs_refuse_what_the_fused_stage_does_not_run():
