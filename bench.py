@@ -205,14 +205,31 @@ def cpu_rate(exe, n, warm, steps, threads):
     return n * n * steps / t, t, d
 
 
-def reference_exe():
-    return os.path.join(ROOT, "oracle", "_ref", "ref_fast_kh_baseline")
+PORTABLE_FLAGS = ("reference Makefile flags (-O3 -ffast-math -funroll-loops, OpenMP) with "
+                  "-march=x86-64-v3 in place of -march=native")
+NATIVE_FLAGS = ("the reference Makefile's flags exactly (-O3 -march=native -ffast-math "
+                "-funroll-loops, OpenMP; native = sapphirerapids, the benchmark hosts' CPU)")
+
+
+def reference_exe(portable=False):
+    """The reference build for this host and its flags: the reference
+    Makefile's flags exactly (oracle/_ref/ref_native_kh_baseline, built for
+    the benchmark hosts' CPU) when it runs here, else the portable build."""
+    native = os.path.join(ROOT, "oracle", "_ref", "ref_native_kh_baseline")
+    port = os.path.join(ROOT, "oracle", "_ref", "ref_fast_kh_baseline")
+    if not portable and os.path.exists(native):
+        try:
+            run_reference_binary(native, 64, 2, 1, timeout=120)
+            return native, NATIVE_FLAGS
+        except Exception:
+            pass
+    return port, PORTABLE_FLAGS
 
 
 def main_reference(args, rank, world):
     if rank != 0:
         return 0
-    exe = reference_exe()
+    exe, flags = reference_exe()
     base = {"metric": METRIC, "unit": UNIT, "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
@@ -233,8 +250,7 @@ def main_reference(args, rank, world):
     rate, secs, _ = cpu_rate(exe, n, warm, args.steps, threads)
     cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
            "sample": f"KH {n}^2 RK2 PLM HLLC, steps {warm + 1}..{warm + args.steps} of one run, "
-                     f"reference Makefile flags (-O3 -ffast-math -funroll-loops, OpenMP) "
-                     f"with -march=x86-64-v3"}
+                     f"{flags}", "build": os.path.basename(exe)}
     out = dict(base)
     out.update({"value": rate, "ms_per_step": 1000.0 * secs / args.steps,
                 "config": config_dict(args.n, "reference-cpu",
@@ -403,16 +419,21 @@ def main_ours(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        exe = reference_exe()
+        exe, flags = reference_exe()
         if os.path.exists(exe):
             threads = host_threads()
             rate0, _, _ = cpu_rate(exe, 1024, 1, 3, threads)
-            # bounded sample: about 15 s of CPU work on the full grid
-            nsteps = int(max(3, min(40, 15.0 * rate0 / cells)))
+            # bounded sample: about 10 s of CPU work on the full grid
+            nsteps = int(max(3, min(40, 10.0 * rate0 / cells)))
             rate, secs, _ = cpu_rate(exe, n, 1, nsteps, threads)
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
-                   "sample": f"KH {n}^2, steps 2..{nsteps + 1} of one run ({secs:.1f} s), "
-                             f"reference Makefile flags with -march=x86-64-v3, OpenMP"}
+                   "sample": f"KH {n}^2, steps 2..{nsteps + 1} of one run ({secs:.1f} s), {flags}",
+                   "build": os.path.basename(exe)}
+            pexe, pflags = reference_exe(portable=True)
+            if pexe != exe and os.path.exists(pexe):
+                prate, psecs, _ = cpu_rate(pexe, n, 1, nsteps, threads)
+                cpu["portable_build"] = {"value": prate, "sample": f"same steps ({psecs:.1f} s), "
+                                                                    f"{pflags}"}
         else:
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                    "sample": "reference build absent"}
@@ -449,6 +470,47 @@ def main_ours(args, rank, world, local_rank):
         print(json.dumps(out))
     sim.close()
     reps.close()
+    return 0
+
+
+def main_ncu_case(args, local_rank):
+    """Short runs for profilers, nothing else:
+    * ensemble: 16 KH instances (sizes drawn from 128^2, 256^2, 512^2) in one
+      ensemble, `steps` steps (k_ens_stage, k_ens_bc);
+    * learned: `steps` Adam steps of batch 65536 on 2^20 synthetic faces
+      (k_mlp_grad, k_adam), then `steps` steps of KH 256^2 with the model
+      installed (the generic path with k_flux_correct)."""
+    import numpy as np
+    import torch
+
+    from gaukuk_b200 import problems
+    from gaukuk_b200.sim import Sim
+    torch.cuda.set_device(local_rank)
+    if args.workload == "ensemble":
+        from gaukuk_b200.ensemble import Ensemble
+        inst = problems.kh_ensemble(16, seed=0)
+        sims = [Sim(p, c, mode=args.mode, device=local_rank) for p, c, _ in inst]
+        ens = Ensemble(sims)
+        ens.run_steps(args.steps)
+        ens.close()
+        for s in sims:
+            s.close()
+    else:
+        from gaukuk_b200 import learned
+        rng = np.random.default_rng(0)
+        X = rng.normal(size=(1 << 20, learned.NI)).astype(np.float32)
+        Y = (0.1 * rng.normal(size=(1 << 20, 4))).astype(np.float32)
+        blob = learned.init_model(X, Y, seed=0)
+        tr = learned.Trainer(blob, X, Y, device=local_rank)
+        tr.train(args.steps, batch=65536, lr=1e-3)
+        blob = tr.model()
+        tr.close()
+        p, c = problems.kh(256)
+        with Sim(p, c, mode="fast", device=local_rank) as s:
+            learned.install(s, blob)
+            s.run_steps(args.steps)
+    torch.cuda.synchronize()
+    print(json.dumps({"ncu_case": True, "workload": args.workload, "steps": args.steps}))
     return 0
 
 
@@ -703,6 +765,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return main_reference(args, rank, world)
+    if args.ncu_case and args.workload in ("ensemble", "learned"):
+        return main_ncu_case(args, local_rank)
     if args.workload == "ensemble":
         return main_ensemble(args, rank, world, local_rank)
     if args.workload == "learned":

@@ -7,8 +7,8 @@ flux of the coarse state.  The coarse solver adds the prediction to its FP64
 HLLC flux at every stage (gk_set_flux_model), so the update stays conservative;
 a shock / positivity detector keeps plain HLLC where it fires.
 
-Everything that touches the grid runs in libgk_cuda.so: the fine runs, the
-flux taps (gk_tap_substeps), the coarse HLLC fluxes (gk_face_fluxes), training
+Everything that touches the grid runs in libgk_cuda.so: the fine runs (as
+ensembles, gk_ens_*), the flux taps (gk_tap_substeps), the coarse HLLC fluxes (gk_face_fluxes), training
 (gk_mlp_train: BF16 tensor-core forward, hand-written backward, Adam) and the
 corrected coarse runs.  NumPy only assembles stencils and statistics.
 
@@ -204,19 +204,23 @@ def perturb(p: Params, cons: np.ndarray, ratio: int, sigma: float, rng) -> np.nd
 def generate(seeds: Sequence[int], coarse: int = 256, ratio: int = 4, t_end: float = 2.0,
              snapshots: int = 16, frac: float = 0.25, mode: str = "fast",
              sample_seed: int = 0, tv_min: float = TV_GATE, noise: float = 0.0,
-             noisy: int = 1, first: float = 1.0, pairs: bool = False,
+             noisy: int = 1, first: float = 1.0, pairs: bool = False, batch: int = 16,
              log=print) -> Tuple[np.ndarray, np.ndarray]:
     """Training pairs from fine runs (coarse*ratio)^2 restricted to coarse^2.
 
-    At `snapshots` times t_end (s + first) / (snapshots + first), s = 0 ..
-    snapshots - 1, the fine state is restricted; one coarse RK2 step of the
-    restricted state is taken with the coarse solver, recording its
-    stage-averaged face fluxes (1/2)(F(U) + F(U*)), and the fine run is
-    advanced over the same interval in `ratio` fixed sub-steps while the
-    fluxes through the coarse faces are accumulated.  The target is their
-    difference: added to both coarse stages it makes the coarse step
-    reproduce the restricted fine step.  A fraction `frac` of the faces whose
-    stencil variation is at least `tv_min` (the faces the correction is
+    The fine runs are the plain method run as ensembles (``Ensemble``: one
+    persistent launch per RK stage over every instance of a batch of `batch`
+    seeds, whole steps in a CUDA graph).  At `snapshots` times
+    t_end (s + first) / (snapshots + first), s = 0 .. snapshots - 1, every
+    instance's fine state is copied into a scratch fine handle and restricted;
+    one coarse RK2 step of the restricted state is taken with the coarse
+    solver, recording its stage-averaged face fluxes (1/2)(F(U) + F(U*)), and
+    the scratch fine state is advanced over the same interval in `ratio`
+    fixed sub-steps while the fluxes through the coarse faces are accumulated.
+    The target is their difference: added to both coarse stages it makes the
+    coarse step reproduce the restricted fine step.  The ensemble's own
+    trajectories are not touched by the taps.  A fraction `frac` of the faces
+    whose stencil variation is at least `tv_min` (the faces the correction is
     applied to) is kept.
 
     With noise > 0 each snapshot also yields `noisy` sets of pairs from the
@@ -229,11 +233,12 @@ def generate(seeds: Sequence[int], coarse: int = 256, ratio: int = 4, t_end: flo
     next cell in the normal direction (rows 2m, 2m + 1), the layout of the
     pair loss (Trainer.set_pair_loss); a pair is kept when f's variation is
     at least `tv_min`."""
+    from .ensemble import Ensemble
     from .sim import Sim
     rng = np.random.default_rng(sample_seed)
     Xs, Ys = [], []
 
-    def pairs(pc, cc, fine, crs, dt_c):
+    def add_pairs(pc, cc, fine, crs, dt_c):
         fx_c, fy_c = tap(crs, 1, dt_c, 1)
         fx_f, fy_f = tap(fine, ratio, dt_c / ratio, ratio)
         a = active2d(pc, cc)
@@ -255,39 +260,39 @@ def generate(seeds: Sequence[int], coarse: int = 256, ratio: int = 4, t_end: flo
                 Xs.append(X[keep].astype(np.float32))
                 Ys.append(Y[keep].astype(np.float32))
 
-    for k, seed in enumerate(seeds):
+    seeds = list(seeds)
+    for b0 in range(0, len(seeds), batch):
         t0 = time.time()
-        pf, cf, _ = kh_instance(seed, coarse * ratio, t_end)
-        fine = Sim(pf, cf, mode=mode)
-        pc, cc = restrict(pf, cf, ratio)
+        group = seeds[b0:b0 + batch]
+        inst = [kh_instance(seed, coarse * ratio, t_end) for seed in group]
+        fines = [Sim(pf, cf, mode=mode) for pf, cf, _ in inst]
+        ens = Ensemble(fines)
+        pf, cf0 = inst[0][0], inst[0][1]  # every instance has the same grid and physics
+        scratch = Sim(pf, cf0, mode=mode)
+        pc, cc = restrict(pf, cf0, ratio)
         crs = Sim(pc, cc, mode=mode)
         drmin_c = min((pc.xmax - pc.xmin) / pc.nx, (pc.ymax - pc.ymin) / pc.ny)
+        t = 0.0
         for s in range(snapshots):
             ts = t_end * (s + first) / (snapshots + first)
-            t = fine.get_time()
             if ts > t + 1e-12:
-                fine.advance(ts - t)
-            f0 = fine.download()
-            if noise > 0:
-                t_f, step_f = fine.get_time(), fine.get_step()
-                for _ in range(noisy):
-                    fn = perturb(pf, f0, ratio, noise, rng)
-                    fine.upload(fn)
-                    fine.set_time(t_f, step_f)
-                    _, cc = restrict(pf, fn, ratio)
+                ens.advance(ts - t)  # every instance from t to ts
+                t = fines[0].get_time()
+            for fine in fines:
+                f0 = fine.download()
+                states = [perturb(pf, f0, ratio, noise, rng) for _ in range(noisy)] if noise > 0 else []
+                for st in states + [f0]:
+                    scratch.upload(st)
+                    scratch.set_time(t, 0)
+                    _, cc = restrict(pf, st, ratio)
                     crs.set_time(0.0, 0)
                     crs.upload(cc)
-                    pairs(pc, cc, fine, crs, pc.cfl * drmin_c / crs.cmax())
-                fine.upload(f0)
-                fine.set_time(t_f, step_f)
-            _, cc = restrict(pf, f0, ratio)
-            crs.set_time(0.0, 0)
-            crs.upload(cc)
-            pairs(pc, cc, fine, crs, pc.cfl * drmin_c / crs.cmax())
-        fine.close()
-        crs.close()
+                    add_pairs(pc, cc, scratch, crs, pc.cfl * drmin_c / crs.cmax())
+        ens.close()
+        for h in fines + [scratch, crs]:
+            h.close()
         if log:
-            log(f"instance {k + 1}/{len(seeds)} (seed {seed}): {time.time() - t0:.1f} s")
+            log(f"instances {b0 + 1}-{b0 + len(group)}/{len(seeds)}: {time.time() - t0:.1f} s")
     return np.concatenate(Xs), np.concatenate(Ys)
 
 
