@@ -50,9 +50,19 @@ def _run(cmd: List[str], verbose: bool) -> None:
         print(r.stderr, flush=True)
 
 
-def build_cuda(verbose: bool = False, force: bool = False) -> str:
-    """Compile the CUDA units and link libgk_cuda.so; returns its path."""
-    os.makedirs(OBJ, exist_ok=True)
+CHECKED_LIB = os.path.join(LIB, "checked", "libgk_cuda.so")
+
+
+def build_cuda(verbose: bool = False, force: bool = False, checked: bool = False) -> str:
+    """Compile the CUDA units and link libgk_cuda.so; returns its path.
+    checked=True builds the bounds-checked variant (GK_CHECKED: coordinates
+    checked and clamped, counters read by gk_checked_report) into
+    lib/checked/, for tests; the product path loads it only with
+    GK_CHECKED=1."""
+    obj_dir = os.path.join(OBJ, "checked") if checked else OBJ
+    lib_path = CHECKED_LIB if checked else CUDA_LIB
+    os.makedirs(obj_dir, exist_ok=True)
+    os.makedirs(os.path.dirname(lib_path), exist_ok=True)
     headers = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
         glob.glob(os.path.join(INCLUDE, "*.h"))
     units = {
@@ -63,20 +73,27 @@ def build_cuda(verbose: bool = False, force: bool = False) -> str:
     extra = sorted(os.path.basename(p) for p in glob.glob(os.path.join(CSRC, "*.cu")))
     for name in extra:
         units.setdefault(name, [])
-    objs = []
+    objs, cmds = [], []
+    extra_flags = ["-DGK_CHECKED=1"] if checked else []
     for name, flags in units.items():
         src = os.path.join(CSRC, name)
-        obj = os.path.join(OBJ, name.replace(".cu", ".o"))
+        obj = os.path.join(obj_dir, name.replace(".cu", ".o"))
         objs.append(obj)
         if force or _newer(obj, [src] + headers):
-            _run([NVCC] + NVCC_FLAGS + flags + ["-c", src, "-o", obj], verbose)
-    if force or _newer(CUDA_LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", CUDA_LIB] + objs, verbose)
-    return CUDA_LIB
+            cmds.append([NVCC] + NVCC_FLAGS + flags + extra_flags + ["-c", src, "-o", obj])
+    # the units compile independently: one nvcc per unit at a time
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, c, verbose) for c in cmds]:
+            f.result()
+    if force or _newer(lib_path, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", lib_path] + objs, verbose)
+    return lib_path
 
 
 def build_all(verbose: bool = False, force: bool = False) -> None:
     build_cuda(verbose=verbose, force=force)
+    build_cuda(verbose=verbose, force=force, checked=True)
     try:
         from . import _build_host
     except ImportError:

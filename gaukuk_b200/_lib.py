@@ -10,6 +10,8 @@ import os
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "lib", "libgk_cuda.so")
+# GK_CHECKED=1: the bounds-checked build of the same library (gk_checked_report)
+CHECKED_LIB_PATH = os.path.join(_PKG, "lib", "checked", "libgk_cuda.so")
 
 GK_OK = 0
 GK_MODE_PARITY = 0
@@ -61,6 +63,8 @@ SIGNATURES = {
     "gk_profile_steps": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _dp,
                                         _ip, ctypes.c_int, _ip]),
     "gk_fastmath_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_ulonglong, _dp]),
+    "gk_checked_report": (ctypes.c_int, [ctypes.POINTER(ctypes.c_ulonglong),
+                                         ctypes.POINTER(ctypes.c_ulonglong)]),
     "gk_rk2_step_noalloc": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(PhysDesc),
                                            _vp, ctypes.c_double, _dp, _vp]),
     "gk_set_tiling": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
@@ -115,11 +119,14 @@ SIGNATURES = {
 _lib = None
 
 
-def load(path: str = LIB_PATH):
-    """Load libgk_cuda.so and declare every entry point; raises if absent."""
+def load(path: str = None):
+    """Load libgk_cuda.so (the bounds-checked build when GK_CHECKED=1) and
+    declare every entry point; raises if absent."""
     global _lib
     if _lib is not None:
         return _lib
+    if path is None:
+        path = CHECKED_LIB_PATH if os.environ.get("GK_CHECKED") == "1" else LIB_PATH
     if not os.path.exists(path):
         raise RuntimeError(
             f"CUDA extension not built: {path} is missing (run __graft_entry__.build())")

@@ -1089,6 +1089,18 @@ int gk_profile_steps(gk_handle* h, int nsteps, char* names, int names_cap, doubl
     return pull_time(h);
 }
 
+int gk_checked_report(unsigned long long* count, unsigned long long* first) {
+    if (!count || !first) return GK_ERR_INVALID;
+    unsigned long long c[2] = {0, 0}, f[2] = {0, 0};
+    const int a = gk_parity::checked_report(&c[0], &f[0]);
+    const int b = gk_fast::checked_report(&c[1], &f[1]);
+    if (a > 0 || b > 0) return GK_ERR_UNSUPPORTED;
+    if (a < 0 || b < 0) return GK_ERR_CUDA;
+    *count = c[0] + c[1];
+    *first = c[0] ? f[0] : f[1];
+    return GK_OK;
+}
+
 int gk_fastmath_check(int n, unsigned long long seed, double* worst3) {
     if (n <= 0 || !worst3) return GK_ERR_INVALID;
     return gk_fast::fastmath_check(n, seed, worst3) == 0 ? GK_OK : GK_ERR_CUDA;

@@ -220,6 +220,7 @@ static const char* const kClassNames[K_NCLASS] = {
                         int kind, double c1, double c2, double c3, cudaStream_t s);            \
     void launch_begin(const gk::Ctx& c, double dtoutput, int steps, cudaStream_t s);           \
     void launch_epilogue(const gk::Ctx& c, cudaStream_t s);                                    \
+    int checked_report(unsigned long long* count, unsigned long long* first);                  \
     void launch_mtz_check(const gk::Ctx& c, const double* u, int* flag, cudaStream_t s);       \
     void launch_ens_stage(int threads, int kind, int plm, const gk::EnsInst* inst,             \
                           const int2* tiles, int ntiles, unsigned* counter, double c1,          \

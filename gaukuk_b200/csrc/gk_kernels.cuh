@@ -42,10 +42,58 @@ using gk::Phys;
 
 constexpr int kSel = GK_SEL;
 
+#ifndef GK_CHECKED
+#define GK_CHECKED 0
+#endif
+#if GK_CHECKED
+// Bounds-checked build (-DGK_CHECKED=1: lib/checked/libgk_cuda.so).  Every
+// cell coordinate that indexes a state or face array (sidx, fidx), every row
+// the stage kernels store and every TMA row coordinate is checked against
+// its array.  A coordinate outside is counted, the first one recorded (site,
+// coordinate, bound: gk_checked_report) and clamped into the array, so the
+// access stays inside the buffer; a TMA row that fails is not issued and its
+// barrier is released empty.  Sites: 1-3 state k, j, i; 4-6 face k, j, i;
+// 7 stage store row; 8 TMA row.
+__device__ unsigned long long gk_chk_count;
+__device__ unsigned long long gk_chk_first;
+__device__ __noinline__ int chk_fail(int x, int lo, int hi, int site) {
+    if (atomicAdd(&gk_chk_count, 1ull) == 0ull)
+        gk_chk_first = ((unsigned long long)(site & 0xffff) << 48) |
+                       ((unsigned long long)((unsigned)x & 0xffffffu) << 24) |
+                       (unsigned long long)((unsigned)hi & 0xffffffu);
+    return x < lo ? lo : (hi > lo ? hi - 1 : lo);
+}
+__device__ __forceinline__ int chk(int x, int lo, int hi, int site) {
+    return (x < lo || x >= hi) ? chk_fail(x, lo, hi, site) : x;
+}
+#define GK_CHK(x, lo, hi, site) chk((x), (lo), (hi), (site))
+#else
+#define GK_CHK(x, lo, hi, site) (x)
+#endif
+
+// The counters of the checked build (1 when this build has none).
+int checked_report(unsigned long long* count, unsigned long long* first) {
+#if GK_CHECKED
+    if (cudaMemcpyFromSymbol(count, gk_chk_count, sizeof(*count)) != cudaSuccess) return -1;
+    if (cudaMemcpyFromSymbol(first, gk_chk_first, sizeof(*first)) != cudaSuccess) return -1;
+    return 0;
+#else
+    (void)count;
+    (void)first;
+    return 1;
+#endif
+}
+
 __device__ __forceinline__ long long sidx(const Geom& g, int k, int j, int i) {
+    k = GK_CHK(k, g.kofs, g.kofs + g.nzs, 1);
+    j = GK_CHK(j, 0, g.leny, 2);
+    i = GK_CHK(i, 0, g.pitch, 3);
     return (long long)(k - g.kofs) * g.kstride + (long long)j * g.pitch + i;
 }
 __device__ __forceinline__ long long fidx(const Geom& g, int k, int j, int i) {
+    k = GK_CHK(k, g.kofs, g.kofs + g.nzs + 1, 4);
+    j = GK_CHK(j, 0, g.leny + 1, 5);
+    i = GK_CHK(i, 0, g.fpitch, 6);
     return (long long)(k - g.kofs) * g.fkstride + (long long)j * g.fpitch + i;
 }
 
@@ -829,7 +877,7 @@ __global__ void __launch_bounds__(kStageThreads, 3)
                 const unsigned long long b = (unsigned long long)__double_as_longlong(local);
                 cbest = b > cbest ? b : cbest;
             }
-            const long long oc = cbase + (f - 1) * P;
+            const long long oc = cbase + (long long)GK_CHK(f - 1, g.jb, g.je, 7) * P;
             out[oc] = r[0];
             out[vs + oc] = r[1];
             out[2 * vs + oc] = r[2];
@@ -911,6 +959,11 @@ __device__ __forceinline__ void tma_row(double* dst, const CUtensorMap* map, int
         "l"((unsigned long long)map), "r"(x), "r"(y), "r"(0), "r"(smem_u32(bar))
         : "memory");
 }
+// A plain arrival (no transaction bytes): completes the phase of a
+// one-arrival barrier without a copy (the checked build's refused rows).
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned phase, int* status) {
     for (int it = 0; it < (1 << 22); ++it) {
         unsigned ok;
@@ -989,10 +1042,24 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
     auto rs0 = [&](int r) { return seq0 + (unsigned)(r - y0); };
     auto issue = [&](int r) {
         const unsigned q = rs(r) % kRing;
+#if GK_CHECKED
+        if ((x0 & 1) || x0 < 0 || x0 >= g.pitch || r < 0 || r >= g.leny) {
+            chk_fail(r, 0, g.leny, 8);
+            mbar_arrive(&sm.bar[q]);
+            return;
+        }
+#endif
         tma_row(ring + q * RD, mapc, x0, r, RB, &sm.bar[q]);
     };
     auto issue0 = [&](int r) {
         const unsigned q = rs0(r) % kRing0;
+#if GK_CHECKED
+        if ((x0 & 1) || x0 < 0 || x0 >= g.pitch || r < 0 || r >= g.leny) {
+            chk_fail(r, 0, g.leny, 8);
+            mbar_arrive(&sm.bar0[q]);
+            return;
+        }
+#endif
         tma_row(ring0 + q * RD, map0, x0, r, RB, &sm.bar0[q]);
     };
     auto wait = [&](int r) { mbar_wait(&sm.bar[rs(r) % kRing], (rs(r) / kRing) & 1u, status); };
@@ -1125,7 +1192,7 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
                 const unsigned long long b = (unsigned long long)__double_as_longlong(local);
                 cbest = b > cbest ? b : cbest;
             }
-            const long long oc = cbase + (f - 1) * P;
+            const long long oc = cbase + (long long)GK_CHK(f - 1, g.jb, g.je, 7) * P;
             out[oc] = r[0];
             out[vs + oc] = r[1];
             out[2 * vs + oc] = r[2];

@@ -330,6 +330,16 @@ int gk_tap_substeps(gk_handle* h, int nsub, double dt_sub, int ratio, double* fx
 int gk_fastmath_check(int n, unsigned long long seed, double* worst3);
 
 
+/* The bounds-checked build (lib/checked/libgk_cuda.so, compiled with
+ * GK_CHECKED; no counterpart in the reference, whose only sanitizer is a
+ * commented-out AddressSanitizer line, Makefile:43-44): the number of cell,
+ * face, stage-row and TMA-row coordinates found outside their arrays since
+ * the library loaded (each was clamped into its array or not issued, so no
+ * access left a buffer), and the first one: site << 48 | coordinate << 24 |
+ * bound (sites: 1-3 state k, j, i; 4-6 face k, j, i; 7 stage store row;
+ * 8 TMA row).  GK_ERR_UNSUPPORTED in the normal build. */
+int gk_checked_report(unsigned long long* count, unsigned long long* first);
+
 /* One RK2 time step of a 2D problem (vz = 0, gz = 0) on a caller-owned
  * device state, for callers that cannot allocate device memory while they
  * run: their memory comes from their own pool or arena, or their budget is
