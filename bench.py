@@ -59,9 +59,9 @@ BYTES_PER_ZU_RK2 = 160  # 5 * V * 8 B with V = 4 (2D): algorithmic HBM bytes per
 STAGE_BYTES_PER_CELL = 80  # per stage launch, averaged over the two RK2 stages
 # FP64 add/mul/fma thread-instructions per zone-update of the fast-mode fused
 # RK2 step (stage 1 + last stage), from the ncu capture in
-# profiles/stage2d_tma_kh2048_ncu_full.md; the FP64 pipe issues 64 lanes per
+# profiles/stage2d_tma_kh2048_ncu.md; the FP64 pipe issues 64 lanes per
 # SM per clock on B200 (148 SMs)
-FP64_OPS_PER_ZU_FAST = 308 + 336
+FP64_OPS_PER_ZU_FAST = 308 + 335
 FP64_LANES = 64 * 148
 
 
@@ -374,7 +374,7 @@ def main_ours(args, rank, world, local_rank):
                   "unit": "T FP64 thread-instructions/s", "frac": ach / pk,
                   "ops_per_zone_update": FP64_OPS_PER_ZU_FAST,
                   "peak_source": "64 FP64 lanes x 148 SMs x " + src,
-                  "ops_source": "ncu, profiles/stage2d_tma_kh2048_ncu_full.md"}
+                  "ops_source": "ncu, profiles/stage2d_tma_kh2048_ncu.md"}
 
     # end to end through the C ABI with pinned host buffers
     e2e_steps = max(1, args.e2e_steps)
