@@ -473,6 +473,61 @@ def main_ours(args, rank, world, local_rank):
     return 0
 
 
+def main_slabs(args, rank, world, local_rank):
+    """One KH grid of n x (n * N) cells split into N y-slabs, one per GPU
+    (weak scaling: n^2 cells per GPU), exchanging ghost rows through NCCL
+    every RK stage and the CFL maximum every step (gaukuk_b200.slabs).
+    value = zone-updates/s of the whole grid over K steps, timed with CUDA
+    events on the library's stream between a barrier + synchronize, max over
+    ranks."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from gaukuk_b200 import problems
+    from gaukuk_b200.slabs import DistSlabs
+
+    torch.cuda.set_device(local_rank)
+    if not dist.is_initialized():
+        if world == 1:
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29531")
+        dist.init_process_group("gloo", rank=rank, world_size=world,
+                                timeout=datetime.timedelta(seconds=120))
+    n = args.n
+    p, c = problems.kh(n, ny=n * world, seed=0)
+    s = DistSlabs(p, c, dist, mode=args.mode, device=local_rank)
+    s.run_steps(args.warmup)
+    torch.cuda.synchronize()
+    blocks = []
+    for _ in range(max(1, args.repeats)):
+        dist.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        s.run_steps(args.steps)
+        ev1.record()
+        ev1.synchronize()
+        ms = torch.tensor([ev0.elapsed_time(ev1)])
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        blocks.append(float(ms[0]))
+    med = statistics.median(blocks)
+    if rank == 0:
+        print(json.dumps({"metric": METRIC + " (one grid in y-slabs)", "unit": UNIT,
+                          "value": p.nx * p.ny * args.steps / (med / 1000.0), "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": med / args.steps,
+                          "higher_is_better": True, "scaling": "weak", "dtype": "f64",
+                          "config": {"workload": f"KH {p.nx}x{p.ny} in {world} y-slabs",
+                                     "arith_mode": args.mode},
+                          "timed_blocks": blocks,
+                          "timing": "CUDA events around run_steps (the host waits for each "
+                                    "step's NCCL calls to be enqueued), max over ranks"}))
+    s.close()
+    dist.destroy_process_group()
+    return 0
+
+
 def main_ncu_case(args, local_rank):
     """Short runs for profilers, nothing else:
     * ensemble: 16 KH instances (sizes drawn from 128^2, 256^2, 512^2) in one
@@ -734,7 +789,8 @@ def main():
     ap.add_argument("--e2e-calls", type=int, default=2)
     ap.add_argument("--e2e-dtoutput", type=float, default=0.1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="kh4096", choices=["kh4096", "ensemble", "learned", "configs"])
+    ap.add_argument("--workload", default="kh4096",
+                    choices=["kh4096", "ensemble", "learned", "configs", "slabs"])
     ap.add_argument("--train-seeds", type=int, default=16)
     ap.add_argument("--eval-seeds", type=int, default=8)
     ap.add_argument("--coarse", type=int, default=256)
@@ -771,6 +827,8 @@ def main():
         return main_ensemble(args, rank, world, local_rank)
     if args.workload == "learned":
         return main_learned(args, rank, world, local_rank)
+    if args.workload == "slabs":
+        return main_slabs(args, rank, world, local_rank)
     if args.workload == "configs":
         return main_configs(args, rank, world, local_rank)
     return main_ours(args, rank, world, local_rank)
