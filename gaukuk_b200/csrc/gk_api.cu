@@ -412,7 +412,9 @@ int run_host_fills(gk_handle* h, double* u) {
     for (const auto& f : h->host_fills)
         if ((rc = copy(f, true)) != GK_OK) return rc;
     GK_CUDA(h, cudaStreamSynchronize(s));
-    for (const auto& f : h->host_fills) f.fn(f.user, f.cons);
+    for (const auto& f : h->host_fills)
+        if (f.fn(f.user, f.cons) != 0)
+            return fail(h, GK_ERR_INVALID, "a host boundary routine reported a failure");
     for (const auto& f : h->host_fills)
         if ((rc = copy(f, false)) != GK_OK) return rc;
     // the host arrays are read again by the next fill: let the copies finish

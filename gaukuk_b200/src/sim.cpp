@@ -122,9 +122,16 @@ void Sim::EnsureDevice() {
 // A self-defined side run by the library at a ghost fill: the library has
 // copied the cells the routine reads into cons and copies its ghost strip
 // back afterwards.
-void Sim::HostFill(void* user, double* /*cons*/) {
+// An exception does not cross the C ABI: it is kept and rethrown by Advance.
+int Sim::HostFill(void* user, double* /*cons*/) {
     HostSide* h = static_cast<HostSide*>(user);
-    h->sim->boundary.RunSide(h->side, h->sim->cons, h->sim->grid, h->sim->eos);
+    try {
+        h->sim->boundary.RunSide(h->side, h->sim->cons, h->sim->grid, h->sim->eos);
+    } catch (const std::exception& e) {
+        h->sim->hostFillError_ = e.what();
+        return 1;
+    }
+    return 0;
 }
 
 // The reference's integrators end with cons.Swap(consTemp) (rk2.cpp:21,
@@ -188,6 +195,11 @@ void Sim::Advance(Real dtoutput) {
         tp += dts[k];
         std::cout << "step = " << step0 + k + 1 << ", t = " << tp << ", dt = " << dts[k]
                   << std::endl;
+    }
+    if (!hostFillError_.empty()) {
+        const std::string e = hostFillError_;
+        hostFillError_.clear();
+        throw std::runtime_error("self-defined boundary: " + e);
     }
     Check(dev_, rc, "gk_advance");
     // The planes the device does not hold (1D/2D: the unused z-planes) and an

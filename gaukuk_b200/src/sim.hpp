@@ -24,6 +24,7 @@
 #include "template_array.hpp"
 
 #include <cstddef>
+#include <string>
 #include <vector>
 
 struct gk_handle;
@@ -95,7 +96,8 @@ private:
         int side;
     };
     HostSide hostSides_[6];
-    static void HostFill(void* user, double* cons);
+    std::string hostFillError_;  // what a host-run side threw, rethrown by Advance
+    static int HostFill(void* user, double* cons);
 };
 
 }  // namespace Gaukuk

@@ -102,11 +102,12 @@ int gk_set_fixed_boundary(gk_handle* h, const double* snapshot, int fix_inner);
  * ghost strip and the `depth` cell layers next to it (depth >= n + nghost:
  * the whole extent), across the whole transverse extent and every variable;
  * fn(user, cons) then fills the strip (ghost layers, active transverse
- * cells), which is copied back.  The device fills the other sides first.  A
- * handle with host sides runs its steps without a CUDA graph, returning to
- * the host at every ghost fill.  fn = NULL removes the side's routine.  Not
- * for ensembles. */
-typedef void (*gk_host_fill_fn)(void* user, double* cons);
+ * cells), which is copied back.  fn returns 0, or non-zero to stop the run
+ * (the advance then returns GK_ERR_INVALID).  The device fills the other
+ * sides first.  A handle with host sides runs its steps without a CUDA
+ * graph, returning to the host at every ghost fill.  fn = NULL removes the
+ * side's routine.  Not for ensembles. */
+typedef int (*gk_host_fill_fn)(void* user, double* cons);
 int gk_set_host_fill(gk_handle* h, int side, int depth, gk_host_fill_fn fn, void* user,
                      double* cons);
 
@@ -399,7 +400,12 @@ int gk_slabs_create(const gk_grid_desc* grid, const gk_phys_desc* phys, int nsla
  * rows are sent and received once per stage, the CFL speed is all-reduced
  * (max) once per step.  id128: a 128-byte NCCL unique id made by one process
  * with gk_slabs_nccl_id and passed to all.  Every process must make the same
- * calls in the same order (they take part in the same collectives). */
+ * calls in the same order (they take part in the same collectives).  The
+ * library's NCCL calls have no timeout: a process that fails or leaves
+ * between steps leaves the others waiting in their next exchange, and the
+ * job's launcher must end them, as for any NCCL job.  A failure that every
+ * process sees (a non-finite state, a timed-out row load) stops all of them
+ * together: the status word is part of the per-step all-reduce. */
 int gk_slabs_nccl_id(void* id128);
 int gk_slabs_create_nccl(const gk_grid_desc* grid, const gk_phys_desc* phys, int nranks, int rank,
                          const void* id128, gk_slabs** out);
