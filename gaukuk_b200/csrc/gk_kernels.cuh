@@ -248,7 +248,7 @@ __global__ void k_immersed(double* __restrict__ u, Geom g, Phys ph, const DevTim
 // EquationOfState::ConsToPrim (adiabatic.cpp:18-61) over every stored cell.
 __device__ __forceinline__ void cons_to_prim5(double d, double mx, double my, double mz, double e,
                                               const Phys& ph, double w[5]) {
-    d = smax(d, ph.dmin);
+    d = GK_FLOOR(d, ph.dmin);
     w[gk::P_RHO] = d;
     double denInv = GK_RCP(d);
     w[gk::P_VX] = mx * denInv;
@@ -256,7 +256,7 @@ __device__ __forceinline__ void cons_to_prim5(double d, double mx, double my, do
     w[gk::P_VZ] = mz * denInv;
     double engKin = 0.5 * denInv * (mx * mx + my * my + mz * mz);
     double pre = ph.gm1 * (e - engKin);
-    w[gk::P_PRE] = (pre > ph.pmin) ? pre : ph.pmin;
+    w[gk::P_PRE] = GK_BELOW(ph.pmin, pre) ? pre : ph.pmin;
 }
 
 __global__ void k_c2p(const double* __restrict__ u, double* __restrict__ w, Geom g, Phys ph,
@@ -339,7 +339,7 @@ __global__ void k_flux(const double* __restrict__ w, double* __restrict__ F, Geo
 // Sim::UpdateCons, both overloads (update_cons.cpp:11-133, 135-269).
 // update_cons.cpp:55-68, five slots (DEN, MTX, MTY, ENG, MTZ).
 __device__ __forceinline__ void floors5(double (&r)[5], const Phys& ph, DevTime* tm) {
-    if (r[gk::S_DEN] < ph.dmin) {
+    if (GK_BELOW(r[gk::S_DEN], ph.dmin)) {
         r[gk::S_DEN] = ph.dmin;
         r[gk::S_MTX] = 0.0;
         r[gk::S_MTY] = 0.0;
@@ -352,7 +352,7 @@ __device__ __forceinline__ void floors5(double (&r)[5], const Phys& ph, DevTime*
                     (r[gk::S_MTX] * r[gk::S_MTX] + r[gk::S_MTY] * r[gk::S_MTY] +
                      r[gk::S_MTZ] * r[gk::S_MTZ]);
         double press = ph.gm1 * (r[gk::S_ENG] - ke);
-        if (press < ph.pmin) {
+        if (GK_BELOW(press, ph.pmin)) {
             r[gk::S_ENG] = ph.pmin / ph.gm1 + ke;
             atomicAdd(&tm->floor_pre, 1ull);
         }
@@ -507,16 +507,16 @@ __global__ void k_kick(double* __restrict__ u, Geom g, Phys ph, const DevTime* _
 // loop body (sim.cpp:93-98) and the next step's dt (sim.cpp:77-81).
 __device__ __forceinline__ double cell_cmax(double d, double mx, double my, double mz, double e,
                                             const Phys& ph, bool has_z) {
-    d = smax(d, ph.dmin);
+    d = GK_FLOOR(d, ph.dmin);
     double denInv = GK_RCP(d);
     double vx = mx * denInv, vy = my * denInv, vz = mz * denInv;
     double engKin = has_z ? 0.5 * (vx * mx + vy * my + vz * mz) : 0.5 * (vx * mx + vy * my);
     double pres = ph.gm1 * (e - engKin);
-    pres = (pres > ph.pmin) ? pres : ph.pmin;
+    pres = GK_BELOW(ph.pmin, pres) ? pres : ph.pmin;
     double cs = GK_SQRT(ph.gamma * pres * denInv);
     double local = fabs(vx) + cs;
-    local = smax(local, fabs(vy) + cs);
-    if (has_z) local = smax(local, fabs(vz) + cs);
+    local = GK_MAXNN(local, fabs(vy) + cs);
+    if (has_z) local = GK_MAXNN(local, fabs(vz) + cs);
     return local;
 }
 
@@ -531,13 +531,7 @@ __device__ __forceinline__ double cell_cmax_inv(double mx, double my, double e, 
     pres = GK_BELOW(ph.pmin, pres) ? pres : ph.pmin;
     double cs = GK_SQRT(ph.gamma * pres * denInv);
     double local = fabs(vx) + cs;
-#if GK_FASTMATH
-    // both non-negative: their bit patterns order like the values
-    const double other = fabs(vy) + cs;
-    local = __double_as_longlong(local) < __double_as_longlong(other) ? other : local;
-#else
-    local = smax(local, fabs(vy) + cs);
-#endif
+    local = GK_MAXNN(local, fabs(vy) + cs);
     return local;
 }
 

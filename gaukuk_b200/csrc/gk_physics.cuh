@@ -72,6 +72,8 @@ __device__ __forceinline__ double floor_at(double x, double f) {
 #define GK_LE0(x) le0(x)
 #define GK_FLOOR(x, f) floor_at((x), (f))
 #define GK_BELOW(x, f) (__double_as_longlong(x) < __double_as_longlong(f))
+// max of two non-negative values (speeds): their bit patterns order alike
+#define GK_MAXNN(a, b) (__double_as_longlong(a) < __double_as_longlong(b) ? (b) : (a))
 #else
 // Parity mode: IEEE division and square root (correctly rounded on the GPU
 // as on the host).
@@ -85,6 +87,7 @@ __device__ __forceinline__ double floor_at(double x, double f) {
 #define GK_LE0(x) ((x) <= 0.0)
 #define GK_FLOOR(x, f) smax((x), (f))
 #define GK_BELOW(x, f) ((x) < (f))
+#define GK_MAXNN(a, b) smax((a), (b))
 #endif
 
 // Reconstruction::VanLeer (reconstruction.hpp:36-42).
