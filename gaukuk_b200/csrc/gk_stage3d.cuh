@@ -214,6 +214,20 @@ __global__ void __launch_bounds__(NT, 384 / NT)
     for (int f = y0 + 1; f <= y1; ++f) {
         const Q5 Q1 = Qn;
         if (f + 2 <= y1 + 1) Qn = load5(uc, g, at(f + 2));
+        // the z fluxes below and above cell row f-1, and its base state, are
+        // loaded here so that they arrive while the row's Riemann problems
+        // are solved
+        double zlo[5], zhi[5], b0[5];
+        if (do_cell) {
+            const long long fc = fidx(g, k, f - 1, xi);
+            const long long c = at(f - 1);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                zlo[v] = __ldg(F3 + v * g.fvstride + fc);
+                zhi[v] = __ldg(F3 + v * g.fvstride + fc + g.fkstride);
+                b0[v] = THREE ? u0[v * g.vstride + c] : uc[v * g.vstride + c];
+            }
+        }
         const W5 P1 = c2p_q(Q1, ph);
 #pragma unroll
         for (int v = 0; v < 5; ++v) sP[v][t] = Pm1.v[v];
@@ -246,15 +260,13 @@ __global__ void __launch_bounds__(NT, 384 / NT)
         if (do_cell) {
             // update_cons.cpp (3D): (Fx(i+1)-Fx(i))*dtdx + (Fy(j+1)-Fy(j))*dtdy + (Fz(k+1)-Fz(k))*dtdz
             const long long c = at(f - 1);
-            const long long fc = fidx(g, k, f - 1, xi);
             double r[5];
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
                 double dF = (sF[v][tr] - fx[v]) * dtdx;
-                dF = dF + (fy[v] - fyPrev[v]) * dtdy +
-                     (F3[v * g.fvstride + fc + g.fkstride] - F3[v * g.fvstride + fc]) * dtdz;
-                if (THREE) r[v] = c1 * u0[v * g.vstride + c] + c2 * uc[v * g.vstride + c] - c3 * dF;
-                else r[v] = c1 * uc[v * g.vstride + c] - c2 * dF;
+                dF = dF + (fy[v] - fyPrev[v]) * dtdy + (zhi[v] - zlo[v]) * dtdz;
+                if (THREE) r[v] = c1 * b0[v] + c2 * uc[v * g.vstride + c] - c3 * dF;
+                else r[v] = c1 * b0[v] - c2 * dF;
             }
             floors5(r, ph, tm);
             if (LAST) {
