@@ -1369,7 +1369,7 @@ static inline int stage3d_nt(const Geom& g) {
 void launch_zflux(const Ctx& c, const double* u, double* F3, cudaStream_t s) {
     const Geom& g = c.g;
     constexpr int zseg = 32;  // faces per thread; nz + 1 faces in all
-    dim3 grid((g.nx + 127) / 128, g.ny, (g.nz + 1 + zseg - 1) / zseg);
+    dim3 grid((g.nx + kZX - 1) / kZX, (g.ny + kZY - 1) / kZY, (g.nz + 1 + zseg - 1) / zseg);
     if (c.ph.plm) k_zflux<true><<<grid, 128, 0, s>>>(u, F3, g, c.ph, c.tm, zseg);
     else k_zflux<false><<<grid, 128, 0, s>>>(u, F3, g, c.ph, c.tm, zseg);
 }

@@ -92,69 +92,102 @@ __device__ __forceinline__ void hllc5_y(const double (&l)[5], const double (&r)[
 }
 
 // ------------------------------------------------------------ z faces
-// A thread owns column (i, j) and marches up a segment of zseg faces.  The
-// y-slope of cell (k, j) gives both its lower state (the right state of face
-// k-1|k) and its upper state (the left state of face k|k+1), so each plane's
-// three rows are converted and sloped once for two faces; the rows of the
-// next plane are in flight while a face is solved.  The expressions are
-// plm_up / plm_down's, so the fluxes are the same bits.
+// A CTA of 128 threads owns a tile of 32 columns x 4 rows of z faces and
+// marches up a segment of zseg faces; a thread owns column (i, j) of the
+// tile.  Per plane the CTA converts the tile's 6 rows (the 4 rows and one
+// halo row below and above) once, 1.5 cells per face instead of the 3 a
+// thread converting its own rows j-1, j, j+1 would, into a double-buffered
+// shared array; the raw values of the next plane are in flight while a face
+// is solved.  The y-slope of cell (k, j) gives both its lower state (the
+// right state of face k-1|k) and its upper state (the left state of face
+// k|k+1).  The expressions are plm_up / plm_down's, so the fluxes are the
+// same bits.
+constexpr int kZX = 32, kZY = 4, kZRows = kZY + 2, kZCells = kZX * kZRows;
+
 template <bool PLM>
 __global__ void __launch_bounds__(128)
     k_zflux(const double* __restrict__ u, double* __restrict__ F3, Geom g, Phys ph,
             const DevTime* __restrict__ tm, int zseg) {
     if (!tm->active) return;
-    const int i = g.ib + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.ie) return;
-    const int j = g.jb + blockIdx.y;
+    __shared__ double sW[2][kZRows][5][kZX];
+    const int t = threadIdx.x, tx = t & (kZX - 1), ty = t / kZX;
+    const int i = g.ib + blockIdx.x * kZX + tx;
+    const int j = g.jb + blockIdx.y * kZY + ty;
+    const bool mine = i < g.ie && j < g.je;
     const int k0 = g.kb + blockIdx.z * zseg;    // first face (k0-1 | k0)
     const int k1 = min(k0 + zseg, g.ke + 1);    // one past the last face
-    // rows j-1, j, j+1 of plane k (ghost rows and planes included)
-    auto plane = [&](int k, Q5 (&q)[3]) {
-        const long long c = sidx(g, k, j, i);
-#pragma unroll
-        for (int r = 0; r < 3; ++r) q[r] = load5(u, g, c + (long long)(r - 1) * g.pitch);
+    // the cells this thread loads: m = t and m = t + 128 (< 192) of the tile's
+    // 6 x 32 cells, rows j0-1 .. j0+4 (clamped into the array: rows and
+    // columns past the grid feed no face of this tile)
+    const int j0 = g.jb + blockIdx.y * kZY;
+    auto cell_of = [&](int m) {
+        const int row = min(j0 - 1 + m / kZX, g.leny - 1);
+        const int col = min(g.ib + blockIdx.x * kZX + (m % kZX), g.lenx - 1);
+        return sidx(g, g.kb, row, col) - sidx(g, g.kb, 0, 0);  // offset within a plane
     };
-    // states of cell (k, j) from its plane's rows j-1, j, j+1
-    auto states = [&](const Q5 (&q)[3], double (&lo)[5], double (&up)[5]) {
-        const W5 b = c2p_q(q[1], ph);
-        if (PLM) {
-            const W5 a = c2p_q(q[0], ph), c = c2p_q(q[2], ph);
+    const long long off0 = cell_of(t);
+    const bool two = t + 128 < kZCells;
+    const long long off1 = two ? cell_of(t + 128) : off0;
+    auto load = [&](int k, Q5& a, Q5& b) {
+        const long long base = sidx(g, k, 0, 0);
+        a = load5(u, g, base + off0);
+        if (two) b = load5(u, g, base + off1);
+    };
+    auto put = [&](int buf, int m, const Q5& q) {
+        const W5 w = c2p_q(q, ph);
 #pragma unroll
-            for (int v = 0; v < 5; ++v) {
+        for (int v = 0; v < 5; ++v) sW[buf][m / kZX][v][m % kZX] = w.v[v];
+    };
+    // states of cell (k, j) from the tile's rows ty, ty+1, ty+2 (= j-1, j, j+1)
+    auto states = [&](int buf, double (&lo)[5], double (&up)[5]) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const double b = sW[buf][ty + 1][v][tx];
+            if (PLM) {
+                const double a = sW[buf][ty][v][tx], c = sW[buf][ty + 2][v][tx];
 #if GK_FASTMATH
-                const double h = vanleer_half(b.v[v] - a.v[v], c.v[v] - b.v[v]);
+                const double h = vanleer_half(b - a, c - b);
 #else
-                const double h = 0.5 * vanleer(b.v[v] - a.v[v], c.v[v] - b.v[v]);
+                const double h = 0.5 * vanleer(b - a, c - b);
 #endif
-                lo[v] = b.v[v] - h;
-                up[v] = b.v[v] + h;
+                lo[v] = b - h;
+                up[v] = b + h;
+            } else {
+                lo[v] = up[v] = b;
             }
-        } else {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) lo[v] = up[v] = b.v[v];
         }
     };
-    Q5 q[3];
+    Q5 qa, qb;
     double wl[5], wr[5], nu[5];
-    plane(k0 - 1, q);
-    states(q, wr, wl);  // the upper state of plane k0-1 is the first face's left state
-    plane(k0, q);
+    load(k0 - 1, qa, qb);
+    put(0, t, qa);
+    if (two) put(0, t + 128, qb);
+    load(k0, qa, qb);
+    __syncthreads();
+    states(0, wr, wl);  // the upper state of plane k0-1 is the first face's left state
+    int buf = 1;
     for (int k = k0; k < k1; ++k) {
-        const Q5 cur[3] = {q[0], q[1], q[2]};
-        if (k + 1 < k1) plane(k + 1, q);
-        states(cur, wr, nu);
-        // z face: (vz | vx, vy)
-        Flux5 f;
-        hllc<true, kSel>(wl[gk::P_RHO], wl[gk::P_VZ], wl[gk::P_VX], wl[gk::P_VY], wl[gk::P_PRE],
-                         wr[gk::P_RHO], wr[gk::P_VZ], wr[gk::P_VX], wr[gk::P_VY], wr[gk::P_PRE], ph, f);
-        const long long c = fidx(g, k, j, i);
-        F3[gk::S_DEN * g.fvstride + c] = f.d;
-        F3[gk::S_MTZ * g.fvstride + c] = f.n;
-        F3[gk::S_MTX * g.fvstride + c] = f.t1;
-        F3[gk::S_MTY * g.fvstride + c] = f.t2;
-        F3[gk::S_ENG * g.fvstride + c] = f.e;
+        put(buf, t, qa);
+        if (two) put(buf, t + 128, qb);
+        if (k + 1 < k1) load(k + 1, qa, qb);
+        __syncthreads();  // plane k in sW[buf]; sW[buf ^ 1] is free for plane k+1
+        states(buf, wr, nu);
+        if (mine) {
+            // z face: (vz | vx, vy)
+            Flux5 f;
+            hllc<true, kSel>(wl[gk::P_RHO], wl[gk::P_VZ], wl[gk::P_VX], wl[gk::P_VY],
+                             wl[gk::P_PRE], wr[gk::P_RHO], wr[gk::P_VZ], wr[gk::P_VX],
+                             wr[gk::P_VY], wr[gk::P_PRE], ph, f);
+            const long long c = fidx(g, k, j, i);
+            F3[gk::S_DEN * g.fvstride + c] = f.d;
+            F3[gk::S_MTZ * g.fvstride + c] = f.n;
+            F3[gk::S_MTX * g.fvstride + c] = f.t1;
+            F3[gk::S_MTY * g.fvstride + c] = f.t2;
+            F3[gk::S_ENG * g.fvstride + c] = f.e;
+        }
 #pragma unroll
         for (int v = 0; v < 5; ++v) wl[v] = nu[v];
+        buf ^= 1;
     }
 }
 
