@@ -247,11 +247,13 @@ __global__ void __launch_bounds__(NT, 384 / NT)
     for (int f = y0 + 1; f <= y1; ++f) {
         const Q5 Q1 = Qn;
         if (f + 2 <= y1 + 1) Qn = load5(uc, g, at(f + 2));
-        // the z fluxes below and above cell row f-1, and its base state, are
-        // loaded here so that they arrive while the row's Riemann problems
-        // are solved
+        // fast mode: the z fluxes below and above cell row f-1, and its base
+        // state, are loaded here so that they arrive while the row's Riemann
+        // problems are solved (parity mode's longer IEEE sequences leave no
+        // registers for them: it loads them where they are used)
         double zlo[5], zhi[5], b0[5];
-        if (do_cell) {
+        constexpr bool kEarly = GK_FASTMATH;
+        auto load_row_inputs = [&]() {
             const long long fc = fidx(g, k, f - 1, xi);
             const long long c = at(f - 1);
 #pragma unroll
@@ -260,7 +262,8 @@ __global__ void __launch_bounds__(NT, 384 / NT)
                 zhi[v] = __ldg(F3 + v * g.fvstride + fc + g.fkstride);
                 b0[v] = THREE ? u0[v * g.vstride + c] : uc[v * g.vstride + c];
             }
-        }
+        };
+        if (kEarly && do_cell) load_row_inputs();
         const W5 P1 = c2p_q(Q1, ph);
 #pragma unroll
         for (int v = 0; v < 5; ++v) sP[v][t] = Pm1.v[v];
@@ -292,6 +295,7 @@ __global__ void __launch_bounds__(NT, 384 / NT)
         __syncthreads();
         if (do_cell) {
             // update_cons.cpp (3D): (Fx(i+1)-Fx(i))*dtdx + (Fy(j+1)-Fy(j))*dtdy + (Fz(k+1)-Fz(k))*dtdz
+            if (!kEarly) load_row_inputs();
             const long long c = at(f - 1);
             double r[5];
 #pragma unroll
