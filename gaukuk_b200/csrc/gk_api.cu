@@ -224,6 +224,7 @@ int build_ctx(gk_handle* h) {
     ph.gm1Rec = 1.0 / (pd.gamma - 1.0);
     ph.gmRec = 1.0 / pd.gamma;
     ph.cq = 0.5 * (1 + ph.gmRec);
+    ph.gm1Rec1 = ph.gm1Rec + 1.0;
     ph.cfl = pd.cfl;
     ph.dmin = pd.dfloor;
     ph.pmin = pd.pfloor;

@@ -173,10 +173,10 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
 #endif
     double ss = GK_DIV(prer - prel + denl * vxl * (sl - vxl) - denr * vxr * (sr - vxr),
                        denl * (sl - vxl) - denr * (sr - vxr));
-    // EquationOfState::EGas (eos.hpp:30-32) + kinetic energy
-    double kl = T2 ? (vxl * vxl + vyl * vyl + vzl * vzl) : (vxl * vxl + vyl * vyl);
-    double kr = T2 ? (vxr * vxr + vyr * vyr + vzr * vzr) : (vxr * vxr + vyr * vyr);
     auto both_sides = [&]() {
+        // EquationOfState::EGas (eos.hpp:30-32) + kinetic energy
+        double kl = T2 ? (vxl * vxl + vyl * vyl + vzl * vzl) : (vxl * vxl + vyl * vyl);
+        double kr = T2 ? (vxr * vxr + vyr * vyr + vzr * vzr) : (vxr * vxr + vyr * vyr);
         double el = prel * ph.gm1Rec + 0.5 * denl * kl;
         double er = prer * ph.gm1Rec + 0.5 * denr * kr;
         double cl = GK_DIV(smin(0.0, sl) * (ss - vxl), sl - ss);
@@ -207,18 +207,21 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
         both_sides();
         return;
     }
-    // The selected side, in the reference's expression order for that side.
+    // The selected side only (fast mode): its kinetic energy from the
+    // selected velocities, and E + p as p/(gamma-1) + p + rho k/2 in one
+    // product with gamma/(gamma-1).
     const bool left = GK_GE0(ss);
     double d = left ? denl : denr, vn = left ? vxl : vxr, v1 = left ? vyl : vyr;
     double v2 = left ? vzl : vzr, p = left ? prel : prer, s = left ? sl : sr;
-    double k = left ? kl : kr;
-    double e = p * ph.gm1Rec + 0.5 * d * k;
+    double k = T2 ? (vn * vn + v1 * v1 + v2 * v2) : (vn * vn + v1 * v1);
+    double ep = p * ph.gm1Rec1 + 0.5 * d * k;  // E + p
     double sc = left ? GK_MIN0(s) : GK_MAX0(s);
     double c = GK_DIV(sc * (ss - vn), s - ss);
-    double f1 = d * (vn + c);
+    double vc = vn + c;
+    double f1 = d * vc;
     f.d = f1;
     f.n = d * (vn * vn + c * s) + p;
     f.t1 = f1 * v1;
     f.t2 = T2 ? f1 * v2 : 0.0;
-    f.e = (e + p) * (vn + c) + d * c * ss * (s - vn);
+    f.e = ep * vc + d * c * ss * (s - vn);
 }
