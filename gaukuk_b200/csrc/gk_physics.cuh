@@ -171,8 +171,14 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
     double sl = vxl - al * ql;
     double sr = vxr + ar * qr;
 #endif
+#if GK_FASTMATH
+    // the contact speed with rho (S - v) of each side formed once
+    const double ml = denl * (sl - vxl), mr = denr * (sr - vxr);
+    double ss = GK_DIV(prer - prel + ml * vxl - mr * vxr, ml - mr);
+#else
     double ss = GK_DIV(prer - prel + denl * vxl * (sl - vxl) - denr * vxr * (sr - vxr),
                        denl * (sl - vxl) - denr * (sr - vxr));
+#endif
     auto both_sides = [&]() {
         // EquationOfState::EGas (eos.hpp:30-32) + kinetic energy
         double kl = T2 ? (vxl * vxl + vyl * vyl + vzl * vzl) : (vxl * vxl + vyl * vyl);
