@@ -225,6 +225,8 @@ int build_ctx(gk_handle* h) {
     ph.gmRec = 1.0 / pd.gamma;
     ph.cq = 0.5 * (1 + ph.gmRec);
     ph.gm1Rec1 = ph.gm1Rec + 1.0;
+    ph.gcq = ph.gamma * ph.cq;
+    ph.hgm1 = 0.5 * ph.gm1;
     ph.cfl = pd.cfl;
     ph.dmin = pd.dfloor;
     ph.pmin = pd.pfloor;

@@ -63,6 +63,8 @@ struct Shell {
 struct Phys {
     double gamma, gm1, gm1Rec, gmRec, cq;  // cq = 0.5*(1+1/gamma) (hllc.cpp:55-58)
     double gm1Rec1;                        // gm1Rec + 1: fast mode's E + p = p*gm1Rec1 + rho k/2
+    double gcq;                            // gamma*cq: fast mode's gamma X = gamma p + gcq max(p* - p, 0)
+    double hgm1;                           // (gamma-1)/2: fast mode's conversion
     double cfl, dmin, pmin;
     double grav[3];
     int has_grav;

@@ -391,12 +391,21 @@ __device__ __forceinline__ double floors4_inv(double (&r)[4], const Phys& ph, De
         return GK_RCP(ph.dmin);
     }
     double inv_den = GK_RCP(r[0]);
+#if GK_FASTMATH
+    const double m2 = r[1] * r[1] + r[2] * r[2];
+    double press = fma(-ph.hgm1 * inv_den, m2, ph.gm1 * r[3]);
+    if (GK_BELOW(press, ph.pmin)) {
+        r[3] = ph.pmin / ph.gm1 + 0.5 * inv_den * m2;
+        atomicAdd(&tm->floor_pre, 1ull);
+    }
+#else
     double ke = 0.5 * inv_den * (r[1] * r[1] + r[2] * r[2]);
     double press = ph.gm1 * (r[3] - ke);
     if (GK_BELOW(press, ph.pmin)) {
         r[3] = ph.pmin / ph.gm1 + ke;
         atomicAdd(&tm->floor_pre, 1ull);
     }
+#endif
     return inv_den;
 }
 
@@ -526,8 +535,12 @@ __device__ __forceinline__ double cell_cmax(double d, double mx, double my, doub
 __device__ __forceinline__ double cell_cmax_inv(double mx, double my, double e, double denInv,
                                                 const Phys& ph) {
     double vx = mx * denInv, vy = my * denInv;
+#if GK_FASTMATH
+    double pres = fma(-ph.hgm1, vx * mx + vy * my, ph.gm1 * e);
+#else
     double engKin = 0.5 * (vx * mx + vy * my);
     double pres = ph.gm1 * (e - engKin);
+#endif
     pres = GK_BELOW(ph.pmin, pres) ? pres : ph.pmin;
     double cs = GK_SQRT(ph.gamma * pres * denInv);
     double local = fabs(vx) + cs;
@@ -681,8 +694,13 @@ __device__ __forceinline__ W4 c2p4(const Q4& q, const Phys& ph) {
     double denInv = GK_RCP(d);
     w.vx = q.mx * denInv;
     w.vy = q.my * denInv;
+#if GK_FASTMATH
+    // p = (gamma-1) E - ((gamma-1)/2) |m|^2 / rho
+    double pre = fma(-ph.hgm1 * denInv, q.mx * q.mx + q.my * q.my, ph.gm1 * q.e);
+#else
     double engKin = 0.5 * denInv * (q.mx * q.mx + q.my * q.my);
     double pre = ph.gm1 * (q.e - engKin);
+#endif
     w.p = GK_BELOW(ph.pmin, pre) ? pre : ph.pmin;
     return w;
 }

@@ -150,8 +150,8 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
     // Branch-free on purpose: a skip when p* <= p (as in parity mode) was
     // measured slower, because it splits the straight-line code in which the
     // x- and y-face solves of a row interleave.
-    const double gxl = gamma * fma(ph.cq, GK_MAX0(prePVRS - prel), prel);
-    const double gxr = gamma * fma(ph.cq, GK_MAX0(prePVRS - prer), prer);
+    const double gxl = fma(ph.gcq, GK_MAX0(prePVRS - prel), gpl);
+    const double gxr = fma(ph.gcq, GK_MAX0(prePVRS - prer), gpr);
     double sl = vxl - gxl * rsqrt_nr(gxl * denl);
     double sr = vxr + gxr * rsqrt_nr(gxr * denr);
 #else
