@@ -6,7 +6,10 @@
 // on the state; with inflowWide = 1 it writes the constant state into the
 // corner ghosts as well, outside the side's strip; otherwise it writes a
 // constant inflow state into the strip, as the reference's solid-body hook
-// does (src/setup/setup_solid_body.cpp:62-96).
+// does (src/setup/setup_solid_body.cpp:62-96).  With inflowThrowAfter = N > 0
+// the routine throws from its (N+1)-th call on (a failing host routine).
+#include <stdexcept>
+
 #include "gaukuk.hpp"
 #include "sim.hpp"
 
@@ -27,6 +30,9 @@ void Sim::Setup() {
 }
 
 void Boundary::SelfDefineBDXL(TArray<Real>& cons, const Grid& grid, const EquationOfState& eos) {
+    static int calls = 0;
+    const int throw_after = static_cast<int>(Config::getInstance().get("inflowThrowAfter", 0));
+    if (throw_after > 0 && ++calls > throw_after) throw std::runtime_error("inflow routine failed");
     const bool copies = Config::getInstance().get("inflowCopies", 0) != 0;
     const bool wide = Config::getInstance().get("inflowWide", 0) != 0;
     const Real q[NVar] = {2.0, 2.0, 0.0, 0.0, 1.0 + eos.EGas(2.0, 1.0)};

@@ -180,6 +180,25 @@ def test_state_dependent_side_matches_the_reference(tmp_path):
         assert (a / f).read_bytes() == (b / f).read_bytes(), f
 
 
+@pytest.mark.gpu
+def test_failing_host_side_stops_the_run_with_its_message(tmp_path):
+    """A host-run boundary routine that throws during the device run: the
+    library stops at that ghost fill and the driver ends with the routine's
+    message (the exception does not cross the C ABI)."""
+    from gaukuk_b200 import _build_host
+    src = os.path.join(ROOT, "tests", "setups", "setup_inflow_sides.cpp")
+    exe = _build_host.build_hook(src, name="inflow_sides", out_dir=str(tmp_path))
+    # 6 calls on the host (the setup's ghost fill and the probes), then two
+    # per step on the device: the 9th call, in the second step, throws
+    (tmp_path / "run.in").write_text(INFLOW.to_in_text({"inflowCopies": 1,
+                                                         "inflowThrowAfter": 8}))
+    r = subprocess.run([exe, "-i", "run.in"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode != 0
+    assert "self-defined boundary: inflow routine failed" in r.stderr, r.stderr[-2000:]
+    assert "step = 1," in r.stdout  # the first step ran on the device
+
+
 PRIM_CASES = ["kh", "disk", "blast", "solid_body"]
 
 
