@@ -98,6 +98,7 @@ SIGNATURES = {
     "gk_tap_substeps": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _vp]),
     "gk_slab_layout": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       _ip, _ip, _ip, _ip]),
+    "gk_slab_exchange_plan": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _ip]),
     "gk_slabs_create": (ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(PhysDesc),
                                        ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "gk_slabs_nccl_id": (ctypes.c_int, [_vp]),

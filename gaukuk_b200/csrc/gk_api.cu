@@ -1760,6 +1760,23 @@ void slab_rows(int ny, int n, int k, int* j0, int* cnt) {
     *j0 = k * base + (k < rem ? k : rem);
 }
 
+// The NCCL calls of one halo exchange of slab k of n, in order: rows going
+// up first (send the top rows to the upper neighbour, receive the lower
+// ghosts from the lower one), then rows going down.  Between any two ranks
+// the k-th send then matches the k-th receive, a single ring slab
+// exchanging with itself included.  Each op: {kind, peer}, kind 0 send top
+// rows, 1 receive lower ghosts, 2 send bottom rows, 3 receive upper ghosts.
+int slab_exchange_plan(int n, int k, bool periodic, int (*ops)[2]) {
+    int m = 0;
+    const int lower = k > 0 ? k - 1 : (periodic ? n - 1 : -1);
+    const int upper = k < n - 1 ? k + 1 : (periodic ? 0 : -1);
+    if (upper >= 0) { ops[m][0] = 0; ops[m][1] = upper; ++m; }
+    if (lower >= 0) { ops[m][0] = 1; ops[m][1] = lower; ++m; }
+    if (lower >= 0) { ops[m][0] = 2; ops[m][1] = lower; ++m; }
+    if (upper >= 0) { ops[m][0] = 3; ops[m][1] = upper; ++m; }
+    return m;
+}
+
 // Neighbours of slab k of n: -1 where the y side is the grid's own boundary
 // (filled by the ghost fill); with periodic y the first and last slabs are
 // each other's neighbours (a single slab is its own).
@@ -1895,14 +1912,17 @@ int slabs_halo(gk_slabs* G, int role) {
     double *slo = G->xbuf, *shi = G->xbuf + cnt, *rlo = G->xbuf + 2 * cnt, *rhi = G->xbuf + 3 * cnt;
     double* u = slab_buf(h, role);
     gk::launch_slab_pack(u, slo, shi, g, h->ctx.tm, G->stream);
-    // rows going up first, then rows going down: between any two ranks the
-    // k-th send matches the k-th receive, self-exchange of a single ring
-    // slab included
+    int ops[4][2];
+    const int nops = slab_exchange_plan(G->nslab, G->first, G->pd.bc[2] == 1, ops);
+    double* const bufs[4] = {shi, rlo, slo, rhi};
     GK_SNCCL(G, G->nccl->GroupStart());
-    if (G->upper >= 0) GK_SNCCL(G, G->nccl->Send(shi, cnt, ncclDouble, G->upper, G->comm, G->stream));
-    if (G->lower >= 0) GK_SNCCL(G, G->nccl->Recv(rlo, cnt, ncclDouble, G->lower, G->comm, G->stream));
-    if (G->lower >= 0) GK_SNCCL(G, G->nccl->Send(slo, cnt, ncclDouble, G->lower, G->comm, G->stream));
-    if (G->upper >= 0) GK_SNCCL(G, G->nccl->Recv(rhi, cnt, ncclDouble, G->upper, G->comm, G->stream));
+    for (int o = 0; o < nops; ++o) {
+        double* b = bufs[ops[o][0]];
+        if (ops[o][0] == 0 || ops[o][0] == 2)
+            GK_SNCCL(G, G->nccl->Send(b, cnt, ncclDouble, ops[o][1], G->comm, G->stream));
+        else
+            GK_SNCCL(G, G->nccl->Recv(b, cnt, ncclDouble, ops[o][1], G->comm, G->stream));
+    }
     GK_SNCCL(G, G->nccl->GroupEnd());
     gk::launch_slab_unpack(u, G->lower >= 0 ? rlo : nullptr, G->upper >= 0 ? rhi : nullptr, g,
                            h->ctx.tm, G->stream);
@@ -2012,6 +2032,17 @@ int gk_slab_layout(int ny, int nslab, int k, int periodic, int* j0, int* rows, i
     if (rows) *rows = b;
     if (lower) *lower = c;
     if (upper) *upper = d;
+    return GK_OK;
+}
+
+int gk_slab_exchange_plan(int nslab, int k, int periodic, int* ops8, int* nops) {
+    if (nslab < 1 || k < 0 || k >= nslab || !ops8 || !nops) return GK_ERR_INVALID;
+    int ops[4][2];
+    *nops = slab_exchange_plan(nslab, k, periodic != 0, ops);
+    for (int o = 0; o < *nops; ++o) {
+        ops8[2 * o] = ops[o][0];
+        ops8[2 * o + 1] = ops[o][1];
+    }
     return GK_OK;
 }
 

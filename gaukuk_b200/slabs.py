@@ -31,6 +31,18 @@ def layout(ny: int, nslab: int, k: int, periodic: bool) -> Tuple[int, int, int, 
     return tuple(o.value for o in out)
 
 
+def exchange_plan(nslab: int, k: int, periodic: bool) -> List[Tuple[int, int]]:
+    """The library's NCCL calls for one halo exchange of slab k, in order:
+    (kind, peer) with kind 0 send top rows, 1 receive lower ghosts, 2 send
+    bottom rows, 3 receive upper ghosts.  Host only."""
+    L = _lib.load()
+    ops = (ctypes.c_int * 8)()
+    n = ctypes.c_int()
+    _lib.check(L.gk_slab_exchange_plan(int(nslab), int(k), int(bool(periodic)), ops,
+                                       ctypes.byref(n)))
+    return [(ops[2 * o], ops[2 * o + 1]) for o in range(n.value)]
+
+
 class _SlabsBase:
     def __init__(self, params: Params):
         self.params = params

@@ -391,6 +391,12 @@ typedef struct gk_slabs gk_slabs;
  * the grid, filled by the ghost fill).  Host only. */
 int gk_slab_layout(int ny, int nslab, int k, int periodic, int* j0, int* rows, int* lower,
                    int* upper);
+/* The NCCL calls of one halo exchange of slab k, in the order the library
+ * makes them: nops pairs {kind, peer} in ops8, kind 0 send the top rows,
+ * 1 receive the lower ghost rows, 2 send the bottom rows, 3 receive the
+ * upper ghost rows (rows going up first, then down: between two ranks the
+ * k-th send matches the k-th receive).  Host only. */
+int gk_slab_exchange_plan(int nslab, int k, int periodic, int* ops8, int* nops);
 /* nslab slabs in this process, on phys->device, exchanging through device
  * copies on one stream (a grid emulated as slabs on one GPU, or slabs that
  * share a GPU). */

@@ -36,6 +36,54 @@ def test_partition_covers_every_row_once():
                 assert firsts == sorted(firsts, reverse=True)  # the extra rows go first
 
 
+def _run_plans(n, periodic):
+    """Match every rank's planned NCCL calls as NCCL pairs point-to-point
+    operations (the k-th send from a to b meets the k-th receive on b from
+    a) and return, per rank, which rows each receive delivered:
+    {rank: {"lower": (src rank, "top"|"bottom"), "upper": ...}}."""
+    from gaukuk_b200.slabs import exchange_plan
+    sends, recvs = {}, {}
+    for k in range(n):
+        for kind, peer in exchange_plan(n, k, periodic):
+            if kind in (0, 2):
+                sends.setdefault((k, peer), []).append("top" if kind == 0 else "bottom")
+            else:
+                recvs.setdefault((peer, k), []).append("lower" if kind == 1 else "upper")
+    got = {k: {} for k in range(n)}
+    assert sorted(sends) == sorted(recvs)  # every send has a receive and back
+    for (a, b), rows in sends.items():
+        targets = recvs[(a, b)]
+        assert len(rows) == len(targets)
+        for r, t in zip(rows, targets):
+            got[b][t] = (a, r)
+    return got
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 8])
+def test_nccl_exchange_plan_delivers_the_right_rows(n, periodic):
+    """Each slab's lower ghost rows must come from its lower neighbour's top
+    rows and its upper ghosts from its upper neighbour's bottom rows (a
+    ring under periodic y; none at the grid's own sides), for the calls in
+    the order the library makes them."""
+    if n == 1 and not periodic:
+        from gaukuk_b200.slabs import exchange_plan
+        assert exchange_plan(1, 0, False) == []
+        return
+    got = _run_plans(n, periodic)
+    for k in range(n):
+        lower = k - 1 if k > 0 else (n - 1 if periodic else None)
+        upper = k + 1 if k < n - 1 else (0 if periodic else None)
+        if lower is None:
+            assert "lower" not in got[k]
+        else:
+            assert got[k]["lower"] == (lower, "top"), (k, got[k])
+        if upper is None:
+            assert "upper" not in got[k]
+        else:
+            assert got[k]["upper"] == (upper, "bottom"), (k, got[k])
+
+
 def _free_port() -> int:
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
