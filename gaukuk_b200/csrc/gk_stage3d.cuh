@@ -198,8 +198,13 @@ __global__ void __launch_bounds__(128)
 // step's last stage also reduces the CFL speed of the new state (CalCmax,
 // adiabatic.cpp:115-160, on the values it writes) and its last CTA runs the
 // step epilogue, as k_cfl would after it.
+// Resident threads per SM: 384 in fast mode (up to 168 registers each), 512
+// in parity mode (128 registers, with 16-72 bytes of spills).  At 256^3 (CTAs of 96) parity
+// mode went from 5.39 to 5.13 ms per step with the extra warps, while fast
+// mode, whose early row loads need the registers, went from 2.28 to 2.42.
+constexpr int kStage3dThreadsPerSM = GK_FASTMATH ? 384 : 512;
 template <int NT, bool THREE, bool PLM, bool LAST>
-__global__ void __launch_bounds__(NT, 384 / NT)
+__global__ void __launch_bounds__(NT, kStage3dThreadsPerSM / NT)
     k_stage3d(const double* __restrict__ uc, const double* u0, double* out,
               const double* __restrict__ F3, Geom g, Phys ph, double c1, double c2, double c3,
               DevTime* tm, int rows) {
