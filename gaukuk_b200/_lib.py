@@ -94,6 +94,7 @@ SIGNATURES = {
     "gk_set_flux_model": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                          ctypes.c_float, ctypes.c_float]),
     "gk_flux_model_fired": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint)]),
+    "gk_set_flux_model_fused": (ctypes.c_int, [_vp, ctypes.c_int]),
     "gk_face_fluxes": (ctypes.c_int, [_vp, _vp, _vp]),
     "gk_tap_substeps": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _vp]),
     "gk_slab_layout": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,

@@ -74,6 +74,7 @@ struct KernelSet {
     decltype(&gk_parity::launch_zflux) zflux;
     decltype(&gk_parity::launch_stage3d) stage3d;
     decltype(&gk_parity::launch_epilogue) epilogue;
+    decltype(&gk_parity::launch_stage2d_learn) stage2d_learn;
 };
 
 const KernelSet kParity = {gk_parity::launch_bc,     gk_parity::launch_c2p,
@@ -83,12 +84,13 @@ const KernelSet kParity = {gk_parity::launch_bc,     gk_parity::launch_c2p,
                            gk_parity::launch_mtz_check, gk_parity::launch_ens_stage,
                            gk_parity::launch_ens_bc,  gk_parity::launch_ens_begin,
                            gk_parity::launch_zflux,   gk_parity::launch_stage3d,
-                           gk_parity::launch_epilogue};
+                           gk_parity::launch_epilogue, gk_parity::launch_stage2d_learn};
 const KernelSet kFast = {gk_fast::launch_bc,     gk_fast::launch_c2p,     gk_fast::launch_flux,
                          gk_fast::launch_update, gk_fast::launch_kick,    gk_fast::launch_cfl,
                          gk_fast::launch_stage2d, gk_fast::launch_begin,  gk_fast::launch_mtz_check,
                          gk_fast::launch_ens_stage, gk_fast::launch_ens_bc, gk_fast::launch_ens_begin,
-                         gk_fast::launch_zflux, gk_fast::launch_stage3d, gk_fast::launch_epilogue};
+                         gk_fast::launch_zflux, gk_fast::launch_stage3d, gk_fast::launch_epilogue,
+                         gk_fast::launch_stage2d_learn};
 
 constexpr int kLogCap = 1 << 20;
 
@@ -124,6 +126,7 @@ struct gk_handle {
     bool tiling_set = false;  // gk_set_tiling overrides the default tiling
     float* model = nullptr;   // learned flux correction (device), or null
     gk::FluxGate gate;
+    int learn_fused = 1;      // the correction runs inside the fused 2D stage where it can
     double* fixed = nullptr;  // state at enrollment of fixed boundaries (device layout)
     gk::Shell* shells = nullptr;  // immersed body's shell table (device)
     int shell_cap = 0;
@@ -351,16 +354,23 @@ int stage_rows(const gk::Geom& g, int threads, bool parity) {
 }
 
 // Path 1, the fused 2D stage, applies to 2D RK2/RK3 runs with MTZ
-// identically zero, no z gravity (it would make MTZ non-zero), no point
+// identically zero, no z gravity (it would make MTZ non-zero) and no point
 // masses (their kicks run between the fused stages' CFL reduction and the
-// epilogue) and no learned correction.  Path 2, the 3D stage (z fluxes, then
-// one fused x-y stage per plane), applies to 3D RK2/RK3 runs (forward Euler
-// updates in place, which the fused stage cannot).  Path 0 is generic.
+// epilogue).  With a learned correction it takes the stage with the network
+// at every face (TMA rows; unless gk_set_flux_model_fused turned that off).
+// Path 2, the 3D stage (z fluxes, then one fused x-y stage per plane),
+// applies to 3D RK2/RK3 runs (forward Euler updates in place, which the
+// fused stage cannot).  Path 0 is generic.
 int choose_path(const gk_handle* h) {
     const gk::Ctx& c = h->ctx;
     if (c.g.ndim == 3 && c.ph.integrator != 1 && env_int("GK_STAGE3D", 1) != 0) return 2;
-    return (c.g.ndim == 2 && !c.has_vz && c.ph.integrator != 1 && c.ph.grav[2] == 0 &&
-            c.ph.npoint == 0 && !h->model) ? 1 : 0;
+    if (!(c.g.ndim == 2 && !c.has_vz && c.ph.integrator != 1 && c.ph.grav[2] == 0 &&
+          c.ph.npoint == 0))
+        return 0;
+    if (!h->model) return 1;
+    if (!h->learn_fused || !c.use_tma || !h->A) return 0;
+    CUtensorMap probe;
+    return gk::encode_rows_map(&probe, h->A, c.g, c.stage_threads == 64 ? 64 : 128) ? 1 : 0;
 }
 
 // Sides filled by host routines (gk_set_host_fill), after the device ghost
@@ -484,16 +494,24 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
     }
     if (h->path == 1) {
         // the last stage also applies the second half kick, the CFL
-        // reduction and the step epilogue
+        // reduction and the step epilogue; with a learned correction the
+        // stage applies it at every face
+        auto stage = [&](const double* uc, const double* u0, double* out, int kind, double c1,
+                         double c2, double c3) {
+            if (h->model)
+                k.stage2d_learn(c, uc, u0, out, kind, c1, c2, c3, h->model, h->gate, h->fired, s);
+            else
+                k.stage2d(c, uc, u0, out, kind, c1, c2, c3, s);
+        };
         GK_L(gk::K_BC, fill(A));
-        GK_L(gk::K_STAGE, k.stage2d(c, A, nullptr, B, 0, 1.0, 1.0, 0.0, s));
+        GK_L(gk::K_STAGE, stage(A, nullptr, B, 0, 1.0, 1.0, 0.0));
         GK_L(gk::K_BC, fill(B));
         if (integ == 3) {
-            GK_L(gk::K_STAGE, k.stage2d(c, B, A, Cb, 1, 0.75, 0.25, 0.25, s));
+            GK_L(gk::K_STAGE, stage(B, A, Cb, 1, 0.75, 0.25, 0.25));
             GK_L(gk::K_BC, fill(Cb));
-            GK_L(gk::K_STAGE, k.stage2d(c, Cb, A, A, 2, frac13, 2 * frac13, 2 * frac13, s));
+            GK_L(gk::K_STAGE, stage(Cb, A, A, 2, frac13, 2 * frac13, 2 * frac13));
         } else {
-            GK_L(gk::K_STAGE, k.stage2d(c, B, A, A, 2, 0.5, 0.5, 0.5, s));
+            GK_L(gk::K_STAGE, stage(B, A, A, 2, 0.5, 0.5, 0.5));
         }
         return;
     }
@@ -630,6 +648,8 @@ int status_error(gk_handle* h) {
     const int st = h->htm->status;
     if (st & gk::STATUS_TMA_TIMEOUT)
         return fail(h, GK_ERR_CUDA, "a TMA row load did not complete within the stage kernel's wait limit");
+    if (st & gk::STATUS_NO_MAP)
+        return fail(h, GK_ERR_CUDA, "the learned stage's tensor map could not be encoded");
     if (st) return fail(h, GK_ERR_NONFINITE, "CFL reduction met a non-finite state");
     return GK_OK;
 }
@@ -1309,7 +1329,7 @@ int gk_ens_create(gk_handle* const* handles, int n, gk_ensemble** out) {
         gk_handle* h = handles[i];
         if (!h || !h->uploaded) return GK_ERR_STATE;
         if (h->path != 1 || h->ctx.ph.integrator != 2 || h->ctx.ph.fix_inner ||
-            !h->host_fills.empty())
+            !h->host_fills.empty() || h->model)
             return GK_ERR_UNSUPPORTED;
         // an instance's physics is copied here: fixed data must already be set
         for (int s = 0; s < 6; ++s)
@@ -1668,6 +1688,24 @@ extern "C" int gk_set_flux_model(gk_handle* h, const float* model_host, int nmod
     // the path and the graph follow the model
     if (h->uploaded) {
         const gk::Geom& g = h->ctx.g;
+        h->path = choose_path(h);
+        if (h->path != 1) {
+            int rc = alloc_generic(h);
+            if (rc != GK_OK) return rc;
+        }
+    }
+    if (h->gexec) {
+        cudaGraphExecDestroy(h->gexec);
+        h->gexec = nullptr;
+    }
+    return GK_OK;
+}
+
+extern "C" int gk_set_flux_model_fused(gk_handle* h, int fused) {
+    if (!h || (fused != 0 && fused != 1)) return GK_ERR_INVALID;
+    GK_CUDA(h, cudaSetDevice(h->device));
+    h->learn_fused = fused;
+    if (h->uploaded) {
         h->path = choose_path(h);
         if (h->path != 1) {
             int rc = alloc_generic(h);

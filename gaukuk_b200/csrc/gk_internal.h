@@ -110,7 +110,7 @@ struct DevTime {
     unsigned long long floor_den, floor_pre;
 };
 
-enum { STATUS_NONFINITE = 1, STATUS_TMA_TIMEOUT = 2 };
+enum { STATUS_NONFINITE = 1, STATUS_TMA_TIMEOUT = 2, STATUS_NO_MAP = 4 };
 
 struct Ctx {
     Geom g;
@@ -221,6 +221,10 @@ static const char* const kClassNames[K_NCLASS] = {
     void launch_cfl(const gk::Ctx& c, const double* u, int epilogue, cudaStream_t s);          \
     void launch_stage2d(const gk::Ctx& c, const double* uc, const double* u0, double* out,     \
                         int kind, double c1, double c2, double c3, cudaStream_t s);            \
+    void launch_stage2d_learn(const gk::Ctx& c, const double* uc, const double* u0,           \
+                              double* out, int kind, double c1, double c2, double c3,          \
+                              const float* model, const gk::FluxGate& gate, unsigned* fired,   \
+                              cudaStream_t s);                                                 \
     void launch_begin(const gk::Ctx& c, double dtoutput, int steps, cudaStream_t s);           \
     void launch_epilogue(const gk::Ctx& c, cudaStream_t s);                                    \
     int checked_report(unsigned long long* count, unsigned long long* first);                  \

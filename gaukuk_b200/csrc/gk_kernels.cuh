@@ -17,6 +17,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 #include <math_constants.h>
 
@@ -34,6 +35,7 @@
 namespace GK_NS {
 
 #include "gk_physics.cuh"
+#include "gk_learn.cuh"
 
 using gk::Ctx;
 using gk::DevTime;
@@ -1005,6 +1007,107 @@ struct StageShared {
     int last;
 };
 
+// The learned flux correction inside the fused stage (the stage with LEARN):
+// each row's x and y faces get the correction the generic path's pass
+// (k_flux_correct, gk_mlp.cu) would add, from the same functions
+// (gk_learn.cuh).  Per warp and row, the 32 x faces and 32 y faces of its
+// lanes are 4 tiles of 16 for the tensor cores: slots 0..31 the x faces of
+// lanes 0..31, slots 32..63 their y faces.
+struct LearnWarp {
+    alignas(16) __nv_bfloat16 x[64 * gklearn::NI];  // standardised inputs per slot
+    float y[64][4];                                 // standardised outputs per slot
+};
+struct LearnArgs {
+    const gklearn::MlpWeights* w;  // shared memory
+    LearnWarp* warps;              // shared memory, one per warp
+    gk::FluxGate gate;
+    unsigned* fired;               // faces the detector left to plain HLLC
+};
+
+// The stencil of a face from four cells along its normal: density, normal
+// and tangential velocity, pressure.
+struct Stencil4 {
+    double r[4], vn[4], vt[4], p[4];
+};
+__device__ __forceinline__ Stencil4 stencil_x(const W4& a, const W4& b, const W4& c, const W4& d) {
+    return Stencil4{{a.r, b.r, c.r, d.r}, {a.vx, b.vx, c.vx, d.vx}, {a.vy, b.vy, c.vy, d.vy},
+                    {a.p, b.p, c.p, d.p}};
+}
+__device__ __forceinline__ Stencil4 stencil_y(const W4& a, const W4& b, const W4& c, const W4& d) {
+    return Stencil4{{a.r, b.r, c.r, d.r}, {a.vy, b.vy, c.vy, d.vy}, {a.vx, b.vx, c.vx, d.vx},
+                    {a.p, b.p, c.p, d.p}};
+}
+
+// Corrects this lane's x face (when hasx) and y face (when hasy); every lane
+// of the warp takes part.  A vetoed face keeps its flux; *nfired counts the
+// vetoed faces this lane owns (countx / county).
+__device__ __forceinline__ void learn_faces(const LearnArgs& la, bool hasx, const Stencil4& sx,
+                                            bool countx, Flux5& fx, double dtdx, bool hasy,
+                                            const Stencil4& sy, bool county, Flux5& fy,
+                                            double dtdy, const Phys& ph, unsigned& nfired) {
+    using namespace gklearn;
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    LearnWarp& lw = la.warps[threadIdx.x >> 5];
+    const MlpWeights& w = *la.w;
+    FaceScale fsx, fsy;
+    fsx.gate = fsy.gate = 2.f;
+    if (hasx) {
+        face_inputs(sx.r, sx.vn, sx.vt, sx.p, ph.gamma, ph.gm1Rec, la.gate, w.norm, lw.x + lane * NI, fsx);
+    } else {
+#pragma unroll
+        for (int e = 0; e < NI; ++e) lw.x[lane * NI + e] = __float2bfloat16_rn(0.f);
+    }
+    if (hasy) {
+        face_inputs(sy.r, sy.vn, sy.vt, sy.p, ph.gamma, ph.gm1Rec, la.gate, w.norm, lw.x + (32 + lane) * NI, fsy);
+    } else {
+#pragma unroll
+        for (int e = 0; e < NI; ++e) lw.x[(32 + lane) * NI + e] = __float2bfloat16_rn(0.f);
+    }
+    // the x tiles and the y tiles each run only where a face needs the
+    // network (none keep plain HLLC because they are absent or smooth)
+    const unsigned needx = __ballot_sync(0xffffffffu, fsx.gate != 2.f);
+    const unsigned needy = __ballot_sync(0xffffffffu, fsy.gate != 2.f);
+    __syncwarp();
+    auto put = [&](int tile, const float (&y)[4]) {
+        if (t < 2) {
+            lw.y[tile * 16 + g][2 * t] = y[0];
+            lw.y[tile * 16 + g][2 * t + 1] = y[1];
+            lw.y[tile * 16 + g + 8][2 * t] = y[2];
+            lw.y[tile * 16 + g + 8][2 * t + 1] = y[3];
+        }
+    };
+    if (needx) {
+        float y[2][4];
+        forward_tiles<2>(w, lw.x, y);
+        put(0, y[0]);
+        put(1, y[1]);
+    }
+    if (needy) {
+        float y[2][4];
+        forward_tiles<2>(w, lw.x + 32 * NI, y);
+        put(2, y[0]);
+        put(3, y[1]);
+    }
+    __syncwarp();
+    auto apply = [&](int slot, const FaceScale& fs, bool count, Flux5& f, double dtn) {
+        if (fs.gate == 2.f) return;
+        double c[4];
+#pragma unroll
+        for (int o = 0; o < 4; ++o) c[o] = face_correction(lw.y[slot][o], o, fs, w.norm);
+        if (face_vetoed(c[0], c[3], dtn, fs, la.gate)) {
+            nfired += count ? 1u : 0u;
+            return;
+        }
+        f.d += c[0];
+        f.n += c[1];
+        f.t1 += c[2];
+        f.e += c[3];
+    };
+    apply(lane, fsx, countx, fx, dtdx);
+    apply(32 + lane, fsy, county, fy, dtdy);
+    __syncwarp();  // lw may be refilled
+}
+
 template <int NT>
 __device__ __forceinline__ void stage_init_barriers(StageShared<NT>& sm) {
     if (threadIdx.x == 0) {
@@ -1019,13 +1122,15 @@ __device__ __forceinline__ void stage_init_barriers(StageShared<NT>& sm) {
 // they fix each row's ring slot and mbarrier phase across tiles.
 // tiles_total: tiles of this problem; the LAST stage's last tile runs the
 // step epilogue.
-template <int NT, int KIND, bool PLM>
+// LEARN: the learned flux correction of every face (la, k_stage2d_learn).
+template <int NT, int KIND, bool PLM, bool LEARN = false>
 __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CUtensorMap* map0,
                                                double* out, const Geom& g, const Phys& ph,
                                                double c1, double c2, double c3, DevTime* tm,
                                                int rows, int bx, int by, unsigned tiles_total,
                                                double* ring, double* ring0, StageShared<NT>& sm,
-                                               unsigned& seq, unsigned& seq0) {
+                                               unsigned& seq, unsigned& seq0,
+                                               const LearnArgs* la = nullptr) {
     constexpr bool THREE = KIND >= 1;
     constexpr bool LAST = KIND == 2;
     constexpr int COLS = NT - 4;
@@ -1097,7 +1202,8 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
 
     // prologue: primitives of rows y0-2, y0-1, y0
     wait(y0 - 2);
-    const W4 Pm2 = c2p4(rowq(y0 - 2), ph);
+    W4 Pm2 = c2p4(rowq(y0 - 2), ph);
+    unsigned nfired = 0;  // LEARN: vetoed faces this thread owns
     wait(y0 - 1);
     W4 Pm1 = c2p4(rowq(y0 - 1), ph);
     wait(y0);
@@ -1120,6 +1226,14 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
             wlNew = plus_half(P0, s);
         }
         hllc_y(wlNext, wr, ph, fyPrev);
+        if constexpr (LEARN) {
+            // y face y0 (rows y0-2 .. y0+1); the segment below computes it
+            // too, so only the grid's first segment counts its veto
+            Flux5 none{};
+            learn_faces(*la, false, Stencil4{}, false, none, dtdx, do_cell,
+                        stencil_y(Pm2, Pm1, P0, P1), do_cell && by == 0, fyPrev, dtdy, ph, nfired);
+            Pm2 = Pm1;
+        }
         wlNext = wlNew;
         Pm1 = P0;
         P0 = P1;
@@ -1158,6 +1272,21 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
         Flux5 fx, fy;
         hllc_x(xl_state, xr, ph, fx);
         hllc_y(wlNext, wr, ph, fy);
+        if constexpr (LEARN) {
+            // x face (xi-1 | xi) of row f-1: cells xi-2 .. xi+1 of sP; a face
+            // computed by two strips counts its veto in the strip that
+            // updates cell xi (the grid's last face: cell xi-1)
+            const int ta = t >= 2 ? t - 2 : 0;
+            const double2 e0 = sm.sP[0][ta], e1 = sm.sP[1][ta];
+            const double2 l0 = sm.sP[0][tl], l1 = sm.sP[1][tl];
+            const double2 r0 = sm.sP[0][tr], r1 = sm.sP[1][tr];
+            const bool hasx = t >= 2 && t <= NT - 2 && xi >= g.ib && xi <= g.ie;
+            learn_faces(*la, hasx,
+                        stencil_x(W4{e0.x, e0.y, e1.x, e1.y}, W4{l0.x, l0.y, l1.x, l1.y}, Pm1,
+                                  W4{r0.x, r0.y, r1.x, r1.y}),
+                        hasx && (t <= NT - 3 || xi == g.ie), fx, dtdx, do_cell,
+                        stencil_y(Pm2, Pm1, P0, P1), do_cell, fy, dtdy, ph, nfired);
+        }
         sm.sF[0][t] = make_double2(fx.d, fx.n); sm.sF[1][t] = make_double2(fx.t1, fx.e);
         __syncthreads();
         if (THREE) wait0(f - 1);
@@ -1212,8 +1341,14 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
         }
         fyPrev = fy;
         wlNext = wlNew;
+        if (LEARN) Pm2 = Pm1;
         Pm1 = P0;
         P0 = P1;
+    }
+    if constexpr (LEARN) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nfired += __shfl_xor_sync(0xffffffffu, nfired, o);
+        if ((t & 31) == 0 && nfired && la->fired) atomicAdd(la->fired, nfired);
     }
     if (LAST) {
 #pragma unroll
@@ -1247,7 +1382,7 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
 }
 
 template <int NT, bool THREE>
-constexpr size_t stage_dyn_bytes() {
+__host__ __device__ constexpr size_t stage_dyn_bytes() {
     return (size_t)(kRing + (THREE ? kRing0 : 0)) * 4 * NT * sizeof(double);
 }
 
@@ -1264,6 +1399,34 @@ __global__ void __launch_bounds__(NT, 512 / NT)
     stage_tile_tma<NT, KIND, PLM>(&mapc, &map0, out, g, ph, c1, c2, c3, tm, rows, blockIdx.x,
                                   blockIdx.y, gridDim.x * gridDim.y, dyn, dyn + kRing * 4 * NT, sm,
                                   seq, seq0);
+}
+
+// The fused stage with the learned flux correction at every face.  Dynamic
+// shared memory: the row rings, then the network (BF16 weights) and one
+// LearnWarp per warp.
+template <int NT, bool THREE>
+__host__ __device__ constexpr size_t learn_dyn_bytes() {
+    return stage_dyn_bytes<NT, THREE>() + sizeof(gklearn::MlpWeights) + (NT / 32) * sizeof(LearnWarp);
+}
+
+template <int NT, int KIND, bool PLM>
+__global__ void __launch_bounds__(NT, 256 / NT)
+    k_stage2d_learn(const __grid_constant__ CUtensorMap mapc, const __grid_constant__ CUtensorMap map0,
+                    double* out, Geom g, Phys ph, double c1, double c2, double c3, DevTime* tm,
+                    int rows, const float* __restrict__ model, gk::FluxGate gate, unsigned* fired) {
+    if (!tm->active) return;
+    extern __shared__ __align__(128) double dyn[];
+    __shared__ StageShared<NT> sm;
+    unsigned char* lp = reinterpret_cast<unsigned char*>(dyn) + stage_dyn_bytes<NT, (KIND >= 1)>();
+    auto* w = reinterpret_cast<gklearn::MlpWeights*>(lp);
+    auto* lw = reinterpret_cast<LearnWarp*>(lp + sizeof(gklearn::MlpWeights));
+    gklearn::load_weights(*w, model);
+    stage_init_barriers(sm);  // its barrier also publishes the weights
+    const LearnArgs la{w, lw, gate, fired};
+    unsigned seq = 0, seq0 = 0;
+    stage_tile_tma<NT, KIND, PLM, true>(&mapc, &map0, out, g, ph, c1, c2, c3, tm, rows, blockIdx.x,
+                                        blockIdx.y, gridDim.x * gridDim.y, dyn, dyn + kRing * 4 * NT,
+                                        sm, seq, seq0, &la);
 }
 
 // Persistent stage over an ensemble: tiles[i] = (instance, tile of that
@@ -1464,6 +1627,59 @@ static void launch_stage2d_tma_nt(const Ctx& c, const CUtensorMap& mc, const CUt
         else if (kind == 1) launch_stage2d_tma<NT, 1, false>(c, mc, m0, out, c1, c2, c3, s);
         else launch_stage2d_tma<NT, 2, false>(c, mc, m0, out, c1, c2, c3, s);
     }
+}
+
+template <int NT, int KIND, bool PLM>
+static void launch_stage2d_learn_k(const Ctx& c, const CUtensorMap& mc, const CUtensorMap& m0,
+                                   double* out, double c1, double c2, double c3, const float* model,
+                                   const gk::FluxGate& gate, unsigned* fired, cudaStream_t s) {
+    const Geom& g = c.g;
+    const int rows = c.h2d_rows;
+    dim3 grid((g.nx + NT - 5) / (NT - 4), (g.ny + rows - 1) / rows);
+    const size_t dyn = learn_dyn_bytes<NT, (KIND >= 1)>();
+    static std::atomic<unsigned long long> attr_set{0};
+    if (gk::first_on_device(attr_set))
+        cudaFuncSetAttribute(k_stage2d_learn<NT, KIND, PLM>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    k_stage2d_learn<NT, KIND, PLM><<<grid, NT, dyn, s>>>(mc, m0, out, g, c.ph, c1, c2, c3, c.tm, rows,
+                                                         model, gate, fired);
+}
+
+template <int NT>
+static void launch_stage2d_learn_nt(const Ctx& c, const CUtensorMap& mc, const CUtensorMap& m0,
+                                    double* out, int kind, double c1, double c2, double c3,
+                                    const float* model, const gk::FluxGate& gate, unsigned* fired,
+                                    cudaStream_t s) {
+#define GK_SL(K, PL) launch_stage2d_learn_k<NT, K, PL>(c, mc, m0, out, c1, c2, c3, model, gate, fired, s)
+    if (c.ph.plm) {
+        if (kind == 0) GK_SL(0, true);
+        else if (kind == 1) GK_SL(1, true);
+        else GK_SL(2, true);
+    } else {
+        if (kind == 0) GK_SL(0, false);
+        else if (kind == 1) GK_SL(1, false);
+        else GK_SL(2, false);
+    }
+#undef GK_SL
+}
+
+__global__ void k_or_status(DevTime* tm, int bits) { tm->status |= bits; }
+
+// The fused stage with the learned correction (TMA rows only; CTAs of 64 or
+// 128 threads).  A tensor map that cannot be encoded sets STATUS_NO_MAP:
+// the step does not run silently without its correction.
+void launch_stage2d_learn(const Ctx& c, const double* uc, const double* u0, double* out, int kind,
+                          double c1, double c2, double c3, const float* model,
+                          const gk::FluxGate& gate, unsigned* fired, cudaStream_t s) {
+    const int nt = c.stage_threads == 64 ? 64 : 128;
+    CUtensorMap mc, m0;
+    if (!gk::encode_rows_map(&mc, uc, c.g, nt) || !gk::encode_rows_map(&m0, u0 ? u0 : uc, c.g, nt)) {
+        std::fprintf(stderr, "gaukuk: tensor map encoding failed for the learned stage\n");
+        k_or_status<<<1, 1, 0, s>>>(c.tm, gk::STATUS_NO_MAP);
+        return;
+    }
+    if (nt == 64) launch_stage2d_learn_nt<64>(c, mc, m0, out, kind, c1, c2, c3, model, gate, fired, s);
+    else launch_stage2d_learn_nt<128>(c, mc, m0, out, kind, c1, c2, c3, model, gate, fired, s);
 }
 
 void launch_stage2d(const Ctx& c, const double* uc, const double* u0, double* out, int kind,

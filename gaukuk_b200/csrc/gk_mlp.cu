@@ -22,95 +22,20 @@
 
 #include "gaukuk_cuda.h"
 #include "gk_internal.h"
+#include "gk_learn.cuh"
 
 namespace {
 
-constexpr int NI = 16, NH = 64, NO = 4;
-constexpr int W1O = 0, B1O = W1O + NH * NI, W2O = B1O + NH, B2O = W2O + NH * NH;
-constexpr int W3O = B2O + NH, B3O = W3O + NO * NH, NPARAM = B3O + NO;  // 5508
-constexpr int XMO = NPARAM, XSO = XMO + NI, YMO = XSO + NI, YSO = YMO + NO;
-constexpr int NMODEL = YSO + NO;  // parameters + normalisation = 5548 floats
-
-constexpr float kGeluA = 0.7978845608028654f;  // sqrt(2/pi)
-constexpr float kGeluB = 0.044715f;
-
-__device__ __forceinline__ float gelu(float x, float* dgelu) {
-    const float u = kGeluA * (x + kGeluB * x * x * x);
-    const float th = tanhf(u);
-    if (dgelu) *dgelu = 0.5f * (1.f + th) + 0.5f * x * (1.f - th * th) * kGeluA * (1.f + 3.f * kGeluB * x * x);
-    return 0.5f * x * (1.f + th);
-}
-
-__device__ __forceinline__ unsigned pack(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-    return (unsigned)__bfloat16_as_ushort(lo) | ((unsigned)__bfloat16_as_ushort(hi) << 16);
-}
-
-__device__ __forceinline__ void mma(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-        "{%8,%9}, {%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// A(m, k) = S[m0 + m][k0 + k], S row-major with leading dimension ld.
-__device__ __forceinline__ void load_a(unsigned (&a)[4], const __nv_bfloat16* S, int ld, int m0, int k0) {
-    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
-    a[0] = pack(S[(m0 + g) * ld + k0 + 2 * t], S[(m0 + g) * ld + k0 + 2 * t + 1]);
-    a[1] = pack(S[(m0 + g + 8) * ld + k0 + 2 * t], S[(m0 + g + 8) * ld + k0 + 2 * t + 1]);
-    a[2] = pack(S[(m0 + g) * ld + k0 + 2 * t + 8], S[(m0 + g) * ld + k0 + 2 * t + 9]);
-    a[3] = pack(S[(m0 + g + 8) * ld + k0 + 2 * t + 8], S[(m0 + g + 8) * ld + k0 + 2 * t + 9]);
-}
-// A(m, k) = S[k0 + k][m0 + m] (the transpose of a row-major S).
-__device__ __forceinline__ void load_at(unsigned (&a)[4], const __nv_bfloat16* S, int ld, int m0, int k0) {
-    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
-    a[0] = pack(S[(k0 + 2 * t) * ld + m0 + g], S[(k0 + 2 * t + 1) * ld + m0 + g]);
-    a[1] = pack(S[(k0 + 2 * t) * ld + m0 + g + 8], S[(k0 + 2 * t + 1) * ld + m0 + g + 8]);
-    a[2] = pack(S[(k0 + 2 * t + 8) * ld + m0 + g], S[(k0 + 2 * t + 9) * ld + m0 + g]);
-    a[3] = pack(S[(k0 + 2 * t + 8) * ld + m0 + g + 8], S[(k0 + 2 * t + 9) * ld + m0 + g + 8]);
-}
-// B(k, n) = S[n0 + n][k0 + k] (S row-major [n][k], e.g. weights W[out][in]).
-__device__ __forceinline__ void load_b_nk(unsigned (&b)[2], const __nv_bfloat16* S, int ld, int n0, int k0) {
-    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
-    b[0] = pack(S[(n0 + g) * ld + k0 + 2 * t], S[(n0 + g) * ld + k0 + 2 * t + 1]);
-    b[1] = pack(S[(n0 + g) * ld + k0 + 2 * t + 8], S[(n0 + g) * ld + k0 + 2 * t + 9]);
-}
-// B(k, n) = S[k0 + k][n0 + n] (S row-major [k][n]).
-__device__ __forceinline__ void load_b_kn(unsigned (&b)[2], const __nv_bfloat16* S, int ld, int n0, int k0) {
-    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
-    b[0] = pack(S[(k0 + 2 * t) * ld + n0 + g], S[(k0 + 2 * t + 1) * ld + n0 + g]);
-    b[1] = pack(S[(k0 + 2 * t + 8) * ld + n0 + g], S[(k0 + 2 * t + 9) * ld + n0 + g]);
-}
-
-// Weights in shared memory as BF16 (W3 padded to 16 output rows with zeros),
-// biases as FP32.
-struct MlpWeights {
-    __nv_bfloat16 w1[NH * NI];
-    __nv_bfloat16 w2[NH * NH];
-    __nv_bfloat16 w3[16 * NH];
-    float b1[NH], b2[NH], b3[8];
-};
-
-__device__ void load_weights(MlpWeights& s, const float* __restrict__ p) {
-    for (int i = threadIdx.x; i < NH * NI; i += blockDim.x) s.w1[i] = __float2bfloat16_rn(p[W1O + i]);
-    for (int i = threadIdx.x; i < NH * NH; i += blockDim.x) s.w2[i] = __float2bfloat16_rn(p[W2O + i]);
-    for (int i = threadIdx.x; i < 16 * NH; i += blockDim.x)
-        s.w3[i] = i < NO * NH ? __float2bfloat16_rn(p[W3O + i]) : __float2bfloat16_rn(0.f);
-    for (int i = threadIdx.x; i < NH; i += blockDim.x) {
-        s.b1[i] = p[B1O + i];
-        s.b2[i] = p[B2O + i];
-    }
-    for (int i = threadIdx.x; i < 8; i += blockDim.x) s.b3[i] = i < NO ? p[B3O + i] : 0.f;
-}
+using namespace gklearn;
 
 // Per-warp activations of one 16-sample tile (BF16, row = sample).
 struct TileAct {
-    __nv_bfloat16 x[16 * NI];
-    __nv_bfloat16 h1[16 * NH];
-    __nv_bfloat16 h2[16 * NH];
-    __nv_bfloat16 dz1[16 * NH];
-    __nv_bfloat16 dz2[16 * NH];
-    __nv_bfloat16 dy[16 * 16];
+    alignas(16) __nv_bfloat16 x[16 * NI];
+    alignas(16) __nv_bfloat16 h1[16 * NH];
+    alignas(16) __nv_bfloat16 h2[16 * NH];
+    alignas(16) __nv_bfloat16 dz1[16 * NH];
+    alignas(16) __nv_bfloat16 dz2[16 * NH];
+    alignas(16) __nv_bfloat16 dy[16 * 16];
 };
 
 // Forward pass of one tile whose inputs are in act.x.  Keeps Z1, Z2 (FP32 C
@@ -434,41 +359,6 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ p
 }
 
 // ------------------------------------------------------------ inference
-// van Leer slope of the PLM reconstruction, (2ab)/(a+b) for ab > 0 else 0.
-__device__ __forceinline__ double vl_slope(double a, double b) {
-    const double m = a * b;
-    return m <= 0.0 ? 0.0 : (2.0 * m) / (a + b);
-}
-
-// PLM face states of the stencil (cells -2, -1 | 0, +1) as conserved
-// variables (mass, normal momentum, tangential momentum, energy) and the fast
-// signal speeds |vn| + c on each side.
-__device__ __forceinline__ void face_states(const double (&r)[4], const double (&vn)[4],
-                                            const double (&vt)[4], const double (&p)[4], double gamma,
-                                            double gm1Rec, double (&ul)[4], double (&ur)[4],
-                                            double& sl, double& sr) {
-    const double* q[4] = {r, vn, vt, p};
-    double wl[4], wr[4];
-    for (int v = 0; v < 4; ++v) {
-        wl[v] = q[v][1] + 0.5 * vl_slope(q[v][1] - q[v][0], q[v][2] - q[v][1]);
-        wr[v] = q[v][2] - 0.5 * vl_slope(q[v][2] - q[v][1], q[v][3] - q[v][2]);
-    }
-    const double* w[2] = {wl, wr};
-    double* u[2] = {ul, ur};
-    double s[2];
-    for (int side = 0; side < 2; ++side) {
-        const double d = fmax(w[side][0], 1e-300), a = w[side][1], b = w[side][2];
-        const double pp = fmax(w[side][3], 0.0);
-        u[side][0] = d;
-        u[side][1] = d * a;
-        u[side][2] = d * b;
-        u[side][3] = pp * gm1Rec + 0.5 * d * (a * a + b * b);
-        s[side] = fabs(a) + sqrt(gamma * pp / d);
-    }
-    sl = s[0];
-    sr = s[1];
-}
-
 // Adds the learned correction to the face fluxes of one direction of a 2D
 // generic-path stage (F: FP64 face fluxes, W: FP64 primitives).  One warp
 // per 16 faces.  The plain HLLC flux is kept where the detector fires (a
@@ -476,15 +366,13 @@ __device__ __forceinline__ void face_states(const double (&r)[4], const double (
 // correction that would move more than pos_frac of an adjacent cell's mass
 // or internal energy through the face in one step) and in smooth flow (the
 // stencil's total variation below tv_min); each component is clipped to
-// diss_frac times the face's HLL dissipation (gk::FluxGate).
+// diss_frac times the face's HLL dissipation (gk::FluxGate).  The fused 2D
+// stage (gk_kernels.cuh) applies the same correction with the same
+// functions (gk_learn.cuh), face by face.
 struct InferShared {
     MlpWeights w;
-    TileAct act[4];
-    float norm[2 * NI + 2 * NO];
-    // per face: rho_ref*c, rho_ref*c^2, rho_ref*c^3, gate (0 shock, 1 correct,
-    // 2 smooth), the smaller density and internal energy of the two cells
-    // next to the face, the clip bounds of the 4 outputs (negative: none)
-    float scale[4][16][10];
+    alignas(16) __nv_bfloat16 x[4][32 * NI];  // a warp's two tiles
+    FaceScale fs[4][32];
 };
 
 __global__ void __launch_bounds__(128) k_flux_correct(const float* __restrict__ model,
@@ -497,10 +385,9 @@ __global__ void __launch_bounds__(128) k_flux_correct(const float* __restrict__ 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     InferShared& sh = *reinterpret_cast<InferShared*>(smem_raw);
     load_weights(sh.w, model);
-    for (int i = threadIdx.x; i < 2 * NI + 2 * NO; i += blockDim.x) sh.norm[i] = model[XMO + i];
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gq = lane >> 2, tq = lane & 3;
-    TileAct& act = sh.act[warp];
+    __nv_bfloat16* const x = sh.x[warp];
     const int nfx = dir == 0 ? g.nx + 1 : g.nx;       // faces per row
     const int nfy = dir == 0 ? g.ny : g.ny + 1;       // rows of faces
     const long long nfaces = (long long)nfx * nfy;
@@ -508,12 +395,12 @@ __global__ void __launch_bounds__(128) k_flux_correct(const float* __restrict__ 
     const double dtdx = tm->dt * (dir == 0 ? g.dxRec : g.dyRec);
     const int sn = dir == 0 ? gk::P_VX : gk::P_VY, st = dir == 0 ? gk::P_VY : gk::P_VX;
     const int mn = dir == 0 ? gk::S_MTX : gk::S_MTY, mt = dir == 0 ? gk::S_MTY : gk::S_MTX;
-    for (long long tile = blockIdx.x * 4 + warp; tile < ntiles; tile += gridDim.x * 4) {
-        // features: lane < 16 builds face tile*16 + lane
-        if (lane < 16) {
-            const long long f = tile * 16 + lane;
-            float feat[NI];
-            float sc[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    // a warp takes two tiles at a time: lane L builds face 32 * pair + L
+    const long long npairs = (ntiles + 1) / 2;
+    for (long long pair = blockIdx.x * 4 + warp; pair < npairs; pair += gridDim.x * 4) {
+        {
+            const long long f = pair * 32 + lane;
+            FaceScale& fs = sh.fs[warp][lane];
             if (f < nfaces) {
                 const int fi = (int)(f % nfx), fj = (int)(f / nfx);
                 const int i = g.ib + fi, j = g.jb + fj;  // face between cells (i-1|i) or (j-1|j)
@@ -526,80 +413,49 @@ __global__ void __launch_bounds__(128) k_flux_correct(const float* __restrict__ 
                     vt[c] = W[st * g.vstride + q];
                     p[c] = W[gk::P_PRE * g.vstride + q];
                 }
-                const double rr = 0.25 * (r[0] + r[1] + r[2] + r[3]);
-                const double pr = 0.25 * (p[0] + p[1] + p[2] + p[3]);
-                const double cr = sqrt(ph.gamma * pr / rr);
-                for (int c = 0; c < 4; ++c) {
-                    feat[4 * c + 0] = (float)(r[c] / rr - 1.0);
-                    feat[4 * c + 1] = (float)(vn[c] / cr);
-                    feat[4 * c + 2] = (float)(vt[c] / cr);
-                    feat[4 * c + 3] = (float)(p[c] / pr - 1.0);
-                }
-                float tv = 0.f;  // total variation of the stencil's features
-                for (int e = 4; e < NI; ++e) tv += fabsf(feat[e] - feat[e - 4]);
-                double pmax = p[0], pmin = p[0];
-                for (int c = 1; c < 4; ++c) { pmax = fmax(pmax, p[c]); pmin = fmin(pmin, p[c]); }
-                const bool shock = pmax > (1.0 + gate.shock_jump) * pmin;
-                sc[0] = (float)(rr * cr);
-                sc[1] = (float)(rr * cr * cr);
-                sc[2] = (float)(rr * cr * cr * cr);
-                sc[3] = shock ? 0.f : (tv >= gate.tv_min ? 1.f : 2.f);
-                sc[4] = (float)fmin(r[1], r[2]);
-                sc[5] = (float)(fmin(p[1], p[2]) * ph.gm1Rec);
-                if (gate.diss_frac >= 0.f) {
-                    // (1/2) max(s) |U_R - U_L| of the van Leer PLM face states
-                    double ul[4], ur[4], sl, sr;
-                    face_states(r, vn, vt, p, ph.gamma, ph.gm1Rec, ul, ur, sl, sr);
-                    const double sm = 0.5 * fmax(sl, sr) * gate.diss_frac;
-                    for (int o = 0; o < 4; ++o) sc[6 + o] = (float)(sm * fabs(ur[o] - ul[o]));
-                } else {
-                    for (int o = 0; o < 4; ++o) sc[6 + o] = -1.f;
-                }
+                face_inputs(r, vn, vt, p, ph.gamma, ph.gm1Rec, gate, sh.w.norm, x + lane * NI, fs);
             } else {
-                for (int e = 0; e < NI; ++e) feat[e] = 0.f;
+                for (int e = 0; e < NI; ++e) x[lane * NI + e] = __float2bfloat16_rn(0.f);
+                fs.gate = 2.f;
             }
-            for (int e = 0; e < NI; ++e)
-                act.x[lane * NI + e] = __float2bfloat16_rn((feat[e] - sh.norm[e]) / sh.norm[NI + e]);
-            for (int e = 0; e < 10; ++e) sh.scale[warp][lane][e] = sc[e];
         }
+        // tiles whose faces all keep plain HLLC (past the end, or smooth) skip the network
+        const unsigned need = __ballot_sync(0xffffffffu, sh.fs[warp][lane].gate != 2.f);
         __syncwarp();
-        float z1[8][4], z2[8][4], y[4];
-        forward_tile(sh.w, act, z1, z2, y);
-        // lane (gq, tq < 2) holds outputs 2tq, 2tq+1 of faces gq and gq+8;
-        // its partner lane ^ 1 holds the face's other two outputs
-        for (int half = 0; half < 2; ++half) {
-            const int fl = gq + 8 * half;
-            const long long f = tile * 16 + fl;
-            const float* sc = sh.scale[warp][fl];
-            const bool mine = tq < 2 && f < nfaces && sc[3] != 2.f;
-            double corr[2] = {0.0, 0.0};
-            int bad = 0;
-            if (mine) {
+        if (!need) continue;
+        float y2[2][4];
+        forward_tiles<2>(sh.w, x, y2);
+        for (int half16 = 0; half16 < 2; ++half16) {
+            if (!((need >> (16 * half16)) & 0xffffu)) continue;
+            const float (&y)[4] = y2[half16];
+            // lane (gq, tq < 2) holds outputs 2tq, 2tq+1 of faces gq and gq+8;
+            // its partner lane ^ 1 holds the face's other two outputs
+            for (int half = 0; half < 2; ++half) {
+                const int fl = 16 * half16 + gq + 8 * half;
+                const long long f = pair * 32 + fl;
+                const FaceScale& fs = sh.fs[warp][fl];
+                const bool mine = tq < 2 && f < nfaces && fs.gate != 2.f;
+                double corr[2] = {0.0, 0.0};
+                if (mine)
+                    for (int o2 = 0; o2 < 2; ++o2) corr[o2] = face_correction(y[2 * half + o2], 2 * tq + o2, fs, sh.w.norm);
+                // lane tq = 0 holds mass (output 0), its partner energy (output 3);
+                // every lane takes part in both exchanges
+                const double p0 = __shfl_xor_sync(0xffffffffu, corr[0], 1);
+                const double p1 = __shfl_xor_sync(0xffffffffu, corr[1], 1);
+                const double c0 = tq == 0 ? corr[0] : p0;
+                const double c3 = tq == 0 ? p1 : corr[1];
+                const bool bad = mine && face_vetoed(c0, c3, dtdx, fs, gate);
+                // one atomic per warp and half-tile for the faces left to plain HLLC
+                const unsigned nbad = __ballot_sync(0xffffffffu, bad && tq == 0);
+                if (lane == 0 && fired && nbad) atomicAdd(fired, (unsigned)__popc(nbad));
+                if (!mine || bad) continue;
+                const int fi = (int)(f % nfx), fj = (int)(f / nfx);
+                const long long fc = (long long)(g.kb - g.kofs) * g.fkstride + (long long)(g.jb + fj) * g.fpitch + g.ib + fi;
                 for (int o2 = 0; o2 < 2; ++o2) {
                     const int o = 2 * tq + o2;
-                    // clip to the training range (+-4 deviations) before de-standardising
-                    const float yc = fminf(fmaxf(y[2 * half + o2], -4.f), 4.f);
-                    const float ys = yc * sh.norm[2 * NI + NO + o] + sh.norm[2 * NI + o];
-                    corr[o2] = (double)ys * (double)(o == 0 ? sc[0] : (o == 3 ? sc[2] : sc[1]));
-                    const double bound = sc[6 + o];
-                    if (bound >= 0.0) corr[o2] = fmin(fmax(corr[o2], -bound), bound);
+                    const int slot = o == 0 ? gk::S_DEN : (o == 1 ? mn : (o == 2 ? mt : gk::S_ENG));
+                    F[slot * g.fvstride + fc] += corr[o2];
                 }
-                // positivity: mass (output 0) and energy (output 3) moved in one step
-                if (tq == 0) bad = fabs(corr[0]) * dtdx > gate.pos_frac * sc[4];
-                else bad = fabs(corr[1]) * dtdx > gate.pos_frac * sc[5];
-                bad |= sc[3] == 0.f;
-            }
-            bad |= __shfl_xor_sync(0xffffffffu, bad, 1);
-            // one atomic per warp and half-tile for the faces left to plain HLLC
-            const unsigned nbad = __ballot_sync(0xffffffffu, mine && bad && tq == 0);
-            if (lane == 0 && fired && nbad) atomicAdd(fired, (unsigned)__popc(nbad));
-            if (!mine || bad) continue;
-            const int fi = (int)(f % nfx), fj = (int)(f / nfx);
-            const long long fc = (long long)(g.kb - g.kofs) * g.fkstride + (long long)(g.jb + fj) * g.fpitch + g.ib + fi;
-            for (int o2 = 0; o2 < 2; ++o2) {
-                const int o = 2 * tq + o2;
-                const int slot = o == 0 ? gk::S_DEN : (o == 1 ? mn : (o == 2 ? mt : gk::S_ENG));
-                F[slot * g.fvstride + fc] += corr[o2];
             }
         }
         __syncwarp();
@@ -765,8 +621,8 @@ void launch_flux_correct(const float* model, const double* W, double* F, const G
         cudaFuncSetAttribute(k_flux_correct, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(InferShared));
     const long long nf = dir == 0 ? (long long)(g.nx + 1) * g.ny : (long long)g.nx * (g.ny + 1);
-    const long long tiles = (nf + 15) / 16;
-    const int ctas = (int)((tiles + 3) / 4 < 148 * 8 ? (tiles + 3) / 4 : 148 * 8);
+    const long long pairs = ((nf + 15) / 16 + 1) / 2;
+    const int ctas = (int)((pairs + 3) / 4 < 148 * 8 ? (pairs + 3) / 4 : 148 * 8);
     k_flux_correct<<<ctas, 128, sizeof(InferShared), s>>>(model, W, F, g, ph, tm, dir, gate,
                                                            fired);
 }

@@ -390,12 +390,15 @@ def r2(blob: np.ndarray, X: np.ndarray, Y: np.ndarray, device: int = 0) -> List[
 
 
 def install(sim, blob: Optional[np.ndarray], shock_jump: float = 0.5, pos_frac: float = 0.02,
-            tv_min: float = TV_GATE, diss_frac: float = DISS_FRAC):
-    """Installs (or, with None, removes) the correction on a 2D Sim."""
+            tv_min: float = TV_GATE, diss_frac: float = DISS_FRAC, fused: bool = True):
+    """Installs (or, with None, removes) the correction on a 2D Sim.  fused:
+    the network runs inside the fused 2D stage where the run takes it
+    (gk_set_flux_model_fused), else as a pass on the generic path."""
     if blob is None:
         _lib.check(sim._L.gk_set_flux_model(sim.h, None, 0, 0.0, 0.0, 0.0, 0.0), sim.h)
         return
     b = np.ascontiguousarray(blob, dtype=np.float32)
+    _lib.check(sim._L.gk_set_flux_model_fused(sim.h, 1 if fused else 0), sim.h)
     _lib.check(sim._L.gk_set_flux_model(sim.h, b.ctypes.data_as(ctypes.c_void_p), b.size,
                                         float(shock_jump), float(pos_frac), float(tv_min),
                                         float(diss_frac)), sim.h)

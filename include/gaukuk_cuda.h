@@ -306,6 +306,14 @@ int gk_mlp_forward(gk_mlp* m, const void* X, long long n, float* Y);
  * disables the clip. */
 int gk_set_flux_model(gk_handle* h, const float* model_host, int nmodel, float shock_jump,
                       float pos_frac, float tv_min, float diss_frac);
+/* Where the correction runs (pattern 4's inference; no counterpart in the
+ * reference).  fused = 1 (the default): inside the fused 2D stage, at the
+ * face where its HLLC flux is formed (hllc.cpp:90-95 within
+ * cal_flux.cpp:89-121), for runs the fused stage takes (2D RK2/RK3, vz = 0,
+ * TMA rows); fused = 0: on the generic path, as a pass over the face fluxes
+ * of each direction.  In parity mode the two give the same bits; the
+ * detector counts the same faces. */
+int gk_set_flux_model_fused(gk_handle* h, int fused);
 /* Faces where the detector has fired since the model was installed. */
 int gk_flux_model_fired(gk_handle* h, unsigned* fired);
 

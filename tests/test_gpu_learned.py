@@ -165,15 +165,16 @@ def test_zero_dissipation_bound_is_plain_hllc():
     assert np.array_equal(active(p, a.download()), active(p, b.download()))
 
 
-def test_zero_model_is_plain_hllc_bitwise():
+@pytest.mark.parametrize("fused", [True, False])
+def test_zero_model_is_plain_hllc_bitwise(fused):
     from gaukuk_b200.sim import Sim
     p, c = problems.kh(96, ny=80, seed=1)
     blob = np.zeros(learned.NMODEL, dtype=np.float32)
     blob[learned.NPARAM + 16:learned.NPARAM + 32] = 1.0  # input deviations
     blob[learned.NPARAM + 36:] = 1.0                    # output deviations
     a, b = Sim(p, c, mode="parity"), Sim(p, c, mode="parity")
-    learned.install(b, blob)
-    assert b.path == "generic"
+    learned.install(b, blob, fused=fused)
+    assert b.path == ("fused2d" if fused else "generic")
     a.run_steps(12)
     b.run_steps(12)
     assert a.dt_log() == b.dt_log()
@@ -241,3 +242,105 @@ def test_trained_correction_against_plain_on_a_held_out_case():
     assert np.isfinite(lrn["l1_at_64"]).all()
     assert lrn["mass_drift"] < 1e-13
     assert lrn["l1_at_64"][-1] > plain2["l1_at_64"][-1]
+
+
+# Gates for the model below (outputs scaled by 0.05): at the initial states
+# the positivity ratio max(|c_mass| dt/dx / rho_min, |c_energy| dt/dx / e_min)
+# is about 0.0065 in the dense layer and 0.0093 outside it for KH, 0.008 to
+# 0.0117 for RT, and the stencil variation's median is about 0.0012, so each
+# gate splits the faces: corrected, vetoed, smooth (and clipped, RT's
+# pressure jumps above 0.1 % vetoed as shocks).
+GATE_KH = dict(shock_jump=0.5, pos_frac=0.008, tv_min=0.0012, diss_frac=-1.0)
+GATE_CLIP = dict(shock_jump=0.5, pos_frac=0.008, tv_min=0.0012, diss_frac=0.5)
+GATE_RT = dict(shock_jump=0.001, pos_frac=0.01, tv_min=0.0012, diss_frac=0.5)
+
+
+def _fused_case(name):
+    """(params, state, tiling or None, gate, vetoes expected) of the
+    fused-correction cases."""
+    from gaukuk_b200.config import BC_PERIODIC, BC_REFLECTIVE
+    if name == "kh_rk2":
+        p, c = problems.kh(96, ny=80, seed=12)
+        return p, c, None, GATE_KH, True
+    if name == "kh_rk3_tiles128_clip":
+        p, c = problems.kh(150, ny=70, seed=13)
+        return dataclasses.replace(p, integrator=3), c, (128, 4), GATE_CLIP, False
+    if name == "rt_rk3_gravity_tiles64":
+        p, c = problems.rt(64, 192)
+        assert p.integrator == 3 and p.bc[2] == BC_REFLECTIVE and p.bc[0] == BC_PERIODIC
+        return p, c, (64, 5), GATE_RT, True
+    if name == "kh_first_order":
+        p, c = problems.kh(64, seed=14)
+        return dataclasses.replace(p, rc_order=1), c, None, GATE_KH, True
+    raise KeyError(name)
+
+
+def _model():
+    X, Y = _data(256)
+    blob = learned.init_model(X, Y, seed=21)
+    blob[learned.NPARAM + 36:] *= 0.05
+    return blob
+
+
+def _pair(name, mode, blob):
+    from gaukuk_b200.sim import Sim
+    p, c, tiling, gate, _ = _fused_case(name)
+    a, b = Sim(p, c, mode=mode), Sim(p, c, mode=mode)
+    for s in (a, b):
+        if tiling:
+            s.set_tiling(*tiling)
+    learned.install(a, blob, fused=True, **gate)
+    learned.install(b, blob, fused=False, **gate)
+    assert a.path == "fused2d" and b.path == "generic"
+    return p, c, a, b
+
+
+CASES = ["kh_rk2", "kh_rk3_tiles128_clip", "rt_rk3_gravity_tiles64", "kh_first_order"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fused_correction_is_the_correction_pass_bitwise(case):
+    """Parity mode: the fused 2D stage with the network at every face (the
+    default) gives the generic path's correction pass bit for bit -- state,
+    dt sequence and detector count -- across strip and segment boundaries
+    (small tiles, both CTA widths), RK2 and RK3, gravity, reflective sides
+    and first order.  The gate settings make every branch occur: corrected,
+    clipped, vetoed (shock and positivity) and smooth faces."""
+    from gaukuk_b200.sim import Sim
+    p, c, a, b = _pair(case, "parity", _model())
+    a.run_steps(8)
+    b.run_steps(8)
+    assert a.dt_log() == b.dt_log()
+    assert np.array_equal(active(p, a.download()), active(p, b.download()))
+    na, nb = learned.detector_count(a), learned.detector_count(b)
+    assert na == nb
+    plain = Sim(p, c, mode="parity")
+    plain.run_steps(8)
+    faces = 8 * (3 if p.integrator == 3 else 2) * (p.ny * (p.nx + 1) + p.nx * (p.ny + 1))
+    print(f"\n{case}: {na} of {faces} faces vetoed")
+    assert na < faces
+    assert na > 0 or not _fused_case(case)[4]
+    assert not np.array_equal(active(p, a.download()), active(p, plain.download()))
+    for s in (a, b, plain):
+        s.close()
+
+
+@pytest.mark.parametrize("case", ["kh_rk2", "rt_rk3_gravity_tiles64"])
+def test_fused_correction_close_to_the_correction_pass_in_fast_mode(case):
+    """Fast mode: the fused stage and the generic path round their fluxes
+    differently in the last bits; with the correction the two stay within
+    the fast-mode tolerance (1e-12 relative; momentum components against the
+    momentum's magnitude, as RT's x-momentum starts at exactly zero) after 8
+    steps, and the detector counts agree."""
+    p, c, a, b = _pair(case, "fast", _model())
+    a.run_steps(8)
+    b.run_steps(8)
+    ga, gb = active(p, a.download()), active(p, b.download())
+    mscale = max(float(np.max(np.abs(gb[1]))), float(np.max(np.abs(gb[2]))))
+    scale = {0: np.max(np.abs(gb[0])), 1: mscale, 2: mscale, 4: np.max(np.abs(gb[4]))}
+    err = max(float(np.max(np.abs(ga[v] - gb[v])) / scale[v]) for v in (0, 1, 2, 4))
+    dev = max(abs(x - y) / y for x, y in zip(a.dt_log(), b.dt_log()))
+    print(f"\n{case} fast: fused vs pass rel Linf {err:.2e}, dt {dev:.2e}, vetoed "
+          f"{learned.detector_count(a)} / {learned.detector_count(b)}")
+    assert err <= 1e-12 and dev <= 1e-12
+    assert abs(learned.detector_count(a) - learned.detector_count(b)) <= 2
