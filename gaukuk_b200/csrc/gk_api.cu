@@ -342,6 +342,29 @@ int stage_threads_for(const gk::Geom& g) {
     return (long long)g.ny * strips / (148 * 4) < 8 ? 64 : 128;
 }
 
+// The stage with the learned correction holds 256 threads per SM (its
+// registers and shared memory), and a tile's time is about its rows plus
+// half a row (the segment's first y faces).  Rows per segment: the r in
+// [2, 24] that minimises waves x (r + 1/2).  KH 256^2 (CTAs of 64): 3 rows,
+// one wave of 430 CTAs (the plain rule's 2 rows made two waves); 1024^2
+// (CTAs of 128): 16 rows, two waves of 288.
+int learn_stage_rows(const gk::Geom& g, int threads) {
+    const long long nt = threads == 64 ? 64 : 128;
+    const long long strips = (g.nx + nt - 5) / (nt - 4);
+    const long long slots = 148LL * (256 / nt);
+    int best = 2;
+    double best_cost = 1e300;
+    for (int r = 2; r <= 24; ++r) {
+        const long long tiles = strips * ((g.ny + r - 1) / r);
+        const double cost = (double)((tiles + slots - 1) / slots) * (r + 0.5);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = r;
+        }
+    }
+    return best;
+}
+
 int stage_rows(const gk::Geom& g, int threads, bool parity) {
     const int forced = env_int("GK_STAGE_ROWS", 0);
     if (forced > 0) return forced;
@@ -772,8 +795,10 @@ int gk_upload_cons(gk_handle* h, const double* cons) {
     if (!h->tiling_set) {
         h->ctx.stage_threads = stage_threads_for(g);
         h->ctx.h2d_rows = stage_rows(g, h->ctx.stage_threads, h->ks == &kParity);
+        h->ctx.learn_rows = learn_stage_rows(g, h->ctx.stage_threads);
     } else {
         h->ctx.h2d_rows = h->tiling_rows;
+        h->ctx.learn_rows = 0;
     }
     if (h->path != 1) {
         int rc = alloc_generic(h);
@@ -1176,6 +1201,7 @@ extern "C" int gk_set_tiling(gk_handle* h, int threads, int rows) {
     if (rows < 1) return fail(h, GK_ERR_INVALID, "rows per segment must be positive");
     h->ctx.stage_threads = threads;
     h->ctx.h2d_rows = rows;
+    h->ctx.learn_rows = 0;  // forced rows serve both stages
     h->tiling_set = true;
     h->tiling_rows = rows;
     if (h->gexec) {  // the graph holds the old launch shapes

@@ -120,6 +120,8 @@ struct Ctx {
     int h2d_rows;       // fused 2D kernel: rows per CTA segment
     int use_tma;        // fused 2D kernel: rows staged in shared memory by TMA
     int stage_threads;  // fused 2D kernel (TMA): threads per CTA, 64 / 128 / 256
+    int learn_rows;     // the fused stage with the learned correction: rows per
+                        // segment (0: h2d_rows)
 };
 
 // One instance of an ensemble, as the persistent stage kernel reads it from

@@ -1016,6 +1016,7 @@ struct StageShared {
 struct LearnWarp {
     alignas(16) __nv_bfloat16 x[64 * gklearn::NI];  // standardised inputs per slot
     float y[64][4];                                 // standardised outputs per slot
+    gklearn::FaceScale fs[64];                      // detector and scales per slot
 };
 struct LearnArgs {
     const gklearn::MlpWeights* w;  // shared memory
@@ -1038,73 +1039,94 @@ __device__ __forceinline__ Stencil4 stencil_y(const W4& a, const W4& b, const W4
                     {a.p, b.p, c.p, d.p}};
 }
 
-// Corrects this lane's x face (when hasx) and y face (when hasy); every lane
-// of the warp takes part.  A vetoed face keeps its flux; *nfired counts the
-// vetoed faces this lane owns (countx / county).
-__device__ __forceinline__ void learn_faces(const LearnArgs& la, bool hasx, const Stencil4& sx,
-                                            bool countx, Flux5& fx, double dtdx, bool hasy,
-                                            const Stencil4& sy, bool county, Flux5& fy,
-                                            double dtdy, const Phys& ph, unsigned& nfired) {
+// Corrects this lane's x face (side 0, when hasx) and y face (side 1, when
+// hasy); every lane of the warp takes part.  stencil(side) gives the face's
+// stencil.  The two sides run as rolled loops, so each piece of the code is
+// in the kernel once per call site.  A vetoed face keeps its flux; nfired
+// counts the vetoed faces this lane owns (countx / county).
+template <class StencilFn>
+__device__ __forceinline__ void learn_faces(const LearnArgs& la, const StencilFn& stencil,
+                                            bool hasx, bool countx, Flux5& fx, double dtdx,
+                                            bool hasy, bool county, Flux5& fy, double dtdy,
+                                            const Phys& ph, unsigned& nfired) {
     using namespace gklearn;
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     LearnWarp& lw = la.warps[threadIdx.x >> 5];
     const MlpWeights& w = *la.w;
-    FaceScale fsx, fsy;
-    fsx.gate = fsy.gate = 2.f;
-    if (hasx) {
-        face_inputs(sx.r, sx.vn, sx.vt, sx.p, ph.gamma, ph.gm1Rec, la.gate, w.norm, lw.x + lane * NI, fsx);
-    } else {
+    unsigned needx = 0, needy = 0;
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+        const int slot = 32 * side + lane;
+        FaceScale& fs = lw.fs[slot];
+        fs.gate = 2.f;
+        if (side ? hasy : hasx) {
+            const Stencil4 st = stencil(side);
+            face_inputs(st.r, st.vn, st.vt, st.p, ph.gamma, ph.gm1Rec, la.gate, w.norm,
+                        lw.x + slot * NI, fs);
+        } else {
 #pragma unroll
-        for (int e = 0; e < NI; ++e) lw.x[lane * NI + e] = __float2bfloat16_rn(0.f);
-    }
-    if (hasy) {
-        face_inputs(sy.r, sy.vn, sy.vt, sy.p, ph.gamma, ph.gm1Rec, la.gate, w.norm, lw.x + (32 + lane) * NI, fsy);
-    } else {
-#pragma unroll
-        for (int e = 0; e < NI; ++e) lw.x[(32 + lane) * NI + e] = __float2bfloat16_rn(0.f);
-    }
-    // the x tiles and the y tiles each run only where a face needs the
-    // network (none keep plain HLLC because they are absent or smooth)
-    const unsigned needx = __ballot_sync(0xffffffffu, fsx.gate != 2.f);
-    const unsigned needy = __ballot_sync(0xffffffffu, fsy.gate != 2.f);
-    __syncwarp();
-    auto put = [&](int tile, const float (&y)[4]) {
-        if (t < 2) {
-            lw.y[tile * 16 + g][2 * t] = y[0];
-            lw.y[tile * 16 + g][2 * t + 1] = y[1];
-            lw.y[tile * 16 + g + 8][2 * t] = y[2];
-            lw.y[tile * 16 + g + 8][2 * t + 1] = y[3];
+            for (int e = 0; e < NI; ++e) lw.x[slot * NI + e] = __float2bfloat16_rn(0.f);
         }
-    };
-    if (needx) {
-        float y[2][4];
-        forward_tiles<2>(w, lw.x, y);
-        put(0, y[0]);
-        put(1, y[1]);
-    }
-    if (needy) {
-        float y[2][4];
-        forward_tiles<2>(w, lw.x + 32 * NI, y);
-        put(2, y[0]);
-        put(3, y[1]);
+        // the tiles of a side run only where a face needs the network (none
+        // keep plain HLLC because they are absent or smooth)
+        const unsigned need = __ballot_sync(0xffffffffu, fs.gate != 2.f);
+        if (side) needy = need;
+        else needx = need;
     }
     __syncwarp();
-    auto apply = [&](int slot, const FaceScale& fs, bool count, Flux5& f, double dtn) {
-        if (fs.gate == 2.f) return;
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+        if (!(side ? needy : needx)) continue;
+        float y[2][4];
+        forward_tiles<2>(w, lw.x + side * 32 * NI, y);
+        if (t < 2) {
+#pragma unroll
+            for (int m = 0; m < 2; ++m) {
+                const int s0 = 32 * side + 16 * m + g;
+                lw.y[s0][2 * t] = y[m][0];
+                lw.y[s0][2 * t + 1] = y[m][1];
+                lw.y[s0 + 8][2 * t] = y[m][2];
+                lw.y[s0 + 8][2 * t + 1] = y[m][3];
+            }
+        }
+    }
+    __syncwarp();
+    double cx[4] = {0.0, 0.0, 0.0, 0.0}, cy[4] = {0.0, 0.0, 0.0, 0.0};
+    bool okx = false, oky = false;
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+        const int slot = 32 * side + lane;
+        const FaceScale& fs = lw.fs[slot];
+        if (fs.gate == 2.f) continue;
         double c[4];
 #pragma unroll
         for (int o = 0; o < 4; ++o) c[o] = face_correction(lw.y[slot][o], o, fs, w.norm);
-        if (face_vetoed(c[0], c[3], dtn, fs, la.gate)) {
-            nfired += count ? 1u : 0u;
-            return;
+        if (face_vetoed(c[0], c[3], side ? dtdy : dtdx, fs, la.gate)) {
+            nfired += (side ? county : countx) ? 1u : 0u;
+            continue;
         }
-        f.d += c[0];
-        f.n += c[1];
-        f.t1 += c[2];
-        f.e += c[3];
-    };
-    apply(lane, fsx, countx, fx, dtdx);
-    apply(32 + lane, fsy, county, fy, dtdy);
+        if (side) {
+#pragma unroll
+            for (int o = 0; o < 4; ++o) cy[o] = c[o];
+            oky = true;
+        } else {
+#pragma unroll
+            for (int o = 0; o < 4; ++o) cx[o] = c[o];
+            okx = true;
+        }
+    }
+    if (okx) {
+        fx.d += cx[0];
+        fx.n += cx[1];
+        fx.t1 += cx[2];
+        fx.e += cx[3];
+    }
+    if (oky) {
+        fy.d += cy[0];
+        fy.n += cy[1];
+        fy.t1 += cy[2];
+        fy.e += cy[3];
+    }
     __syncwarp();  // lw may be refilled
 }
 
@@ -1230,8 +1252,9 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
             // y face y0 (rows y0-2 .. y0+1); the segment below computes it
             // too, so only the grid's first segment counts its veto
             Flux5 none{};
-            learn_faces(*la, false, Stencil4{}, false, none, dtdx, do_cell,
-                        stencil_y(Pm2, Pm1, P0, P1), do_cell && by == 0, fyPrev, dtdy, ph, nfired);
+            const auto st = [&](int) { return stencil_y(Pm2, Pm1, P0, P1); };
+            learn_faces(*la, st, false, false, none, dtdx, do_cell, do_cell && by == 0, fyPrev,
+                        dtdy, ph, nfired);
             Pm2 = Pm1;
         }
         wlNext = wlNew;
@@ -1277,15 +1300,17 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
             // computed by two strips counts its veto in the strip that
             // updates cell xi (the grid's last face: cell xi-1)
             const int ta = t >= 2 ? t - 2 : 0;
-            const double2 e0 = sm.sP[0][ta], e1 = sm.sP[1][ta];
-            const double2 l0 = sm.sP[0][tl], l1 = sm.sP[1][tl];
-            const double2 r0 = sm.sP[0][tr], r1 = sm.sP[1][tr];
+            const auto st = [&](int side) {
+                if (side) return stencil_y(Pm2, Pm1, P0, P1);
+                const double2 e0 = sm.sP[0][ta], e1 = sm.sP[1][ta];
+                const double2 l0 = sm.sP[0][tl], l1 = sm.sP[1][tl];
+                const double2 r0 = sm.sP[0][tr], r1 = sm.sP[1][tr];
+                return stencil_x(W4{e0.x, e0.y, e1.x, e1.y}, W4{l0.x, l0.y, l1.x, l1.y}, Pm1,
+                                 W4{r0.x, r0.y, r1.x, r1.y});
+            };
             const bool hasx = t >= 2 && t <= NT - 2 && xi >= g.ib && xi <= g.ie;
-            learn_faces(*la, hasx,
-                        stencil_x(W4{e0.x, e0.y, e1.x, e1.y}, W4{l0.x, l0.y, l1.x, l1.y}, Pm1,
-                                  W4{r0.x, r0.y, r1.x, r1.y}),
-                        hasx && (t <= NT - 3 || xi == g.ie), fx, dtdx, do_cell,
-                        stencil_y(Pm2, Pm1, P0, P1), do_cell, fy, dtdy, ph, nfired);
+            learn_faces(*la, st, hasx, hasx && (t <= NT - 3 || xi == g.ie), fx, dtdx, do_cell,
+                        do_cell, fy, dtdy, ph, nfired);
         }
         sm.sF[0][t] = make_double2(fx.d, fx.n); sm.sF[1][t] = make_double2(fx.t1, fx.e);
         __syncthreads();
@@ -1634,7 +1659,7 @@ static void launch_stage2d_learn_k(const Ctx& c, const CUtensorMap& mc, const CU
                                    double* out, double c1, double c2, double c3, const float* model,
                                    const gk::FluxGate& gate, unsigned* fired, cudaStream_t s) {
     const Geom& g = c.g;
-    const int rows = c.h2d_rows;
+    const int rows = c.learn_rows > 0 ? c.learn_rows : c.h2d_rows;
     dim3 grid((g.nx + NT - 5) / (NT - 4), (g.ny + rows - 1) / rows);
     const size_t dyn = learn_dyn_bytes<NT, (KIND >= 1)>();
     static std::atomic<unsigned long long> attr_set{0};

@@ -24,6 +24,7 @@ constexpr int NMODEL = YSO + NO;  // parameters + normalisation = 5548 floats
 constexpr float kGeluA = 0.7978845608028654f;  // sqrt(2/pi)
 constexpr float kGeluB = 0.044715f;
 constexpr float kGeluE = -2.0f * 0.7978845608028654f * 1.4426950408889634f;  // -2 sqrt(2/pi) log2(e)
+constexpr float kGeluEB = kGeluE * 0.044715f;
 
 __device__ __forceinline__ float ex2_approx(float x) {
     float y;
@@ -38,12 +39,13 @@ __device__ __forceinline__ float rcp_approx(float x) {
 
 // GELU, tanh form: 0.5 x (1 + tanh(u)), u = sqrt(2/pi) (x + 0.044715 x^3),
 // evaluated as x * s with s = 0.5 (1 + tanh(u)) = 1 / (1 + exp(-2u)) (an
-// identity, with no cancellation for small u); dgelu receives its
-// derivative s + 2 x s (1 - s) sqrt(2/pi) (1 + 3 * 0.044715 x^2).
+// identity, with no cancellation for small u), exp(-2u) = 2^(x (E + E B x^2))
+// with E = -2 sqrt(2/pi) log2(e); dgelu receives the derivative
+// s + 2 x s (1 - s) sqrt(2/pi) (1 + 3 * 0.044715 x^2).
 __device__ __forceinline__ float gelu(float x, float* dgelu) {
     const float x2 = __fmul_rn(x, x);
-    const float inner = __fmaf_rn(__fmul_rn(kGeluB, x2), x, x);  // x + B x^3
-    const float s = rcp_approx(__fadd_rn(1.f, ex2_approx(__fmul_rn(kGeluE, inner))));
+    const float arg = __fmul_rn(x, __fmaf_rn(kGeluEB, x2, kGeluE));
+    const float s = rcp_approx(__fadd_rn(1.f, ex2_approx(arg)));
     if (dgelu) {
         const float du = __fmul_rn(2.f * kGeluA, __fmaf_rn(3.f * kGeluB, x2, 1.f));
         *dgelu = __fmaf_rn(__fmul_rn(x, __fmul_rn(s, __fsub_rn(1.f, s))), du, s);
