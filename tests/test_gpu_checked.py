@@ -1,7 +1,8 @@
 """The bounds-checked build (lib/checked/libgk_cuda.so, GK_CHECKED) on the
 small parity cases: every path's cell, face, stage-row and TMA-row
 coordinates stay inside their arrays (gk_checked_report counts none), and the
-results are the normal build's bits.  The checked build runs in a child
+results are the normal build's bits -- the learned correction included, in
+the fused stage and as the generic path's pass.  The checked build runs in a child
 process (GK_CHECKED=1 selects it when the library loads)."""
 import json
 import os
@@ -46,6 +47,18 @@ sims = [Sim(dataclasses.replace(q, tmax=0.02, dtoutput=0.02), d) for q, d in ins
 Ensemble(sims).run_steps(6)
 for i, s in enumerate(sims):
     out["ens%d" % i] = (s.download(), s.dt_log(), s.path)
+from gaukuk_b200 import learned
+rng = np.random.default_rng(5)
+blob = learned.init_model(rng.normal(size=(256, 16)).astype(np.float32),
+                          (0.1 * rng.normal(size=(256, 4))).astype(np.float32), seed=2)
+blob[learned.NPARAM + 36:] *= 1e-3
+p, c = problems.kh(150, ny=70, seed=6)
+for fused in (True, False):
+    with Sim(dataclasses.replace(p, stepmax=6), c) as s:
+        learned.install(s, blob, fused=fused, diss_frac=0.25)
+        s.set_tiling(128, 5)
+        s.run(p.tmax, p.dtoutput)
+        out["learned_fused" if fused else "learned_pass"] = (s.download(), s.dt_log(), s.path)
 p, c = problems.kh(96, ny=90, seed=3)
 p = dataclasses.replace(p, stepmax=10)
 with Slabs(p, c, 3) as s:
@@ -80,6 +93,8 @@ def test_checked_build_finds_no_stray_index_and_keeps_the_bits(tmp_path):
     assert chk["count"] == 0, f"first stray coordinate: {chk['first']:#x}"
     assert chk["paths"] == plain["paths"]
     assert {"fused2d", "stage3d", "generic"} <= set(chk["paths"].values())
+    assert chk["paths"]["learned_fused"] == "fused2d" and chk["paths"]["learned_pass"] == "generic"
+    assert np.array_equal(a["learned_fused"], a["learned_pass"])
     for k in b.files:
         if k == "fused2d_fast":
             # fast mode: the checks may change the compiler's FMA contraction
