@@ -215,10 +215,17 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
     }
     // The selected side only (fast mode): its kinetic energy from the
     // selected velocities, and E + p as p/(gamma-1) + p + rho k/2 in one
-    // product with gamma/(gamma-1).
+    // product with gamma/(gamma-1).  m = rho (S - v) of the side, formed for
+    // the contact speed, carries the star-state terms:
+    //   rho (vn^2 + c S) = f1 vn + c m,   rho c ss (S - vn) = c ss m.
     const bool left = GK_GE0(ss);
     double d = left ? denl : denr, vn = left ? vxl : vxr, v1 = left ? vyl : vyr;
     double v2 = left ? vzl : vzr, p = left ? prel : prer, s = left ? sl : sr;
+#if GK_FASTMATH
+    const double m = left ? ml : mr;
+#else
+    const double m = d * (s - vn);  // unused: parity mode evaluates both sides
+#endif
     double k = T2 ? (vn * vn + v1 * v1 + v2 * v2) : (vn * vn + v1 * v1);
     double ep = p * ph.gm1Rec1 + 0.5 * d * k;  // E + p
     double sc = left ? GK_MIN0(s) : GK_MAX0(s);
@@ -226,8 +233,8 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
     double vc = vn + c;
     double f1 = d * vc;
     f.d = f1;
-    f.n = d * (vn * vn + c * s) + p;
+    f.n = f1 * vn + (c * m + p);
     f.t1 = f1 * v1;
     f.t2 = T2 ? f1 * v2 : 0.0;
-    f.e = ep * vc + d * c * ss * (s - vn);
+    f.e = ep * vc + c * ss * m;
 }
