@@ -152,8 +152,11 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
     // x- and y-face solves of a row interleave.
     const double gxl = fma(ph.gcq, GK_MAX0(prePVRS - prel), gpl);
     const double gxr = fma(ph.gcq, GK_MAX0(prePVRS - prer), gpr);
-    double sl = vxl - gxl * rsqrt_nr(gxl * denl);
-    double sr = vxr + gxr * rsqrt_nr(gxr * denr);
+    // S - v = -+ gX rsqrt(gX rho), so rho (S - v) = -+ (gX rho) rsqrt(gX rho)
+    const double xl = gxl * denl, xr = gxr * denr;
+    const double rl = rsqrt_nr(xl), rr = rsqrt_nr(xr);
+    double sl = vxl - gxl * rl;
+    double sr = vxr + gxr * rr;
 #else
     double ql, qr;
     // q = sqrt(1 + 0.5*(1+1/gamma)*max(p*/p - 1, 0)) is exactly 1 whenever
@@ -173,7 +176,7 @@ __device__ __forceinline__ void hllc(double denl, double vxl, double vyl, double
 #endif
 #if GK_FASTMATH
     // the contact speed with rho (S - v) of each side formed once
-    const double ml = denl * (sl - vxl), mr = denr * (sr - vxr);
+    const double ml = -(xl * rl), mr = xr * rr;
     double ss = GK_DIV(prer - prel + ml * vxl - mr * vxr, ml - mr);
 #else
     double ss = GK_DIV(prer - prel + denl * vxl * (sl - vxl) - denr * vxr * (sr - vxr),
