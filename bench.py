@@ -61,7 +61,7 @@ STAGE_BYTES_PER_CELL = 80  # per stage launch, averaged over the two RK2 stages
 # RK2 step (stage 1 + last stage), from the ncu capture in
 # profiles/stage2d_tma_kh2048_ncu.md; the FP64 pipe issues 64 lanes per
 # SM per clock on B200 (148 SMs)
-FP64_OPS_PER_ZU_FAST = 292 + 319
+FP64_OPS_PER_ZU_FAST = 283 + 310
 FP64_LANES = 64 * 148
 
 
