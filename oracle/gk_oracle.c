@@ -37,6 +37,9 @@ struct gko_sim {
     double *cons, *consTemp, *prim, *flx1, *flx2, *flx3;
     int step, isContinue, has_src;
     double t, dt, dtUntilOutput, cmax;
+    /* a y-slab of a split grid (gko_advance_split): fills the type-5 sides */
+    gko_halo_fn halo;
+    void* halo_user;
 };
 
 /* TArray index (template_array.hpp:67-72) for dims (NVAR, n3, n2, n1). */
@@ -475,6 +478,7 @@ static void update_bd(gko_sim* s, double* u) {
         if (d == 2 && s->p.nz <= 1) break;
         for (int side = 0; side < 2; ++side) {
             int type = s->p.bc[2 * d + side];
+            if (type == 5) continue; /* a side between slabs: gko_advance_split's halo */
             if (type < 0 || type > 3) type = 0;
             if (d == 2 && type == 0) bc_fill(s, u, 1, side, 0);
             else bc_fill(s, u, d, side, type);
@@ -508,15 +512,22 @@ static void swap_state(gko_sim* s) {
     double* t = s->cons; s->cons = s->consTemp; s->consTemp = t;
 }
 
+/* The ghost fill of a stage: UpdateBD, then (a slab of a split grid) the
+ * rows between slabs from the neighbours. */
+static void fill_ghosts(gko_sim* s, double* u) {
+    update_bd(s, u);
+    if (s->halo) s->halo(s->halo_user, u);
+}
+
 /* Sim::ForwardEuler_ / RK2_ / RK3_ (forward_euler.cpp:11-18, rk2.cpp:11-23,
  * rk3.cpp:11-29). */
 static void integrate(gko_sim* s) {
-    update_bd(s, s->cons);
+    fill_ghosts(s, s->cons);
     cons_to_prim(s, s->cons);
     cal_flux(s);
     update_cons(s, s->cons, s->consTemp, 0, 1.0, 1.0, 0.0);
     if (s->p.integrator == 1) { swap_state(s); return; }
-    update_bd(s, s->consTemp);
+    fill_ghosts(s, s->consTemp);
     cons_to_prim(s, s->consTemp);
     cal_flux(s);
     if (s->p.integrator != 3) {
@@ -525,7 +536,7 @@ static void integrate(gko_sim* s) {
         return;
     }
     update_cons(s, s->cons, s->consTemp, 1, 0.75, 0.25, 0.25);
-    update_bd(s, s->consTemp);
+    fill_ghosts(s, s->consTemp);
     cons_to_prim(s, s->consTemp);
     cal_flux(s);
     double frac13 = 1.0 / 3.0;
@@ -553,4 +564,46 @@ int gko_advance(gko_sim* s, double dtoutput, double* dtlog, int cap) {
         nsteps++;
     }
     return nsteps;
+}
+
+/* ------------------------------------------------------- y-slab split --- */
+
+void gko_set_spacing(gko_sim* s, double dx, double dy, double dz) {
+    s->dx = dx;
+    s->dy = dy;
+    s->dz = dz;
+    s->dxRec = 1. / dx;
+    s->dyRec = s->p.ny <= 1 ? 0 : 1. / dy;
+    s->dzRec = s->p.nz <= 1 ? 0 : 1. / dz;
+    s->drmin = smin(smin(dx, dy), dz);
+}
+
+/* Sim::Advance on a y-slab of a split grid, at most nsteps steps: the loop
+ * of gko_advance with the CFL maximum taken over all slabs (reduce) and the
+ * slab's type-5 y sides filled by halo after each stage's UpdateBD. */
+int gko_advance_split(gko_sim* s, double dtoutput, int nsteps, gko_halo_fn halo,
+                      gko_max_fn reduce, void* user, double* dtlog, int cap) {
+    int n = 0;
+    double tNext = s->t + dtoutput;
+    s->dtUntilOutput = dtoutput;
+    s->halo = halo;
+    s->halo_user = user;
+    while (fabs(tNext - s->t) > 1e-12 && s->isContinue && n < nsteps) {
+        const double local = gko_cmax(s);
+        s->cmax = reduce ? reduce(user, local) : local;
+        s->dt = s->p.cfl * s->drmin / s->cmax;
+        s->dt = smin(s->dt, s->dtUntilOutput);
+        if (s->has_src) const_gravity(s, s->cons, 0.5 * s->dt);
+        integrate(s);
+        if (s->has_src) const_gravity(s, s->cons, 0.5 * s->dt);
+        s->t += s->dt;
+        s->step++;
+        s->dtUntilOutput = tNext - s->t;
+        if (s->p.stepmax > 0 && s->step >= s->p.stepmax) s->isContinue = 0;
+        if (dtlog && n < cap) dtlog[n] = s->dt;
+        n++;
+    }
+    s->halo = NULL;
+    s->halo_user = NULL;
+    return n;
 }

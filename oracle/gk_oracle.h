@@ -37,6 +37,11 @@ typedef struct gko_params {
 
 typedef struct gko_sim gko_sim;
 
+/* The y-slab split (gko_advance_split): fills the y ghost rows of state u
+ * that come from the neighbouring slabs; the maximum over all slabs. */
+typedef void (*gko_halo_fn)(void* user, double* u);
+typedef double (*gko_max_fn)(void* user, double local);
+
 /* Sim::Sim (sim.cpp:45-67).  Returns NULL on invalid parameters. */
 gko_sim* gko_create(const gko_params* p);
 void gko_destroy(gko_sim* s);
@@ -58,6 +63,15 @@ double gko_cmax(const gko_sim* s);
 /* Sim::Advance (sim.cpp:69-117).  Appends each step's dt to dtlog (if not
  * NULL, up to cap entries) and returns the number of steps taken. */
 int gko_advance(gko_sim* s, double dtoutput, double* dtlog, int cap);
+
+/* A y-slab of a grid split across ranks (the multi-GPU decomposition of
+ * gk_slabs_*, restated): the whole grid's spacings, then Sim::Advance with
+ * the CFL maximum over all slabs (reduce) and the y sides of type 5 (between
+ * slabs) filled by halo after every stage's UpdateBD, at most nsteps
+ * steps.  The slabs' states are the undivided grid's bits. */
+void gko_set_spacing(gko_sim* s, double dx, double dy, double dz);
+int gko_advance_split(gko_sim* s, double dtoutput, int nsteps, gko_halo_fn halo,
+                      gko_max_fn reduce, void* user, double* dtlog, int cap);
 
 double gko_time(const gko_sim* s);
 double gko_dt(const gko_sim* s);

@@ -38,6 +38,10 @@ class GkoParams(ctypes.Structure):
     ]
 
 
+# callbacks of gko_advance_split: halo(user, state), reduce(user, local) -> max
+HALO_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double))
+MAX_FN = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_void_p, ctypes.c_double)
+
 _lib = None
 
 
@@ -71,6 +75,11 @@ def lib():
         L.gko_vanleer_batch.argtypes = [ctypes.c_int, dp, dp, dp]
         L.gko_cons_to_prim_batch.argtypes = [ctypes.c_int, dp, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_double, dp]
+        L.gko_set_spacing.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double]
+        L.gko_advance_split.restype = ctypes.c_int
+        L.gko_advance_split.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, HALO_FN,
+                                        MAX_FN, ctypes.c_void_p, dp, ctypes.c_int]
         _lib = L
     return _lib
 

@@ -1,5 +1,10 @@
 """Host logic of the y-slab split, on CPU (no device needed).
 
+* The decomposition itself, run by two gloo ranks on the oracle: each rank
+  advances its slab with the y ghost rows between slabs exchanged over gloo
+  after every stage's ghost fill and the CFL maximum all-reduced every step;
+  the slabs together are the undivided grid's bits, dt sequence included.
+
 * The partition: every active row belongs to exactly one slab, the first
   ny % n slabs take one row more, neighbours form a chain (a ring under
   periodic y; a single periodic slab is its own neighbour).
@@ -136,3 +141,128 @@ def test_two_ranks_agree_on_id_and_layout():
     # is the other's lower and upper neighbour
     assert out[0][1] == (0, 515, 1, 1)
     assert out[1][1] == (515, 515, 0, 0)
+
+
+def _split_case(name):
+    from gaukuk_b200 import problems
+    if name == "kh_periodic":
+        return problems.kh(24, ny=20, seed=3)
+    if name == "rt_walls_rk3_gravity":
+        p, c = problems.rt(16, 24)
+        assert p.integrator == 3 and p.bc[2] == p.bc[3] == 2 and p.grav[1] != 0
+        return p, c
+    raise KeyError(name)
+
+
+def _split_worker(rank, world, port, case, nsteps, q):
+    """One slab on the oracle: halo rows over gloo (sends of the top rows up
+    with tag 0 and of the bottom rows down with tag 1), the maximum by
+    all-reduce."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    try:
+        import dataclasses
+        import datetime
+
+        import numpy as np
+        import torch
+        import torch.distributed as dist
+
+        import gk_oracle
+        from gaukuk_b200.slabs import layout
+        dist.init_process_group("gloo", rank=rank, world_size=world,
+                                timeout=datetime.timedelta(seconds=30))
+        p, c = _split_case(case)
+        g = p.ng
+        periodic = p.bc[2] == 1
+        j0, cnt, lo, up = layout(p.ny, world, rank, periodic)
+        dy = (p.ymax - p.ymin) / p.ny
+        bc = list(p.bc)
+        bc[2] = 5 if lo >= 0 else p.bc[2]
+        bc[3] = 5 if up >= 0 else p.bc[3]
+        ps = dataclasses.replace(p, ny=cnt, ymin=p.ymin + j0 * dy, ymax=p.ymin + (j0 + cnt) * dy,
+                                 bc=tuple(bc), stepmax=-1)
+        sim = gk_oracle.OracleSim(ps, np.ascontiguousarray(c[:, :, j0:j0 + cnt + 2 * g, :]))
+        L = gk_oracle.lib()
+        L.gko_set_spacing(sim.h, (p.xmax - p.xmin) / p.nx, dy, (p.zmax - p.zmin) / p.nz)
+        kb, ib, ie = g, g, g + p.nx
+
+        def halo(user, ptr):
+            u = np.ctypeslib.as_array(ptr, shape=ps.shape)
+            reqs, got = [], {}
+            if up >= 0:
+                reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(u[:, kb, cnt:cnt + g, ib:ie])),
+                                       up, tag=0))
+            if lo >= 0:
+                reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(u[:, kb, g:2 * g, ib:ie])),
+                                       lo, tag=1))
+            if lo >= 0:
+                got["lo"] = torch.empty((5, g, p.nx), dtype=torch.float64)
+                reqs.append(dist.irecv(got["lo"], lo, tag=0))
+            if up >= 0:
+                got["up"] = torch.empty((5, g, p.nx), dtype=torch.float64)
+                reqs.append(dist.irecv(got["up"], up, tag=1))
+            for r in reqs:
+                r.wait()
+            if "lo" in got:
+                u[:, kb, 0:g, ib:ie] = got["lo"].numpy()
+            if "up" in got:
+                u[:, kb, cnt + g:cnt + 2 * g, ib:ie] = got["up"].numpy()
+
+        def reduce(user, local):
+            t = torch.tensor([local], dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+
+        hf, rf = gk_oracle.HALO_FN(halo), gk_oracle.MAX_FN(reduce)
+        dts = np.zeros(nsteps)
+        n = L.gko_advance_split(sim.h, 1e6, nsteps, hf, rf, None, gk_oracle._dp(dts), nsteps)
+        q.put((rank, (j0, cnt, n, dts.tolist(), sim.get_cons()[:, kb, g:g + cnt, ib:ie].copy())))
+        dist.destroy_process_group()
+    except Exception:  # reported to the test
+        import traceback
+        q.put((rank, "error: " + traceback.format_exc()))
+
+
+@pytest.mark.parametrize("case", ["kh_periodic", "rt_walls_rk3_gravity"])
+def test_two_gloo_ranks_advance_the_split_grid_bit_for_bit(case):
+    """Two slabs, one per gloo rank: a periodic ring (KH, RK2) and a grid
+    whose bottom and top are reflecting walls (RT, RK3 with constant
+    gravity), 10 steps, against the oracle on the undivided grid."""
+    import dataclasses
+
+    import numpy as np
+    gk_oracle = pytest.importorskip("gk_oracle")
+    world, nsteps = 2, 10
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_split_worker, args=(r, world, port, case, nsteps, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    out = {}
+    deadline = time.time() + 120
+    while len(out) < world and time.time() < deadline:
+        try:
+            r, v = q.get(timeout=max(0.1, deadline - time.time()))
+            out[r] = v
+        except Exception:
+            break
+    for p in procs:
+        p.join(timeout=10)
+        if p.is_alive():
+            p.kill()
+    assert sorted(out) == [0, 1], out
+    for r in range(world):
+        assert not isinstance(out[r], str), out[r]
+    p, c = _split_case(case)
+    whole = gk_oracle.OracleSim(dataclasses.replace(p, stepmax=nsteps), c)
+    ref_dts = whole.advance(1e6)
+    g = p.ng
+    ref = whole.get_cons()[:, g, g:g + p.ny, g:g + p.nx]
+    assert len(ref_dts) == nsteps
+    got = np.concatenate([out[r][4] for r in range(world)], axis=1)
+    assert [out[r][0] for r in range(world)] == [0, out[0][1]]
+    for r in range(world):
+        assert out[r][2] == nsteps and out[r][3] == ref_dts, (r, out[r][3], ref_dts)
+    assert np.array_equal(got, ref)
