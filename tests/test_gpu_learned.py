@@ -282,9 +282,15 @@ def _model():
     return blob
 
 
-def _pair(name, mode, blob):
+# A gate that decides nothing: no shocks, no positivity vetoes, no smooth
+# faces, no clip.
+GATE_OPEN = dict(shock_jump=1e30, pos_frac=1e30, tv_min=0.0, diss_frac=-1.0)
+
+
+def _pair(name, mode, blob, gate=None):
     from gaukuk_b200.sim import Sim
-    p, c, tiling, gate, _ = _fused_case(name)
+    p, c, tiling, case_gate, _ = _fused_case(name)
+    gate = case_gate if gate is None else gate
     a, b = Sim(p, c, mode=mode), Sim(p, c, mode=mode)
     for s in (a, b):
         if tiling:
@@ -328,11 +334,13 @@ def test_fused_correction_is_the_correction_pass_bitwise(case):
 @pytest.mark.parametrize("case", ["kh_rk2", "rt_rk3_gravity_tiles64"])
 def test_fused_correction_close_to_the_correction_pass_in_fast_mode(case):
     """Fast mode: the fused stage and the generic path round their fluxes
-    differently in the last bits; with the correction the two stay within
-    the fast-mode tolerance (1e-12 relative; momentum components against the
-    momentum's magnitude, as RT's x-momentum starts at exactly zero) after 8
-    steps, and the detector counts agree."""
-    p, c, a, b = _pair(case, "fast", _model())
+    differently in the last bits, and so do the network's inputs.  With a
+    gate that makes no threshold decision (a last-bit difference could flip
+    a face across tv_min or a veto, which parity mode's bitwise tests cover)
+    the two stay within the fast-mode tolerance (1e-12 relative; momentum
+    components against the momentum's magnitude, as RT's x-momentum starts
+    at exactly zero) after 8 steps."""
+    p, c, a, b = _pair(case, "fast", _model(), gate=GATE_OPEN)
     a.run_steps(8)
     b.run_steps(8)
     ga, gb = active(p, a.download()), active(p, b.download())
@@ -343,4 +351,4 @@ def test_fused_correction_close_to_the_correction_pass_in_fast_mode(case):
     print(f"\n{case} fast: fused vs pass rel Linf {err:.2e}, dt {dev:.2e}, vetoed "
           f"{learned.detector_count(a)} / {learned.detector_count(b)}")
     assert err <= 1e-12 and dev <= 1e-12
-    assert abs(learned.detector_count(a) - learned.detector_count(b)) <= 2
+    assert learned.detector_count(a) == learned.detector_count(b) == 0
