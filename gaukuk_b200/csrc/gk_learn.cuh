@@ -8,9 +8,10 @@
 // The units that include it are compiled with and without FMA contraction
 // (the parity unit has -fmad=false).  Every product that feeds a sum here is
 // therefore written with explicit round-to-nearest intrinsics (__dmul_rn,
-// __dadd_rn, __fmaf_rn, ...), and the activation uses the exponent and
-// reciprocal instructions directly, so the same inputs give the same bits in
-// every unit: the fused stage's corrections equal the correction pass's.
+// __dadd_rn, __fmaf_rn, ...), and the activation, reciprocals and roots use
+// the approximation instructions directly (with explicit Newton steps), so
+// the same inputs give the same bits in every unit: the fused stage's
+// corrections equal the correction pass's.
 #pragma once
 
 namespace gklearn {
@@ -210,10 +211,26 @@ __device__ __forceinline__ void forward_tiles(const MlpWeights& w, const __nv_bf
         for (int e = 0; e < 4; ++e) y[m][e] = acc[m][e];
 }
 
+// Reciprocal and square root of the features and bounds: the hardware
+// approximations with one Newton step (relative error about 2^-44; the
+// features go to BF16 and the bounds to FP32), written as explicit products
+// and fused multiply-adds so every unit compiles them alike.  x > 0.
+__device__ __forceinline__ double lrcp(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    return fma(y, fma(-x, y, 1.0), y);
+}
+__device__ __forceinline__ double lsqrt(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double s = __dmul_rn(x, y);
+    return fma(__dmul_rn(0.5, y), fma(-s, s, x), s);
+}
+
 // van Leer slope of the PLM reconstruction, (2ab)/(a+b) for ab > 0 else 0.
 __device__ __forceinline__ double vl_slope(double a, double b) {
     const double m = __dmul_rn(a, b);
-    return m <= 0.0 ? 0.0 : __ddiv_rn(__dmul_rn(2.0, m), __dadd_rn(a, b));
+    return m <= 0.0 ? 0.0 : __dmul_rn(__dmul_rn(2.0, m), lrcp(__dadd_rn(a, b)));
 }
 
 // What the detector and the output scaling need of one face, from its
@@ -238,9 +255,9 @@ __device__ __forceinline__ void face_inputs(const double (&r)[4], const double (
     const double rr = __dmul_rn(0.25, __dadd_rn(__dadd_rn(__dadd_rn(r[0], r[1]), r[2]), r[3]));
     const double pr = __dmul_rn(0.25, __dadd_rn(__dadd_rn(__dadd_rn(p[0], p[1]), p[2]), p[3]));
     // the features go to BF16: reciprocals of the references serve all four cells
-    const double irr = __drcp_rn(rr), ipr = __drcp_rn(pr);
-    const double cr = __dsqrt_rn(__dmul_rn(__dmul_rn(gamma, pr), irr));
-    const double icr = __drcp_rn(cr);
+    const double irr = lrcp(rr), ipr = lrcp(pr);
+    const double cr = lsqrt(__dmul_rn(__dmul_rn(gamma, pr), irr));
+    const double icr = lrcp(cr);
     float feat[NI];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
@@ -289,7 +306,8 @@ __device__ __forceinline__ void face_inputs(const double (&r)[4], const double (
             u[2] = __dmul_rn(d, b);
             u[3] = __dadd_rn(__dmul_rn(pp, gm1Rec),
                              __dmul_rn(__dmul_rn(0.5, d), __dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b))));
-            sp[side] = __dadd_rn(fabs(a), __dsqrt_rn(__ddiv_rn(__dmul_rn(gamma, pp), d)));
+            const double c2 = __dmul_rn(__dmul_rn(gamma, pp), lrcp(d));
+            sp[side] = __dadd_rn(fabs(a), c2 > 0.0 ? lsqrt(c2) : 0.0);
         }
         const double sm = __dmul_rn(__dmul_rn(0.5, fmax(sp[0], sp[1])), (double)gate.diss_frac);
 #pragma unroll
