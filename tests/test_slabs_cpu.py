@@ -223,16 +223,19 @@ def _split_worker(rank, world, port, case, nsteps, q):
         q.put((rank, "error: " + traceback.format_exc()))
 
 
+@pytest.mark.parametrize("world", [2, 3])
 @pytest.mark.parametrize("case", ["kh_periodic", "rt_walls_rk3_gravity"])
-def test_two_gloo_ranks_advance_the_split_grid_bit_for_bit(case):
-    """Two slabs, one per gloo rank: a periodic ring (KH, RK2) and a grid
-    whose bottom and top are reflecting walls (RT, RK3 with constant
-    gravity), 10 steps, against the oracle on the undivided grid."""
+def test_gloo_ranks_advance_the_split_grid_bit_for_bit(case, world):
+    """Two or three slabs, one per gloo rank: a periodic ring (KH, RK2) and
+    a grid whose bottom and top are reflecting walls (RT, RK3 with constant
+    gravity), 10 steps, against the oracle on the undivided grid.  With
+    three ranks the middle slab has different neighbours below and above,
+    and the ring's slabs have unequal rows (20 = 7 + 7 + 6)."""
     import dataclasses
 
     import numpy as np
     gk_oracle = pytest.importorskip("gk_oracle")
-    world, nsteps = 2, 10
+    nsteps = 10
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
@@ -252,7 +255,7 @@ def test_two_gloo_ranks_advance_the_split_grid_bit_for_bit(case):
         p.join(timeout=10)
         if p.is_alive():
             p.kill()
-    assert sorted(out) == [0, 1], out
+    assert sorted(out) == list(range(world)), out
     for r in range(world):
         assert not isinstance(out[r], str), out[r]
     p, c = _split_case(case)
@@ -262,7 +265,8 @@ def test_two_gloo_ranks_advance_the_split_grid_bit_for_bit(case):
     ref = whole.get_cons()[:, g, g:g + p.ny, g:g + p.nx]
     assert len(ref_dts) == nsteps
     got = np.concatenate([out[r][4] for r in range(world)], axis=1)
-    assert [out[r][0] for r in range(world)] == [0, out[0][1]]
+    starts = [out[r][0] for r in range(world)]
+    assert starts == [sum(out[q][1] for q in range(r)) for r in range(world)]
     for r in range(world):
         assert out[r][2] == nsteps and out[r][3] == ref_dts, (r, out[r][3], ref_dts)
     assert np.array_equal(got, ref)
