@@ -75,6 +75,7 @@ struct KernelSet {
     decltype(&gk_parity::launch_stage3d) stage3d;
     decltype(&gk_parity::launch_epilogue) epilogue;
     decltype(&gk_parity::launch_stage2d_learn) stage2d_learn;
+    decltype(&gk_parity::launch_run1d) run1d;
 };
 
 const KernelSet kParity = {gk_parity::launch_bc,     gk_parity::launch_c2p,
@@ -84,13 +85,14 @@ const KernelSet kParity = {gk_parity::launch_bc,     gk_parity::launch_c2p,
                            gk_parity::launch_mtz_check, gk_parity::launch_ens_stage,
                            gk_parity::launch_ens_bc,  gk_parity::launch_ens_begin,
                            gk_parity::launch_zflux,   gk_parity::launch_stage3d,
-                           gk_parity::launch_epilogue, gk_parity::launch_stage2d_learn};
+                           gk_parity::launch_epilogue, gk_parity::launch_stage2d_learn,
+                           gk_parity::launch_run1d};
 const KernelSet kFast = {gk_fast::launch_bc,     gk_fast::launch_c2p,     gk_fast::launch_flux,
                          gk_fast::launch_update, gk_fast::launch_kick,    gk_fast::launch_cfl,
                          gk_fast::launch_stage2d, gk_fast::launch_begin,  gk_fast::launch_mtz_check,
                          gk_fast::launch_ens_stage, gk_fast::launch_ens_bc, gk_fast::launch_ens_begin,
                          gk_fast::launch_zflux, gk_fast::launch_stage3d, gk_fast::launch_epilogue,
-                         gk_fast::launch_stage2d_learn};
+                         gk_fast::launch_stage2d_learn, gk_fast::launch_run1d};
 
 constexpr int kLogCap = 1 << 20;
 
@@ -383,10 +385,20 @@ int stage_rows(const gk::Geom& g, int threads, bool parity) {
 // at every face (TMA rows; unless gk_set_flux_model_fused turned that off).
 // Path 2, the 3D stage (z fluxes, then one fused x-y stage per plane),
 // applies to 3D RK2/RK3 runs (forward Euler updates in place, which the
-// fused stage cannot).  Path 0 is generic.
+// fused stage cannot).  Path 3, a 1D run in one CTA (k_run1d, many steps
+// per launch), applies to 1D runs of up to 1024 cells per row (lenx) with
+// the device's own ghost fills (copy, periodic, reflecting, outflow) and no
+// source term, learned correction or host routine.  Path 0 is generic.
 int choose_path(const gk_handle* h) {
     const gk::Ctx& c = h->ctx;
     if (c.g.ndim == 3 && c.ph.integrator != 1 && env_int("GK_STAGE3D", 1) != 0) return 2;
+    if (c.g.ndim == 1) {
+        bool own_fills = true;
+        for (int s = 0; s < 2; ++s) own_fills = own_fills && c.ph.bc[s] >= 0 && c.ph.bc[s] <= 3;
+        return (c.g.lenx <= 1024 && own_fills && !c.ph.has_grav && c.ph.npoint == 0 &&
+                c.ph.nshell == 0 && !c.ph.fix_inner && !h->model && h->host_fills.empty() &&
+                env_int("GK_RUN1D", 1) != 0) ? 3 : 0;
+    }
     if (!(c.g.ndim == 2 && !c.has_vz && c.ph.integrator != 1 && c.ph.grav[2] == 0 &&
           c.ph.npoint == 0))
         return 0;
@@ -491,6 +503,11 @@ void enqueue_step(gk_handle* h, Profiler* prof) {
     const int integ = c.ph.integrator;
     const double frac13 = 1.0 / 3.0;
     if (c.ph.has_grav || c.ph.npoint) GK_L(gk::K_KICK, k.kick(c, A, 0, s));
+    if (h->path == 3) {
+        // the whole step in one launch (ghost fills, stages, CFL, epilogue)
+        GK_L(gk::K_STAGE, k.run1d(c, A, B, 1, s));
+        return;
+    }
     if (h->path == 2) {
         // z fluxes of the stage's state into F3, then the fused x-y stage;
         // without a kick after it the last stage also reduces the CFL speed
@@ -590,7 +607,10 @@ int ensure_graph(gk_handle* h) {
     h->graph_steps = steps_per_graph_of(h->ctx.g);
     cudaGraph_t graph;
     GK_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < h->graph_steps; ++i) enqueue_step(h, nullptr);
+    if (h->path == 3)  // one launch runs the graph's steps
+        h->ks->run1d(h->ctx, h->A, h->B, h->graph_steps, h->stream);
+    else
+        for (int i = 0; i < h->graph_steps; ++i) enqueue_step(h, nullptr);
     GK_CUDA(h, cudaStreamEndCapture(h->stream, &graph));
     cudaError_t e = cudaGraphInstantiate(&h->gexec, graph, 0);
     cudaGraphDestroy(graph);
@@ -862,7 +882,7 @@ static int download(gk_handle* h, double* cons, bool zero_other_planes) {
     // and 1D y rows follow the reference's in-place order, so both keep A's.
     const double* donor = nullptr;
     if (h->htm->step > h->upload_step && h->ctx.ph.integrator != 1)
-        donor = (h->path >= 1 && h->ctx.ph.integrator == 3) ? h->C : h->B;
+        donor = ((h->path == 1 || h->path == 2) && h->ctx.ph.integrator == 3) ? h->C : h->B;
     if (donor) {
         const size_t rowb = sizeof(double) * g.lenx, prow = sizeof(double) * g.pitch;
         for (int n = 0; n < 5; ++n) {
@@ -1094,6 +1114,8 @@ int gk_graph_info(gk_handle* h, int* steps_per_graph, int* launches_per_step) {
         per = (c.ph.has_grav ? 1 : 0) + (2 + inner) * stages;  // kick, (ghost fill + stage) per stage
     } else if (h->path == 2) {
         per = (c.ph.has_grav || c.ph.npoint ? 3 : 0) + (3 + inner) * stages;
+    } else if (h->path == 3) {
+        per = 1;  // in a graph, one launch runs all of its steps
     } else {
         per = (c.ph.has_grav || c.ph.npoint ? 2 : 0) + stages * (3 + inner + c.g.ndim) + 1;
     }

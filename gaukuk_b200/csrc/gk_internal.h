@@ -221,6 +221,7 @@ static const char* const kClassNames[K_NCLASS] = {
                         const double* F3, int three, double c1, double c2, double c3,          \
                         cudaStream_t s);                                                       \
     void launch_cfl(const gk::Ctx& c, const double* u, int epilogue, cudaStream_t s);          \
+    void launch_run1d(const gk::Ctx& c, double* A, double* B, int nsteps, cudaStream_t s);     \
     void launch_stage2d(const gk::Ctx& c, const double* uc, const double* u0, double* out,     \
                         int kind, double c1, double c2, double c3, cudaStream_t s);            \
     void launch_stage2d_learn(const gk::Ctx& c, const double* uc, const double* u0,           \

@@ -651,6 +651,129 @@ __global__ void k_epilogue(DevTime* tm, Geom g, Phys ph) {
     step_epilogue(tm, g, ph, 1);
 }
 
+// ------------------------------------------------------------ 1D in one CTA
+// A 1D run of up to 1024 cells per array row (lenx) in one CTA: each step
+// runs the generic path's phases -- ghost fill (x sides), ConsToPrim of the
+// row, x fluxes, UpdateCons per RK stage, then CalCmax and the step
+// epilogue -- with the generic kernels' expressions in their order (the
+// same bits), the primitives and fluxes in shared memory and a barrier
+// where the generic path has a launch.  Up to nsteps steps per launch,
+// while the run is active.
+template <bool HAS_Z>
+__global__ void __launch_bounds__(1024) k_run1d(double* A, double* B, Geom g, Phys ph, DevTime* tm,
+                                                int nsteps) {
+    extern __shared__ double sh1[];
+    const int t = threadIdx.x;
+    const int nf = g.nx + 1;
+    double* W = sh1;               // primitives [5][lenx]
+    double* F = sh1 + 5 * g.lenx;  // x fluxes [5][nx + 1], face ib + f
+    const long long vs = g.vstride;
+    const long long row = sidx(g, g.kb, g.jb, 0);
+    __shared__ unsigned long long wmax[32];
+    // one RK stage: out = c1*uc - c2*dF (three = 0) or c1*u0 + c2*uc - c3*dF
+    auto stage = [&](double* uc, const double* u0, double* out, bool three, double c1, double c2,
+                     double c3) {
+        if (t < 2 * g.ng) bc_fill_one(uc, g, ph, 0, t / g.ng, t % g.ng);
+        __syncthreads();
+        if (t < g.lenx) {
+            const long long c = row + t;
+            double q[5];
+            cons_to_prim5(uc[gk::S_DEN * vs + c], uc[gk::S_MTX * vs + c], uc[gk::S_MTY * vs + c],
+                          uc[gk::S_MTZ * vs + c], uc[gk::S_ENG * vs + c], ph, q);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) W[v * g.lenx + t] = q[v];
+        }
+        __syncthreads();
+        if (t < nf) {
+            const int i = g.ib + t;  // the face between cells i-1 and i
+            double wl[5], wr[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                const double* p = W + v * g.lenx;
+                const double l1 = p[i - 2], l2 = p[i - 1], l3 = p[i];
+                const double r1 = l2, r2 = l3, r3 = p[i + 1];
+                if (ph.plm) {
+#if GK_FASTMATH
+                    wl[v] = l2 + vanleer_half(l2 - l1, l3 - l2);
+                    wr[v] = r2 - vanleer_half(r2 - r1, r3 - r2);
+#else
+                    wl[v] = l2 + 0.5 * vanleer(l2 - l1, l3 - l2);
+                    wr[v] = r2 - 0.5 * vanleer(r2 - r1, r3 - r2);
+#endif
+                } else {
+                    wl[v] = l2;
+                    wr[v] = r2;
+                }
+            }
+            Flux5 f;
+            hllc<true, kSel>(wl[gk::P_RHO], wl[gk::P_VX], wl[gk::P_VY], wl[gk::P_VZ], wl[gk::P_PRE],
+                             wr[gk::P_RHO], wr[gk::P_VX], wr[gk::P_VY], wr[gk::P_VZ], wr[gk::P_PRE],
+                             ph, f);
+            F[gk::S_DEN * nf + t] = f.d;
+            F[gk::P_VX * nf + t] = f.n;
+            F[gk::P_VY * nf + t] = f.t1;
+            F[gk::P_VZ * nf + t] = f.t2;
+            F[gk::S_ENG * nf + t] = f.e;
+        }
+        __syncthreads();
+        if (t < g.nx) {
+            const long long c = row + g.ib + t;
+            const double dt = tm->dt;
+            const double dtdx = dt * g.dxRec;
+            double r[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                double dF = (F[v * nf + t + 1] - F[v * nf + t]) * dtdx;
+                if (three) r[v] = c1 * u0[v * vs + c] + c2 * uc[v * vs + c] - c3 * dF;
+                else r[v] = c1 * uc[v * vs + c] - c2 * dF;
+            }
+            floors5(r, ph, tm);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) out[v * vs + c] = r[v];
+        }
+        __syncthreads();
+    };
+    const double frac13 = 1.0 / 3.0;
+    for (int s = 0; s < nsteps; ++s) {
+        if (!tm->active) break;  // set by the previous step's epilogue (or the begin kernel)
+        if (ph.integrator == 1) {
+            stage(A, nullptr, A, false, 1.0, 1.0, 0.0);
+        } else {
+            stage(A, nullptr, B, false, 1.0, 1.0, 0.0);
+            if (ph.integrator == 3) {
+                stage(B, A, B, true, 0.75, 0.25, 0.25);
+                stage(B, A, A, true, frac13, 2 * frac13, 2 * frac13);
+            } else {
+                stage(B, A, A, true, 0.5, 0.5, 0.5);
+            }
+        }
+        // CalCmax of the new state and the step epilogue (k_cfl's)
+        unsigned long long best = 0ull;
+        if (t < g.nx) {
+            const long long c = row + g.ib + t;
+            const double mz = HAS_Z ? A[gk::S_MTZ * vs + c] : 0.0;
+            const double local = cell_cmax(A[gk::S_DEN * vs + c], A[gk::S_MTX * vs + c],
+                                           A[gk::S_MTY * vs + c], mz, A[gk::S_ENG * vs + c], ph,
+                                           HAS_Z);
+            best = (unsigned long long)__double_as_longlong(local);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long x = __shfl_xor_sync(0xffffffffu, best, o);
+            best = x > best ? x : best;
+        }
+        if ((t & 31) == 0) wmax[t >> 5] = best;
+        __syncthreads();
+        if (t == 0) {
+            unsigned long long m = wmax[0];
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = wmax[w] > m ? wmax[w] : m;
+            atomicMax(&tm->cmax_acc, m);
+            step_epilogue(tm, g, ph, 1);
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_mtz_check(const double* __restrict__ u, Geom g, int* flag) {
     const long long ncell = (long long)g.nx * g.ny * g.nz;
     for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < ncell;
@@ -1613,6 +1736,23 @@ void launch_stage3d(const Ctx& c, const double* uc, const double* u0, double* ou
 
 void launch_kick(const Ctx& c, double* u, int which, cudaStream_t s) {
     k_kick<<<cell_grid(c.g, 128), 128, 0, s>>>(u, c.g, c.ph, c.tm, which);
+}
+
+// Shared memory of k_run1d: primitives and x fluxes of the row.
+static size_t run1d_smem(const Geom& g) { return (size_t)(5 * g.lenx + 5 * (g.nx + 1)) * sizeof(double); }
+
+void launch_run1d(const Ctx& c, double* A, double* B, int nsteps, cudaStream_t s) {
+    const Geom& g = c.g;
+    const int nt = (g.lenx + 31) / 32 * 32;
+    const size_t smem = run1d_smem(g);
+    static std::atomic<unsigned long long> attr_set{0};
+    if (gk::first_on_device(attr_set)) {  // the largest row: lenx 1024
+        const int most = (int)((5 * 1024 + 5 * 1021) * sizeof(double));
+        cudaFuncSetAttribute(k_run1d<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        cudaFuncSetAttribute(k_run1d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+    }
+    if (c.has_vz) k_run1d<true><<<1, nt, smem, s>>>(A, B, g, c.ph, c.tm, nsteps);
+    else k_run1d<false><<<1, nt, smem, s>>>(A, B, g, c.ph, c.tm, nsteps);
 }
 
 void launch_cfl(const Ctx& c, const double* u, int epilogue, cudaStream_t s) {

@@ -165,7 +165,7 @@ class Sim:
     def path(self) -> str:
         p = ctypes.c_int()
         _lib.check(self._L.gk_path(self.h, ctypes.byref(p)), self.h)
-        return {0: "generic", 1: "fused2d", 2: "stage3d"}[p.value]
+        return {0: "generic", 1: "fused2d", 2: "stage3d", 3: "run1d"}[p.value]
 
     def set_fixed_boundary(self, snapshot: Optional[np.ndarray], fix_inner: bool = False) -> None:
         """Data of the fixed (type 4) sides: the reference-layout state at

@@ -215,7 +215,9 @@ int gk_cmax(gk_handle* h, double* cmax);
 int gk_stream(gk_handle* h, void** stream);
 
 /* Which device implementation the handle selected: 0 generic (unfused
- * per-phase kernels, any dimension), 1 fused 2D stage kernel. */
+ * per-phase kernels, any dimension), 1 fused 2D stage kernel, 2 3D stage
+ * (z fluxes and a fused x-y stage per plane), 3 a 1D run in one CTA (up to
+ * 1024 cells per row, many steps per launch). */
 int gk_path(gk_handle* h, int* path);
 
 /* Launch accounting: whole time steps per graph launch, and kernel launches

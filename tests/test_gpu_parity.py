@@ -87,6 +87,8 @@ def test_paths_selected():
     s.set_point_gravity([(1.0, 0.0, 0.0, 0.0, 0.1)])  # point masses run on the generic path
     assert s.path == "generic"
     p, c = problems.sod(64)
+    assert _sim(p, c).path == "run1d"  # a 1D row of up to 1024 cells: one CTA
+    p, c = problems.sod(2000)
     assert _sim(p, c).path == "generic"
     p = Params(nx=16, ny=16, nz=16, bc=(1,) * 6, integrator=2, tmax=1.0, dtoutput=1.0)
     c = problems.random_smooth(p, seed=1, with_vz=True)
