@@ -89,6 +89,10 @@ struct Phys {
     // A slab of a grid split in y: the last stage leaves the step epilogue
     // to launch_epilogue, which runs after the CFL maximum over all slabs.
     int defer_epilogue;
+    // The fused 2D stage writes the periodic ghost images of the cells it
+    // updates (a grid periodic on all four sides, no source term): the
+    // steps skip the ghost fill.
+    int periodic_images;
 };
 
 // Device-resident clock of Sim::Advance (sim.cpp:69-117).  Written by the

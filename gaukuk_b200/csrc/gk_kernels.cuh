@@ -805,6 +805,26 @@ __global__ void k_mtz_check(const double* __restrict__ u, Geom g, int* flag) {
 constexpr int kStageThreads = 128;
 constexpr int kStageCols = kStageThreads - 4;
 
+// The periodic images of a cell the fused 2D stage writes (row = its row,
+// xi = its column, oc = its offset): on a grid periodic on all four sides
+// (ph.periodic_images) the stage stores the values the ghost fill would copy
+// from the cell into the x and y ghosts, so the steps need no ghost fill.
+// Corners, which no fill touches, stay as they are.  Planes DEN, MTX, MTY,
+// ENG (the fused path never writes MTZ).
+__device__ __forceinline__ void store_images(double* out, long long vs, long long P, long long oc,
+                                             int xi, int row, const Geom& g, const double (&r)[4]) {
+    auto put = [&](long long o) {
+        out[o] = r[0];
+        out[vs + o] = r[1];
+        out[2 * vs + o] = r[2];
+        out[3 * vs + o] = r[3];
+    };
+    if (xi < g.ib + g.ng) put(oc + (GK_CHK(xi + g.nx, 0, g.lenx, 10) - xi));
+    if (xi >= g.ie - g.ng) put(oc + (GK_CHK(xi - g.nx, 0, g.lenx, 10) - xi));
+    if (row < g.jb + g.ng) put(oc + (long long)(GK_CHK(row + g.ny, 0, g.leny, 11) - row) * P);
+    if (row >= g.je - g.ng) put(oc + (long long)(GK_CHK(row - g.ny, 0, g.leny, 11) - row) * P);
+}
+
 struct W4 {
     double r, vx, vy, p;
 };
@@ -1019,6 +1039,7 @@ __global__ void __launch_bounds__(kStageThreads, 3)
             out[vs + oc] = r[1];
             out[2 * vs + oc] = r[2];
             out[3 * vs + oc] = r[3];
+            if (ph.periodic_images) store_images(out, vs, P, oc, xi, f - 1, g, r);
         }
         fyPrev = fy;
         wlNext = wlNew;
@@ -1486,6 +1507,7 @@ __device__ __forceinline__ void stage_tile_tma(const CUtensorMap* mapc, const CU
             out[vs + oc] = r[1];
             out[2 * vs + oc] = r[2];
             out[3 * vs + oc] = r[3];
+            if (ph.periodic_images) store_images(out, vs, P, oc, xi, f - 1, g, r);
         }
         fyPrev = fy;
         wlNext = wlNew;
