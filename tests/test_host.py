@@ -62,3 +62,49 @@ def test_cabi_library_exports_every_declared_symbol():
         assert hasattr(L, s), s
     assert set(syms) == set(_lib.SIGNATURES)
     assert L.gk_strerror(0) == b"ok"
+
+
+_C_SCALARS = {"int": ("i", 4), "unsigned": ("u", 4), "unsigned int": ("u", 4),
+              "long long": ("i", 8), "unsigned long long": ("u", 8), "size_t": ("u", 8),
+              "float": ("f", 4), "double": ("f", 8), "void": "void"}
+
+
+def _c_class(decl):
+    """One parameter (or 'return-type name') of a C prototype: 'ptr' for data
+    and function pointers, else (kind, bytes)."""
+    words = decl.replace("*", " * ").replace("const", " ").split()
+    if "*" in words or words[0].endswith("_fn"):
+        return "ptr"
+    return _C_SCALARS.get(" ".join(words[:-1]), "?" + decl)
+
+
+def _py_class(t):
+    import ctypes
+    if t is None:
+        return "void"
+    if t in (ctypes.c_void_p, ctypes.c_char_p) or issubclass(t, (ctypes._Pointer, ctypes._CFuncPtr)):
+        return "ptr"
+    kind = {"i": "i", "l": "i", "q": "i", "I": "u", "L": "u", "Q": "u", "f": "f", "d": "f"}[t._type_]
+    return kind, ctypes.sizeof(t)
+
+
+def test_cabi_signatures_match_the_header():
+    """Each prototype in include/gaukuk_cuda.h against the ctypes signature the
+    Python binding declares: parameter count, pointer or scalar, and each
+    scalar's kind and width."""
+    from gaukuk_b200 import _lib
+    with open(os.path.join(ROOT, "include", "gaukuk_cuda.h")) as f:
+        text = f.read()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", " ", text)
+    protos = re.findall(r"([A-Za-z_][\w \t*]*?)\b(gk_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S)
+    seen = set()
+    for ret, name, params in protos:
+        params = " ".join(params.split())
+        want_args = [] if params in ("", "void") else [_c_class(q) for q in params.split(",")]
+        want_ret = _c_class(ret.strip() + " f")
+        rt, at = _lib.SIGNATURES[name]
+        assert [_py_class(a) for a in at] == want_args, name
+        assert _py_class(rt) == want_ret, name
+        seen.add(name)
+    assert seen == set(_lib.SIGNATURES)
