@@ -77,3 +77,47 @@ def test_model_blob_layout():
     assert b.size == learned.NMODEL == 5548 and b.dtype == np.float32
     Xn, Yn = learned.standardise(b, X, Y)
     assert np.allclose(Xn.mean(0), 0, atol=1e-5) and np.allclose(Yn.std(0), 1, atol=1e-3)
+
+
+def test_hll_dissipation_vanishes_on_a_uniform_state_and_not_at_a_jump():
+    """(1/2) max(|vn| + c) |U_R - U_L| at each face: zero where the PLM face
+    states agree, positive across the shear layers of a KH state, and the
+    same face count as the features."""
+    p, c = problems.kh(16, amp=0.0, noise=0.0)
+    a = learned.active2d(p, c)
+    uniform = np.broadcast_to(a[:, :1, :1], a.shape).copy()
+    for d in (0, 1):
+        D = learned.hll_dissipation(p, uniform, d)
+        assert D.shape == (16 * 16, 4) and np.all(D == 0.0)
+    Dy = learned.hll_dissipation(p, a, 1)
+    assert np.all(Dy >= 0.0) and Dy[:, 0].max() > 0.0
+    assert Dy.shape[0] == learned.face_features(p, a, 1)[0].shape[0]
+    # x faces see no jump: density and vx change only along y
+    assert np.all(learned.hll_dissipation(p, a, 0) == 0.0)
+
+
+def test_stencil_variation_and_face_rotation():
+    X = np.zeros((2, 16))
+    X[1, 4:8] = [1.0, -2.0, 0.5, 0.0]  # the second cell differs from its two neighbours
+    assert learned.stencil_variation(X).tolist() == [0.0, 2 * 3.5]
+    planes = np.arange(4 * 6, dtype=np.float64).reshape(4, 2, 3)
+    x = learned.rotate_to_face(planes, 0)
+    y = learned.rotate_to_face(planes, 1)
+    assert np.array_equal(x[:, 1], planes[1].ravel()) and np.array_equal(x[:, 2], planes[2].ravel())
+    assert np.array_equal(y[:, 1], planes[2].ravel()) and np.array_equal(y[:, 2], planes[1].ravel())
+    assert np.array_equal(x[:, [0, 3]], y[:, [0, 3]])
+
+
+def test_summary_leaves_out_diverged_runs():
+    def run(l1, secs, diverged=False):
+        return {"l1_at_64": l1, "seconds": secs, "diverged": diverged}
+
+    rows = [{"plain_64": run([1.0, 2.0], 1.0), "plain_128": run([0.5, 1.0], 4.0),
+             "learned_64": run([0.8, 1.5], 2.0)},
+            {"plain_64": run([3.0, 4.0], 3.0), "plain_128": run([1.5, 2.0], 8.0),
+             "learned_64": run([9.0, 9.0], 9.0, diverged=True)}]
+    s = learned.summarise(rows, 64)
+    assert s["plain_64"]["mean_l1_at_64"] == [2.0, 3.0] and s["plain_64"]["mean_seconds"] == 2.0
+    assert s["plain_128"]["median_l1_at_64"] == [1.0, 1.5]
+    assert s["learned_64"]["runs"] == 1 and s["learned_64"]["diverged"] == 1
+    assert s["learned_64"]["mean_l1_at_64"] == [0.8, 1.5] and s["learned_64"]["mean_seconds"] == 2.0
