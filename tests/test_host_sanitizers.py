@@ -3,9 +3,10 @@
 through their first frame: the setup, the host ghost fill with fixed sides,
 an immersed body's table and its fill, point and binary gravity enrollment,
 and the frame writer.  The frames must equal the plain build's.
-A hook whose own boundary routine depends on the state is refused at the
-first Advance; that path (the three probes of the routine) runs under the
-sanitizers too, before any device work, so all of this runs on the CPU."""
+The probes of a hook's own boundary routine run under the sanitizers too:
+one that writes outside its ghost strip is refused, and one that reads the
+state gets its depth search (it then runs on the host at every ghost fill).
+The probes come before any device work, so all of this runs on the CPU."""
 import dataclasses
 import os
 import subprocess
