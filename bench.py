@@ -94,7 +94,7 @@ def ncu_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 100 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -134,12 +134,20 @@ class ClockSampler:
             self.proc.kill()
         self.out.flush()
         with open(self.out.name) as f:
-            rows = [r.split(",") for r in f.read().strip().splitlines() if r.strip()]
+            text = f.read()
         self.out.close()
         try:
             os.unlink(self.out.name)
         except OSError:
             pass
+        return self.summarise(text)
+
+    @staticmethod
+    def summarise(text: str):
+        """Median SM clock, the highest max clock and the throttle reasons seen
+        Active in nvidia-smi's CSV rows (FIELDS, no header, no units); rows
+        that do not parse are skipped."""
+        rows = [r.split(",") for r in text.strip().splitlines() if r.strip()]
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
