@@ -80,7 +80,9 @@ typedef struct gk_handle gk_handle;
  * step = 0 (sim.cpp:45-46). */
 int gk_create(const gk_grid_desc* grid, const gk_phys_desc* phys, gk_handle** out);
 
-/* Releases the handle, its stream, graphs and device memory. */
+/* Releases the handle, its stream, graphs and device memory: the end of a
+ * Sim's lifetime, where the reference's TArray members free their arrays
+ * (~TArray, template_array.hpp:89-91). */
 void gk_destroy(gk_handle* h);
 
 /* Fixed (type 4) boundaries: Boundary::EnrollFixedBoundaryData
@@ -138,7 +140,8 @@ int gk_set_point_gravity(gk_handle* h, int n, const double* params);
 int gk_set_immersed(gk_handle* h, int n, const int* ids, const int* ntar, const double* dir,
                     const double* w);
 
-/* Number of doubles in one reference-layout state: 5*lenz*leny*lenx. */
+/* Number of doubles in one reference-layout state, the size of Sim::cons
+ * (cons.NewArray(NVar, lenz, leny, lenx), sim.cpp:49): 5*lenz*leny*lenx. */
 long long gk_state_size(const gk_handle* h);
 
 /* Loads Sim::cons from the host after the setup hook ran (main.cpp:25-30):
@@ -174,7 +177,8 @@ int gk_download_planes(gk_handle* h, double* cons);
 int gk_floor_hits(gk_handle* h, unsigned long long* density, unsigned long long* pressure);
 
 /* Bytes the last gk_upload_cons and the last download moved across the bus
- * (either pointer may be NULL). */
+ * (either pointer may be NULL).  No counterpart in the reference, whose state
+ * never leaves host memory. */
 int gk_io_bytes(const gk_handle* h, long long* upload, long long* download);
 
 /* Replaces Sim::Advance (sim.cpp:69-117, sim.hpp:39): runs time steps on the
@@ -185,9 +189,10 @@ int gk_io_bytes(const gk_handle* h, long long* upload, long long* download);
  * and the isContinue flag after the call. */
 int gk_advance(gk_handle* h, double dtoutput, double* t, int* step, int* is_continue);
 
-/* Runs exactly nsteps steps (fewer if stepmax stops the run) with no output
- * time to clamp dt, i.e. Sim::Advance with an infinite dtoutput.  Returns
- * after the stream synchronises; *done receives the steps taken. */
+/* Runs exactly nsteps steps (fewer if stepmax stops the run, sim.cpp:96-97)
+ * with no output time to clamp dt, i.e. Sim::Advance (sim.cpp:69-117) with an
+ * infinite dtoutput.  Returns after the stream synchronises; *done receives
+ * the steps taken. */
 int gk_run_steps(gk_handle* h, int nsteps, int* done);
 
 /* As gk_run_steps, but only enqueues the work on the handle's stream and
@@ -198,7 +203,9 @@ int gk_enqueue_steps(gk_handle* h, int nsteps);
 /* Sim::GetTime / Getdt / GetStep and Sim::isContinue (sim.hpp:26,44-46). */
 int gk_get_time(gk_handle* h, double* t, double* dt, int* step, int* is_continue);
 
-/* Sets the simulation clock (restart from a written frame). */
+/* Sets the simulation clock, for a restart from a written frame (the frame
+ * holds t, write_sim.cpp:33).  The reference has no setter: t and step are
+ * private members of Sim (sim.hpp:48-49). */
 int gk_set_time(gk_handle* h, double t, int step);
 
 /* The dt of every step since the last upload, at full precision: the values
@@ -211,23 +218,26 @@ int gk_dt_log(gk_handle* h, double* buf, int cap, int* n);
 int gk_cmax(gk_handle* h, double* cmax);
 
 /* The handle's CUDA stream (a cudaStream_t), for callers that time or order
- * work around the library's launches. */
+ * work around the library's launches.  No counterpart in the reference (CPU
+ * only). */
 int gk_stream(gk_handle* h, void** stream);
 
 /* Which device implementation the handle selected: 0 generic (unfused
  * per-phase kernels, any dimension), 1 fused 2D stage kernel, 2 3D stage
  * (z fluxes and a fused x-y stage per plane), 3 a 1D run in one CTA (up to
- * 1024 cells per row, many steps per launch). */
+ * 1024 cells per row, many steps per launch).  No counterpart in the
+ * reference, which has one CPU path for every dimension. */
 int gk_path(gk_handle* h, int* path);
 
 /* Launch accounting: whole time steps per graph launch, and kernel launches
- * per time step on the selected path. */
+ * per time step on the selected path.  No counterpart in the reference. */
 int gk_graph_info(gk_handle* h, int* steps_per_graph, int* launches_per_step);
 
 /* Device time of each kernel class over `nsteps` un-graphed steps, measured
  * with CUDA events on the handle's stream: names (';'-separated, into
  * `names`, size `names_cap`), per-class total milliseconds and launch counts
- * (arrays of `cap` entries).  *n receives the number of classes. */
+ * (arrays of `cap` entries).  *n receives the number of classes.  The
+ * reference times only the whole run (main.cpp:42-43, 54-58). */
 int gk_profile_steps(gk_handle* h, int nsteps, char* names, int names_cap,
                      double* total_ms, int* launches, int cap, int* n);
 
@@ -337,7 +347,8 @@ int gk_tap_substeps(gk_handle* h, int nsub, double dt_sub, int ratio, double* fx
  * IEEE result, of its refined reciprocal, square root and reciprocal square
  * root against CUDA's IEEE division and sqrt, over n arguments spread over
  * [2^-60, 2^60] (worst3 = {reciprocal, sqrt, rsqrt}).  Runs on the current
- * device. */
+ * device.  No counterpart in the reference, whose arithmetic is the host
+ * compiler's. */
 int gk_fastmath_check(int n, unsigned long long seed, double* worst3);
 
 
@@ -441,7 +452,9 @@ int gk_slabs_dt_log(gk_slabs* s, double* buf, int cap, int* n);
 int gk_slabs_info(gk_slabs* s, int* nslab_local, int* first, int* j0, int* rows);
 const char* gk_slabs_last_error(const gk_slabs* s);
 
-/* Text for a status code, and the last failure message on a handle. */
+/* Text for a status code, and the last failure message on a handle.  The
+ * reference throws instead (grid.hpp:24, read_config.cpp:22,
+ * write_sim.cpp:25) and main does not catch. */
 const char* gk_strerror(int status);
 const char* gk_last_error(const gk_handle* h);
 
