@@ -24,7 +24,8 @@ enum { DEN = 0, MTX = 1, MTY = 2, MTZ = 3, ENG = 4 };
 enum { VLX = 1, VLY = 2, VLZ = 3, PRE = 4 };
 #define NVAR 5
 
-/* libstdc++ std::max / std::min: max(a,b) = (a<b)?b:a, min(a,b) = (b<a)?b:a */
+/* libstdc++ std::max / std::min as the reference calls them (adiabatic.cpp:49,
+ * 153-156; sim.cpp:35): max(a,b) = (a<b)?b:a, min(a,b) = (b<a)?b:a */
 static inline double smax(double a, double b) { return (a < b) ? b : a; }
 static inline double smin(double a, double b) { return (b < a) ? b : a; }
 
@@ -96,6 +97,7 @@ gko_sim* gko_create(const gko_params* p) {
     return s;
 }
 
+/* Sim's arrays freed (~TArray, template_array.hpp:89-91). */
 void gko_destroy(gko_sim* s) {
     if (!s) return;
     free(s->cons); free(s->consTemp); free(s->prim);
@@ -103,6 +105,10 @@ void gko_destroy(gko_sim* s) {
     free(s);
 }
 
+/* Sim::cons as a setup hook leaves it (main.cpp:25-30), and as Sim::WriteData
+ * reads it (write_sim.cpp:14-58); the clock as Sim::GetTime / Getdt / GetStep
+ * and isContinue give it (sim.hpp:26, 43-45).  gko_set_time has no reference
+ * counterpart (t and step are private, sim.hpp:48-49): restarts use it. */
 void gko_set_cons(gko_sim* s, const double* cons) {
     memcpy(s->cons, cons, sizeof(double) * (size_t)gko_state_size(s));
 }
@@ -178,6 +184,8 @@ double gko_cmax(const gko_sim* s) {
     return cmax;
 }
 
+/* The per-cell body of EquationOfState::ConsToPrim (adiabatic.cpp:49-57) over
+ * n cells of planar arrays, for tests of single cells. */
 void gko_cons_to_prim_batch(int n, const double* cons, double gamma,
                             double dfloor, double pfloor, double* prim) {
     const double gm1 = gamma - 1.0;
@@ -205,6 +213,7 @@ static inline double vanleer(double a, double b) {
     return (multi <= 0.0) ? 0.0 : sigma;
 }
 
+/* Reconstruction::VanLeer (reconstruction.hpp:36-42) over n slope pairs. */
 void gko_vanleer_batch(int n, const double* a, const double* b, double* out) {
     for (int c = 0; c < n; ++c) out[c] = vanleer(a[c], b[c]);
 }
@@ -268,6 +277,7 @@ static inline void hllc(const double wl[5], const double wr[5], int dir,
     f[ENG] = selectl * fl5 + selectr * fr5;
 }
 
+/* Flux::RiemannSolver (hllc.cpp:22-101) over n interfaces of planar states. */
 void gko_hllc_batch(int n, const double* wl, const double* wr, int dir,
                     double gamma, double* flux) {
     const double gm1Rec = 1.0 / (gamma - 1.0);
@@ -412,7 +422,9 @@ static void update_cons(gko_sim* s, const double* u, double* ut, int three_coef,
 
 /* One ghost-fill routine of boundary/{outflow_copy,periodic,reflective,
  * outflow}.cpp for direction d (0 x, 1 y, 2 z), side (0 left, 1 right) and
- * type (0 copy, 1 periodic, 2 reflective, 3 outflow).  Ghosts are filled on
+ * type (0 copy, 1 periodic, 2 reflective, 3 outflow): OutflowCopyXL..ZR
+ * (outflow_copy.cpp:16-182), PeriodicXL..ZR (periodic.cpp:19-191),
+ * ReflectiveXL..ZR (reflective.cpp:19-244), OutflowXL..ZR (outflow.cpp:20-312).  Ghosts are filled on
  * active rows/columns only; corners are never touched.  Loop order follows
  * the reference so the in-place semantics match even when n < nGhost. */
 static void bc_fill(gko_sim* s, double* u, int d, int side, int type) {
@@ -486,6 +498,7 @@ static void update_bd(gko_sim* s, double* u) {
     }
 }
 
+/* Boundary::UpdateBD on Sim::cons (boundary.cpp:127-142), for tests. */
 void gko_update_bd(gko_sim* s) { update_bd(s, s->cons); }
 
 /* ------------------------------------------------------------- source --- */
@@ -508,12 +521,14 @@ static void const_gravity(gko_sim* s, double* u, double dt) {
 
 /* ---------------------------------------------------------- integrate --- */
 
+/* cons.Swap(consTemp), the integrators' last line (forward_euler.cpp:16,
+ * rk2.cpp:21, rk3.cpp:27). */
 static void swap_state(gko_sim* s) {
     double* t = s->cons; s->cons = s->consTemp; s->consTemp = t;
 }
 
-/* The ghost fill of a stage: UpdateBD, then (a slab of a split grid) the
- * rows between slabs from the neighbours. */
+/* The ghost fill of a stage: UpdateBD (rk2.cpp:12, 17; rk3.cpp:12, 17, 22),
+ * then (a slab of a split grid) the rows between slabs from the neighbours. */
 static void fill_ghosts(gko_sim* s, double* u) {
     update_bd(s, u);
     if (s->halo) s->halo(s->halo_user, u);
@@ -568,6 +583,9 @@ int gko_advance(gko_sim* s, double dtoutput, double* dtlog, int cap) {
 
 /* ------------------------------------------------------- y-slab split --- */
 
+/* A slab's spacings set to the whole grid's, as Sim forms them (sim.cpp:26-35:
+ * dxRec, dyRec = 0 for one row, drmin); the slab's own extent would round
+ * differently. */
 void gko_set_spacing(gko_sim* s, double dx, double dy, double dz) {
     s->dx = dx;
     s->dy = dy;
@@ -578,9 +596,10 @@ void gko_set_spacing(gko_sim* s, double dx, double dy, double dz) {
     s->drmin = smin(smin(dx, dy), dz);
 }
 
-/* Sim::Advance on a y-slab of a split grid, at most nsteps steps: the loop
- * of gko_advance with the CFL maximum taken over all slabs (reduce) and the
- * slab's type-5 y sides filled by halo after each stage's UpdateBD. */
+/* Sim::Advance (sim.cpp:69-117) on a y-slab of a split grid, at most nsteps
+ * steps: the loop of gko_advance with the CFL maximum taken over all slabs
+ * (reduce) and the slab's type-5 y sides filled by halo after each stage's
+ * UpdateBD.  No counterpart in the reference, which runs one grid whole. */
 int gko_advance_split(gko_sim* s, double dtoutput, int nsteps, gko_halo_fn halo,
                       gko_max_fn reduce, void* user, double* dtlog, int cap) {
     int n = 0;
