@@ -1308,6 +1308,8 @@ int efail(gk_ensemble* e, int code, const std::string& msg) {
             return efail((e), GK_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
+// Whether any instance of an ensemble is still inside its Sim::Advance loop
+// (sim.cpp:72): the host's loop condition for the whole ensemble.
 __global__ void k_ens_any_active(const gk::EnsInst* __restrict__ inst, int n, int* any) {
     int a = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) a |= inst[i].tm->active;
@@ -1510,11 +1512,14 @@ const char* gk_ens_last_error(const gk_ensemble* e) { return e ? e->err.c_str() 
 // current state, and restricted fine-grid fluxes over fixed sub-steps.
 namespace {
 
+// The clock of a fixed-dt tap: dt set and the run active, so the per-phase
+// kernels run (the reference's dt comes from sim.cpp:79-81 instead).
 __global__ void k_arm_clock(gk::DevTime* tm, double dt) {
     tm->dt = dt;
     tm->active = 1;
 }
 
+// t += dt and step++ for each of n steps (sim.cpp:92-93), then inactive.
 __global__ void k_clock_advance(gk::DevTime* tm, double dt, int n) {
     for (int i = 0; i < n; ++i) tm->t += dt;
     tm->step += n;

@@ -159,6 +159,9 @@ __device__ __forceinline__ void bc_fill_one(double* __restrict__ u, const Geom& 
     for (int v = 0; v < 5; ++v) u[v * g.vstride + dst] = q[v];
 }
 
+// Boundary::UpdateBD (boundary.cpp:127-142) for the run's dimensions: one
+// grid row per side (blockIdx.y = 2 * direction + side), one ghost cell per
+// thread through bc_fill_one.
 __global__ void k_bc(double* __restrict__ u, Geom g, Phys ph, const DevTime* __restrict__ tm) {
     if (!tm->active) return;
     const int dir = blockIdx.y >> 1, side = blockIdx.y & 1;
@@ -261,6 +264,8 @@ __device__ __forceinline__ void cons_to_prim5(double d, double mx, double my, do
     w[gk::P_PRE] = GK_BELOW(ph.pmin, pre) ? pre : ph.pmin;
 }
 
+// EquationOfState::ConsToPrim (adiabatic.cpp:18-61) of every stored cell,
+// ghosts included.
 __global__ void k_c2p(const double* __restrict__ u, double* __restrict__ w, Geom g, Phys ph,
                       const DevTime* __restrict__ tm) {
     if (!tm->active) return;
@@ -411,6 +416,8 @@ __device__ __forceinline__ double floors4_inv(double (&r)[4], const Phys& ph, De
     return inv_den;
 }
 
+// Sim::UpdateCons (update_cons.cpp:11-68) of one RK stage: the flux
+// difference of every active cell, the stage combine and the floors.
 __global__ void k_update(const double* u0, const double* uc, double* out,
                          const double* __restrict__ F1, const double* __restrict__ F2,
                          const double* __restrict__ F3, Geom g, Phys ph, int three, double c1,
@@ -575,6 +582,10 @@ __device__ void step_epilogue(DevTime* tm, const Geom& g, const Phys& ph, int ep
     }
 }
 
+// EquationOfState::CalCmax (adiabatic.cpp:115-160) as a maximum of the
+// non-negative doubles' bit patterns folded into tm->cmax_acc; with
+// `epilogue` the last CTA to finish runs the tail of the Sim::Advance loop
+// body (sim.cpp:92-103) through step_epilogue.
 template <bool HAS_Z>
 __global__ void __launch_bounds__(256) k_cfl(const double* __restrict__ u, Geom g, Phys ph,
                                              DevTime* tm, int epilogue) {
@@ -640,6 +651,7 @@ __device__ __forceinline__ void begin_one(DevTime* tm, const Geom& g, const Phys
     tm->active = act;
 }
 
+// begin_one on the device clock (sim.cpp:70-72, 77-81).
 __global__ void k_begin(DevTime* tm, Geom g, Phys ph, double dtoutput, int steps) {
     begin_one(tm, g, ph, dtoutput, steps);
 }
@@ -774,6 +786,9 @@ __global__ void __launch_bounds__(1024) k_run1d(double* A, double* B, Geom g, Ph
     }
 }
 
+// Sets *flag when MTZ is non-zero on an active cell: the fused 2D path
+// evolves four variables and needs MTZ = 0 (no reference counterpart; the
+// reference evolves all five everywhere).
 __global__ void k_mtz_check(const double* __restrict__ u, Geom g, int* flag) {
     const long long ncell = (long long)g.nx * g.ny * g.nz;
     for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < ncell;
@@ -1556,6 +1571,9 @@ __host__ __device__ constexpr size_t stage_dyn_bytes() {
     return (size_t)(kRing + (THREE ? kRing0 : 0)) * 4 * NT * sizeof(double);
 }
 
+// One RK stage of a 2D run (ConsToPrim, PLM, HLLC x and y, UpdateCons with
+// the stage combine and floors: adiabatic.cpp:18-61, recon_piecewise_linear.cpp:8-50,
+// hllc.cpp:22-101, update_cons.cpp:11-68), tiles staged by TMA: stage_tile_tma.
 template <int NT, int KIND, bool PLM>
 __global__ void __launch_bounds__(NT, 512 / NT)
     k_stage2d_tma(const __grid_constant__ CUtensorMap mapc, const __grid_constant__ CUtensorMap map0,
@@ -1579,6 +1597,8 @@ __host__ __device__ constexpr size_t learn_dyn_bytes() {
     return stage_dyn_bytes<NT, THREE>() + sizeof(gklearn::MlpWeights) + (NT / 32) * sizeof(LearnWarp);
 }
 
+// k_stage2d_tma with the learned correction added to every face's HLLC flux
+// (hllc.cpp:90-95, cal_flux.cpp:89-121), the model's weights in shared memory.
 template <int NT, int KIND, bool PLM>
 __global__ void __launch_bounds__(NT, 256 / NT)
     k_stage2d_learn(const __grid_constant__ CUtensorMap mapc, const __grid_constant__ CUtensorMap map0,
@@ -1647,6 +1667,7 @@ __global__ void k_ens_bc(const gk::EnsInst* __restrict__ inst, int which) {
     bc_fill_one(which ? I->B : I->A, g, I->ph, dir, side, id);
 }
 
+// begin_one (sim.cpp:70-72, 77-81) for every instance of an ensemble.
 __global__ void k_ens_begin(const gk::EnsInst* __restrict__ inst, int n, double dtoutput,
                             int steps) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1850,6 +1871,8 @@ static void launch_stage2d_learn_nt(const Ctx& c, const CUtensorMap& mc, const C
 #undef GK_SL
 }
 
+// Adds status bits to the device clock, in stream order (no reference
+// counterpart: the reference throws).
 __global__ void k_or_status(DevTime* tm, int bits) { tm->status |= bits; }
 
 // The fused stage with the learned correction (TMA rows only; CTAs of 64 or

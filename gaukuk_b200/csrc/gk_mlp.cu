@@ -360,7 +360,8 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ p
 
 // ------------------------------------------------------------ inference
 // Adds the learned correction to the face fluxes of one direction of a 2D
-// generic-path stage (F: FP64 face fluxes, W: FP64 primitives).  One warp
+// generic-path stage (F: FP64 face fluxes, W: FP64 primitives), after
+// Flux::CalFlux formed them (cal_flux.cpp:89-121; no reference counterpart).  One warp
 // per 16 faces.  The plain HLLC flux is kept where the detector fires (a
 // pressure jump max(p)/min(p) > 1 + shock_jump over the stencil, or a
 // correction that would move more than pos_frac of an adjacent cell's mass

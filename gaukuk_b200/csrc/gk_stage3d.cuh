@@ -92,7 +92,8 @@ __device__ __forceinline__ void hllc5_y(const double (&l)[5], const double (&r)[
 }
 
 // ------------------------------------------------------------ z faces
-// A CTA of 128 threads owns a tile of 32 columns x 4 rows of z faces and
+// Flux::CalFlux's z sweep (cal_flux.cpp:140-156; first order 72-87): PLM states and HLLC at
+// every z face.  A CTA of 128 threads owns a tile of 32 columns x 4 rows of z faces and
 // marches up a segment of zseg faces; a thread owns column (i, j) of the
 // tile.  Per plane the CTA converts the tile's 6 rows (the 4 rows and one
 // halo row below and above) once, 1.5 cells per face instead of the 3 a
