@@ -42,6 +42,8 @@ class Sim:
 
     def __init__(self, params: Params, cons: Optional[np.ndarray] = None, mode: str = "parity",
                  device: int = 0):
+        """Sim::Sim (sim.cpp:45-67) through gk_create; ``cons``, if given, is
+        uploaded as a setup hook leaves Sim::cons (main.cpp:25-30)."""
         self.params = params
         self.mode = mode
         self._L = _lib.load()
@@ -71,6 +73,8 @@ class Sim:
 
     # -- state -----------------------------------------------------------
     def upload(self, cons: np.ndarray) -> None:
+        """Loads Sim::cons (reference layout, ghosts included) after a setup hook
+        or between outputs (main.cpp:25-30); clears the dt log."""
         c = np.ascontiguousarray(cons, dtype=np.float64)
         if c.shape != self.params.shape:
             raise ValueError(f"state shape {c.shape} != {self.params.shape}")
@@ -102,6 +106,7 @@ class Sim:
 
     # -- time loop -------------------------------------------------------
     def advance(self, dtoutput: float) -> Tuple[float, int, bool]:
+        """Sim::Advance(dtoutput) (sim.cpp:69-117); returns (t, step, isContinue)."""
         t, step, cont = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
         _lib.check(self._L.gk_advance(self.h, float(dtoutput), ctypes.byref(t), ctypes.byref(step),
                                       ctypes.byref(cont)), self.h)
@@ -119,11 +124,14 @@ class Sim:
             t, _, _ = self.advance(dtoutput)
 
     def run_steps(self, n: int) -> int:
+        """n steps of the Sim::Advance loop body (sim.cpp:72-103) with no output
+        time; returns the steps taken (fewer if stepmax ends the run)."""
         done = ctypes.c_int()
         _lib.check(self._L.gk_run_steps(self.h, int(n), ctypes.byref(done)), self.h)
         return done.value
 
     def enqueue_steps(self, n: int) -> None:
+        """As run_steps, but returns once the steps are enqueued on ``stream``."""
         _lib.check(self._L.gk_enqueue_steps(self.h, int(n)), self.h)
 
     def _time(self):
@@ -133,22 +141,30 @@ class Sim:
         return t.value, dt.value, step.value, bool(cont.value)
 
     def get_time(self) -> float:
+        """Sim::GetTime (sim.hpp:43)."""
         return self._time()[0]
 
     def get_dt(self) -> float:
+        """Sim::Getdt (sim.hpp:44)."""
         return self._time()[1]
 
     def get_step(self) -> int:
+        """Sim::GetStep (sim.hpp:45)."""
         return self._time()[2]
 
     @property
     def is_continue(self) -> bool:
+        """Sim::isContinue (sim.hpp:26)."""
         return self._time()[3]
 
     def set_time(self, t: float, step: int) -> None:
+        """Sets the clock for a restart from a frame (no reference counterpart:
+        t and step are private, sim.hpp:48-49)."""
         _lib.check(self._L.gk_set_time(self.h, float(t), int(step)), self.h)
 
     def dt_log(self) -> List[float]:
+        """dt of every step since the last upload, at full precision (the values
+        Sim::Advance prints, sim.cpp:100-103)."""
         n = ctypes.c_int()
         _lib.check(self._L.gk_dt_log(self.h, None, 0, ctypes.byref(n)), self.h)
         buf = np.empty(max(n.value, 1), dtype=np.float64)
@@ -157,12 +173,16 @@ class Sim:
         return buf[:n.value].tolist()
 
     def cmax(self) -> float:
+        """EquationOfState::CalCmax seeded with 1e-16 (sim.cpp:77-78) of the
+        current state."""
         c = ctypes.c_double()
         _lib.check(self._L.gk_cmax(self.h, ctypes.byref(c)), self.h)
         return c.value
 
     @property
     def path(self) -> str:
+        """The device implementation selected: "generic", "fused2d", "stage3d"
+        or "run1d" (the results are the same bits in parity mode)."""
         p = ctypes.c_int()
         _lib.check(self._L.gk_path(self.h, ctypes.byref(p)), self.h)
         return {0: "generic", 1: "fused2d", 2: "stage3d", 3: "run1d"}[p.value]
@@ -240,6 +260,7 @@ class Sim:
 
     @property
     def stream(self) -> int:
+        """The handle's CUDA stream (a cudaStream_t as an integer)."""
         s = ctypes.c_void_p()
         _lib.check(self._L.gk_stream(self.h, ctypes.byref(s)), self.h)
         return s.value or 0
