@@ -1782,7 +1782,6 @@ extern "C" int gk_set_flux_model(gk_handle* h, const float* model_host, int nmod
     }
     // the path and the graph follow the model
     if (h->uploaded) {
-        const gk::Geom& g = h->ctx.g;
         set_path(h);
         if (h->path != 1) {
             int rc = alloc_generic(h);
