@@ -21,7 +21,6 @@ from __future__ import annotations
 
 import glob
 import os
-import subprocess
 from typing import List, Optional
 
 from ._build import BIN, CUDA_LIB, INCLUDE, LIB, OBJ, PKG, _newer, _run, build_cuda

@@ -8,7 +8,7 @@ Results equal those of running each instance alone.
 from __future__ import annotations
 
 import ctypes
-from typing import List, Optional, Sequence
+from typing import Optional, Sequence
 
 from . import _lib
 from .sim import Sim
