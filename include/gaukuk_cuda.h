@@ -200,7 +200,7 @@ int gk_run_steps(gk_handle* h, int nsteps, int* done);
  * Used to time a device-resident loop with events on gk_stream(). */
 int gk_enqueue_steps(gk_handle* h, int nsteps);
 
-/* Sim::GetTime / Getdt / GetStep and Sim::isContinue (sim.hpp:26,44-46). */
+/* Sim::GetTime / Getdt / GetStep and Sim::isContinue (sim.hpp:26, 43-45). */
 int gk_get_time(gk_handle* h, double* t, double* dt, int* step, int* is_continue);
 
 /* Sets the simulation clock, for a restart from a written frame (the frame
